@@ -1,0 +1,146 @@
+/*
+ * pfd_abi.h -- C ABI of the B200 plenoptic depth engine (libpfd.so).
+ *
+ * The engine replaces the GPU half of the reference's micro-image matching
+ * path.  In fengyunxuan6/plenoptic-for-depth that path is
+ *   MIStereoMatch::StereoMatchingForMIA_FrameCrossViews (MIStereo/MIStereoMatch.cpp:626-696)
+ *     -> AdaptMIPMFrame::Initialize / RunPatchMatchCUDAForFrame /
+ *        WriteBackResults / ReleaseMemory          (MIStereo/AdaptMIPMFrame.h:23-27)
+ *     -> RandomInitializationForFrame, CheckerboardUpdateFrame
+ *                                                  (MIStereo/AdaptMIPMFrame.cu:474-995)
+ * The C++ classes that keep the reference's signatures (AdaptMIPMFrame,
+ * MIStereoMatch; include/pfd/) sit on top of these functions.
+ *
+ * Conventions
+ *  - Every function returns a pfd_status: 0 on success, a negative PFD_E* code
+ *    otherwise; pfd_last_error() describes the last failure of a context.
+ *    Nothing here exits the process or resets the device (the reference's
+ *    CudaSafeCall exits, Common/CommonCUDA.cpp:77-86, and DepthSolver resets
+ *    the device every frame, DepthSolver.cpp:371).
+ *  - The caller owns every host buffer; the library owns the device state of
+ *    each frame until pfd_frame_free or pfd_destroy.
+ *  - One context per host thread.  Work is ordered on the context's stream;
+ *    functions that return host data synchronise that stream.
+ *  - Micro-image ("view") order is the caller's: the reference uses the
+ *    problem-map order, tile keys ascending by (row, column)
+ *    (Common/QuadTree.h:137-148, AdaptMIPMFrame.cpp:152-180).
+ */
+#ifndef PFD_ABI_H
+#define PFD_ABI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pfd_ctx pfd_ctx;
+typedef int pfd_status;
+
+#define PFD_OK           0
+#define PFD_EINVAL      -1   /* bad argument, size or parameter */
+#define PFD_ENOMEM      -2   /* device allocation failed or the context's HBM budget is exhausted */
+#define PFD_ECUDA       -3   /* a CUDA runtime call failed */
+#define PFD_ENOFRAME    -4   /* unknown frame id */
+#define PFD_ETIMEDOUT   -5   /* a bounded device wait gave up */
+#define PFD_ENODEV      -6   /* no such CUDA device */
+#define PFD_ESTATE      -7   /* call out of order (e.g. a sweep before initialisation) */
+
+/* Matching parameters: the fields of PatchMatchParamsLF (MVStereo/LFDepthInfo.h:19-46)
+ * that the frame path reads, as AdaptMIPMFrame::InitGPUParamsFromCPUParams sets
+ * them (AdaptMIPMFrame.cpp:126-143). */
+typedef struct {
+    int   max_iterations;    /* red-black iterations (3 in the reference) */
+    int   patch_size;        /* odd NCC patch side */
+    int   radius_increment;  /* tap stride inside the patch (1) */
+    int   top_k;             /* views averaged by the initial cost (5) */
+    float sigma_spatial;     /* bilateral spatial sigma (> 0) */
+    float sigma_color;       /* bilateral colour sigma (> 0) */
+    float depth_min;         /* disparity search range: 0 ... */
+    float depth_max;         /* ... baseline / 2 */
+    float base;              /* lens pitch in pixels (LightFieldParams::baseline) */
+} pfd_pm_params;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Opens a context on CUDA device `device` with its own stream.  hbm_budget_bytes
+ * caps the device memory the context's frames may hold (0 = no cap). */
+pfd_status pfd_create(pfd_ctx** out, int device, size_t hbm_budget_bytes);
+/* Frees every frame and the context.  Safe on NULL. */
+void pfd_destroy(pfd_ctx* ctx);
+/* Text of the context's last failure ("" if none).  Valid until the next call. */
+const char* pfd_last_error(pfd_ctx* ctx);
+/* The context's cudaStream_t, for callers that time or order work around it. */
+void* pfd_stream(pfd_ctx* ctx);
+/* Waits for the context's stream; reports any device-side error flag. */
+pfd_status pfd_sync(pfd_ctx* ctx);
+/* Device memory currently held by the context's frames. */
+size_t pfd_bytes_in_use(pfd_ctx* ctx);
+
+/* ---- frames ---------------------------------------------------------------
+ * Replaces AdaptMIPMFrame::Initialize (AdaptMIPMFrame.cpp:329-335):
+ * BuildViewIndexMap (:145-222) becomes the caller's arrays, InitializeGPU's
+ * texture objects and state buffers (:278-327) become the frame's device state.
+ *
+ *   raw        8-bit grayscale frame, W x H, row pitch raw_pitch bytes
+ *              (BGR2GRAY of the reference's raw is exact for gray input)
+ *   centers    [n_views][2] lens centres in raw pixels (MLA_Info::GetCenter)
+ *   tilekeys   [n_views][2] (column, row) tile keys; used by the consistency pass
+ *   mi_w, mi_h matching window, floor(pitch * 0.7071) (Common/Common.cpp:34-38);
+ *              view v's window starts at trunc(center - (mi - 1) / 2)
+ *              (DepthSolver.cpp:1894-1895), and must lie inside the frame
+ *   nb_ids     [n_views][max_nb] neighbour view ids in matching order, -1 padded
+ *              (m_NeighsSortVecForMatch, AdaptMIPMFrame.cpp:207-218)
+ *   nb_counts  [n_views], each <= max_nb <= 32
+ *   blur       optional [n_views][mi_h][mi_w] 8-bit blur channel
+ *              (MLA_Problem::m_Image_Blureness); NULL = no blur penalty
+ */
+pfd_status pfd_frame_create(pfd_ctx* ctx, int* frame_id, int W, int H,
+                            const float* centers, const int* tilekeys, int n_views,
+                            int mi_w, int mi_h, const int* nb_ids, const int* nb_counts,
+                            int max_nb, const uint8_t* blur);
+/* Copies a raw frame from host memory and slices the micro-images
+ * (Slice_RawMLAImage, DepthSolver.cpp:1951-1997). */
+pfd_status pfd_frame_set_raw(pfd_ctx* ctx, int frame_id, const uint8_t* raw, int raw_pitch);
+/* Same, from a raw frame already in this device's memory. */
+pfd_status pfd_frame_set_raw_device(pfd_ctx* ctx, int frame_id, const uint8_t* raw_dev, int raw_pitch);
+/* pfd_frame_create + pfd_frame_set_raw. */
+pfd_status pfd_frame_upload(pfd_ctx* ctx, int* frame_id, const uint8_t* raw, int W, int H, int raw_pitch,
+                            const float* centers, const int* tilekeys, int n_views,
+                            int mi_w, int mi_h, const int* nb_ids, const int* nb_counts,
+                            int max_nb, const uint8_t* blur);
+/* Releases a frame's device memory (AdaptMIPMFrame::ReleaseMemory, AdaptMIPMFrame.cpp:53-124). */
+pfd_status pfd_frame_free(pfd_ctx* ctx, int frame_id);
+
+/* ---- PatchMatch ------------------------------------------------------------
+ * Replaces AdaptMIPMFrame::RunPatchMatchCUDAForFrame (AdaptMIPMFrame.cpp:343-357,
+ * AdaptMIPMFrame.cu:949-995): random initialisation, then max_iterations x
+ * (red half-sweep, black half-sweep), enqueued without host synchronisation.
+ * seed keys the Philox streams (the reference seeds cuRAND from clock64()). */
+pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed);
+/* The steps of pfd_patchmatch, separately: RandomInitializationForFrame
+ * (AdaptMIPMFrame.cu:474-518) and one CheckerboardUpdateFrame launch (:520-947). */
+pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed);
+pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed,
+                        int iter, int phase);
+
+/* Per-hypothesis cost vectors: ComputeMultiViewCostVector_Frame
+ * (AdaptMIPMFrame.cu:181-225) for n (view, pixel, plane) hypotheses.
+ * vids[n], pxy[n][2] (x, y inside the window), planes[n][4] (nx, ny, nz, d);
+ * costs[n][max_nb] receives the costs (2.0 past the view's neighbour count). */
+pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
+                         const int* vids, const int* pxy, const float* planes, int n, float* costs);
+
+/* Copies the frame's current per-pixel state to host buffers, each
+ * [n_views * mi_w * mi_h] in view-major, row-major order; any may be NULL.
+ * Replaces the device-to-host copies of AdaptMIPMFrame.cpp:352-356 that
+ * WriteBackResults (:359-384) scatters into DisparityAndNormal::{ph_cuda,
+ * c_cuda, disp_v_cuda, selected_views}. */
+pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane /*[.][4]*/, float* cost,
+                        float* disp /*[.][4]*/, uint32_t* sel);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFD_ABI_H */

@@ -1,0 +1,104 @@
+/*
+ * oracle/pfd_oracle.h -- CPU oracle of the plenoptic depth hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the CPU
+ * baseline legs of bench.py load this library, and only to check or time the
+ * reference algorithm; the product library never links it.
+ *
+ * PARITY UNPINNED: the reference (fengyunxuan6/plenoptic-for-depth) ships no
+ * tests, fixtures or golden vectors, and it cannot be built here (it needs the
+ * OpenCV C++ SDK, Eigen, Boost, libpleno, yaml-cpp and libv, none of which is
+ * installed), so nothing the reference itself computed pins this restatement.
+ * What pins it instead: known-answer tests (fronto-parallel scenes, shifted
+ * copies), an FP64 cross-check, and a device test comparing the texture
+ * emulation with tex2D on a B200.
+ *
+ * Every function cites the reference lines it restates.  Arithmetic follows
+ * oracle/canon.h.
+ */
+#ifndef PFD_ORACLE_H
+#define PFD_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One frame of micro-images (views), the layout AdaptMIPMFrame builds in
+ * BuildViewIndexMap (AdaptMIPMFrame.cpp:145-222): views in problem-map order,
+ * neighbour ids padded with -1, counts per view. */
+typedef struct {
+    int n_views;
+    int mi_w, mi_h;              /* MLA_Mask_Width_Cuda / Height (AdaptMIPMFrame.cpp:139-140) */
+    int max_nb;                  /* m_max_neighbors (16 in the reference; up to 32 here) */
+    const float* gray;           /* [V][mi_h][mi_w], integer values 0..255 */
+    const float* blur;           /* [V][mi_h][mi_w] or NULL (no blur channel: penalty 0) */
+    const float* centers;        /* [V][2] lens centres, raw pixel coordinates */
+    const int* nb_ids;           /* [V][max_nb] view ids, -1 padded */
+    const int* nb_counts;        /* [V] */
+} orc_frame;
+
+/* PatchMatchParamsLF (LFDepthInfo.h:19-46) fields the Frame path reads. */
+typedef struct {
+    int max_iterations;
+    int patch_size;
+    int radius_increment;
+    int top_k;
+    float sigma_spatial;
+    float sigma_color;
+    float depth_min;
+    float depth_max;
+    float base;                  /* Base: lens pitch in pixels (AdaptMIPMFrame.cpp:138) */
+} orc_params;
+
+/* Per-pixel state, the four ping-pong buffers of AdaptMIPMFrame
+ * (AdaptMIPMFrame.cpp:311-318), each [V * mi_w * mi_h]. */
+typedef struct {
+    float* plane;                /* float4: nx, ny, nz, disparity */
+    float* cost;
+    float* disp;                 /* float4: d, d_real, baseline, baseline/d_real */
+    uint32_t* sel;
+} orc_state;
+
+/* Cost of each hypothesis against each neighbour of its view:
+ * ComputeMultiViewCostVector_Frame (AdaptMIPMFrame.cu:181-225).  costs is
+ * [n][max_nb] (2.0 beyond the view's count), disps [n][max_nb][4]. */
+int orc_cost_vectors(const orc_frame* f, const orc_params* p, const int* vids, const int* pxy,
+                     const float* planes, int n, float* costs, float* disps);
+
+/* NCC of one (pixel, plane, neighbour) in FP64 with exact (unquantised)
+ * bilinear sampling: the precision oracle. */
+double orc_ncc_fp64(const orc_frame* f, const orc_params* p, int vid, int k, int px, int py,
+                    const float* plane);
+
+/* RandomInitializationForFrame (AdaptMIPMFrame.cu:474-518) over all pixels. */
+int orc_pm_init(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int nthreads);
+
+/* One CheckerboardUpdateFrame launch (AdaptMIPMFrame.cu:520-947): next <- update(prev). */
+int orc_pm_sweep(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
+                 const orc_state* prev, orc_state* next, int nthreads);
+
+/* Same, restricted to views [v0, v1): the bounded sample the CPU baseline times. */
+int orc_pm_sweep_views(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
+                       const orc_state* prev, orc_state* next, int v0, int v1, int nthreads);
+
+/* RunPatchMatchCUDAForFrame_Impl (AdaptMIPMFrame.cu:949-995): init, then
+ * max_iterations x (phase 0, phase 1).  Result in out. */
+int orc_patchmatch(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int nthreads);
+
+/* Scalar hooks for unit tests of the canonical arithmetic. */
+float orc_expf(float x);
+float orc_uniform(uint64_t seed, uint32_t sweep, uint32_t pixel, uint32_t n);
+float orc_tex_fetch(const float* img, int w, int h, float sx, float sy);
+void  orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* Count of NCC taps with both reference and source sample inside the window,
+ * for the hypotheses given (the algorithmic unit of the roofline). */
+long long orc_count_taps(const orc_frame* f, const orc_params* p, const int* vids, const int* pxy,
+                         const float* planes, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

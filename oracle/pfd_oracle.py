@@ -1,0 +1,176 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py, never by the product.  PARITY UNPINNED: see
+oracle/pfd_oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+
+class OrcFrame(ctypes.Structure):
+    _fields_ = [("n_views", _I), ("mi_w", _I), ("mi_h", _I), ("max_nb", _I), ("gray", _P), ("blur", _P),
+                ("centers", _P), ("nb_ids", _P), ("nb_counts", _P)]
+
+
+class OrcParams(ctypes.Structure):
+    _fields_ = [("max_iterations", _I), ("patch_size", _I), ("radius_increment", _I), ("top_k", _I),
+                ("sigma_spatial", _F), ("sigma_color", _F), ("depth_min", _F), ("depth_max", _F), ("base", _F)]
+
+
+class OrcState(ctypes.Structure):
+    _fields_ = [("plane", _P), ("cost", _P), ("disp", _P), ("sel", _P)]
+
+
+def build() -> str:
+    """make -C oracle (gcc, -ffp-contract=off)."""
+    r = subprocess.run(["make", "-s", "-C", ORACLE_DIR], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        FP, PP, SP = ctypes.POINTER(OrcFrame), ctypes.POINTER(OrcParams), ctypes.POINTER(OrcState)
+        L.orc_cost_vectors.argtypes = [FP, PP, _P, _P, _P, _I, _P, _P]
+        L.orc_count_taps.argtypes = [FP, PP, _P, _P, _P, _I]
+        L.orc_count_taps.restype = ctypes.c_longlong
+        L.orc_ncc_fp64.argtypes = [FP, PP, _I, _I, _I, _I, _P]
+        L.orc_ncc_fp64.restype = ctypes.c_double
+        L.orc_pm_init.argtypes = [FP, PP, ctypes.c_uint64, SP, _I]
+        L.orc_pm_sweep.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I]
+        L.orc_pm_sweep_views.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I, _I, _I]
+        L.orc_patchmatch.argtypes = [FP, PP, ctypes.c_uint64, SP, _I]
+        L.orc_expf.argtypes = [_F]
+        L.orc_expf.restype = _F
+        L.orc_uniform.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+        L.orc_uniform.restype = _F
+        L.orc_tex_fetch.argtypes = [_P, _I, _I, _F, _F]
+        L.orc_tex_fetch.restype = _F
+        L.orc_philox.argtypes = [_P, _P, _P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+class Oracle:
+    """One frame of views for the oracle.  gray: [V][h][w] uint8/float."""
+
+    def __init__(self, gray, centers, nb_ids, nb_counts, blur=None):
+        self.gray = np.ascontiguousarray(gray, dtype=np.float32)
+        self.blur = None if blur is None else np.ascontiguousarray(blur, dtype=np.float32)
+        self.centers = np.ascontiguousarray(centers, dtype=np.float32)
+        self.nb_ids = np.ascontiguousarray(nb_ids, dtype=np.int32)
+        self.nb_counts = np.ascontiguousarray(nb_counts, dtype=np.int32)
+        V, h, w = self.gray.shape
+        self.V, self.h, self.w = V, h, w
+        self.K = self.nb_ids.shape[1]
+        self.f = OrcFrame(V, w, h, self.K, _p(self.gray), _p(self.blur), _p(self.centers), _p(self.nb_ids),
+                          _p(self.nb_counts))
+
+    @staticmethod
+    def params(p) -> OrcParams:
+        """From the package's PmParams (same fields)."""
+        c = p.c()
+        return OrcParams(c.max_iterations, c.patch_size, c.radius_increment, c.top_k, c.sigma_spatial, c.sigma_color,
+                         c.depth_min, c.depth_max, c.base)
+
+    def new_state(self):
+        n = self.V * self.h * self.w
+        arr = dict(plane=np.zeros((n, 4), np.float32), cost=np.zeros(n, np.float32),
+                   disp=np.zeros((n, 4), np.float32), sel=np.zeros(n, np.uint32))
+        st = OrcState(_p(arr["plane"]), _p(arr["cost"]), _p(arr["disp"]), _p(arr["sel"]))
+        return arr, st
+
+    def cost_vectors(self, params, vids, pxy, planes):
+        v = np.ascontiguousarray(vids, np.int32)
+        xy = np.ascontiguousarray(pxy, np.int32)
+        pl = np.ascontiguousarray(planes, np.float32)
+        costs = np.empty((v.shape[0], self.K), np.float32)
+        disps = np.empty((v.shape[0], self.K, 4), np.float32)
+        p = self.params(params)
+        rc = lib().orc_cost_vectors(ctypes.byref(self.f), ctypes.byref(p), _p(v), _p(xy), _p(pl), v.shape[0],
+                                    _p(costs), _p(disps))
+        assert rc == 0
+        return costs, disps
+
+    def count_taps(self, params, vids, pxy, planes) -> int:
+        v = np.ascontiguousarray(vids, np.int32)
+        xy = np.ascontiguousarray(pxy, np.int32)
+        pl = np.ascontiguousarray(planes, np.float32)
+        p = self.params(params)
+        return int(lib().orc_count_taps(ctypes.byref(self.f), ctypes.byref(p), _p(v), _p(xy), _p(pl), v.shape[0]))
+
+    def ncc_fp64(self, params, vid, k, px, py, plane) -> float:
+        pl = np.ascontiguousarray(plane, np.float32)
+        p = self.params(params)
+        return float(lib().orc_ncc_fp64(ctypes.byref(self.f), ctypes.byref(p), vid, k, px, py, _p(pl)))
+
+    def init(self, params, seed, nthreads=0):
+        arr, st = self.new_state()
+        p = self.params(params)
+        assert lib().orc_pm_init(ctypes.byref(self.f), ctypes.byref(p), seed, ctypes.byref(st), nthreads) == 0
+        return arr
+
+    def sweep(self, params, seed, it, phase, prev, nthreads=0, views=None):
+        arr, st = self.new_state()
+        ps = OrcState(_p(prev["plane"]), _p(prev["cost"]), _p(prev["disp"]), _p(prev["sel"]))
+        p = self.params(params)
+        if views is None:
+            rc = lib().orc_pm_sweep(ctypes.byref(self.f), ctypes.byref(p), seed, it, phase, ctypes.byref(ps),
+                                    ctypes.byref(st), nthreads)
+        else:
+            rc = lib().orc_pm_sweep_views(ctypes.byref(self.f), ctypes.byref(p), seed, it, phase, ctypes.byref(ps),
+                                          ctypes.byref(st), views[0], views[1], nthreads)
+        assert rc == 0
+        return arr
+
+    def patchmatch(self, params, seed, nthreads=0):
+        arr, st = self.new_state()
+        p = self.params(params)
+        assert lib().orc_patchmatch(ctypes.byref(self.f), ctypes.byref(p), seed, ctypes.byref(st), nthreads) == 0
+        return arr
+
+
+def expf(x: float) -> float:
+    return float(lib().orc_expf(x))
+
+
+def uniform(seed: int, sweep: int, pixel: int, n: int) -> float:
+    return float(lib().orc_uniform(seed, sweep, pixel, n))
+
+
+def tex_fetch(img: np.ndarray, sx: float, sy: float) -> float:
+    a = np.ascontiguousarray(img, np.float32)
+    return float(lib().orc_tex_fetch(_p(a), a.shape[1], a.shape[0], sx, sy))
+
+
+def philox(ctr, key):
+    c = np.asarray(ctr, np.uint32)
+    k = np.asarray(key, np.uint32)
+    o = np.zeros(4, np.uint32)
+    lib().orc_philox(_p(c), _p(k), _p(o))
+    return [int(x) for x in o]

@@ -1,0 +1,342 @@
+"""Python binding of the B200 plenoptic depth engine (libpfd.so).
+
+A thin ctypes layer over include/pfd_abi.h, the way a maintainer of the
+reference would bind the C ABI from Python.  Every call goes to the CUDA
+library: there is no CPU fallback, and loading fails loudly when the library
+has not been built.
+
+    ctx = Context(device=0)
+    fid = ctx.frame_upload(raw, centers, tilekeys, mi_w, mi_h, nb_ids, nb_counts)
+    ctx.patchmatch(fid, PmParams(...), seed=1)
+    plane, cost, disp, sel = ctx.download(fid)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+BUILD_DIR = os.path.join(PKG_DIR, "_build")
+LIB_PATH = os.path.join(BUILD_DIR, "libpfd.so")
+SYNTH_PATH = os.path.join(BUILD_DIR, "libpfd_synth.so")
+
+PFD_OK = 0
+_ERRNAMES = {-1: "PFD_EINVAL", -2: "PFD_ENOMEM", -3: "PFD_ECUDA", -4: "PFD_ENOFRAME",
+             -5: "PFD_ETIMEDOUT", -6: "PFD_ENODEV", -7: "PFD_ESTATE"}
+
+
+class PfdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class PmParamsC(ctypes.Structure):
+    _fields_ = [("max_iterations", ctypes.c_int), ("patch_size", ctypes.c_int), ("radius_increment", ctypes.c_int),
+                ("top_k", ctypes.c_int), ("sigma_spatial", ctypes.c_float), ("sigma_color", ctypes.c_float),
+                ("depth_min", ctypes.c_float), ("depth_max", ctypes.c_float), ("base", ctypes.c_float)]
+
+
+@dataclass
+class PmParams:
+    """PatchMatchParamsLF fields of the frame path (LFDepthInfo.h:19-46)."""
+    base: float
+    max_iterations: int = 3
+    patch_size: int = 11
+    radius_increment: int = 1
+    top_k: int = 5
+    sigma_spatial: float = 3.0
+    sigma_color: float = 12.0
+    depth_min: float = 0.0
+    depth_max: float = field(default=-1.0)
+
+    def c(self) -> PmParamsC:
+        dmax = self.depth_max if self.depth_max >= 0 else self.base * 0.5
+        return PmParamsC(self.max_iterations, self.patch_size, self.radius_increment, self.top_k,
+                         self.sigma_spatial, self.sigma_color, self.depth_min, dmax, self.base)
+
+
+_lib = None
+_synth = None
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+
+def lib() -> ctypes.CDLL:
+    """The engine library.  Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run plenoptic-for-depth_b200/build.py (nvcc, sm_100a)")
+        L = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "pfd_create": [ctypes.POINTER(_P), _I, ctypes.c_size_t],
+            "pfd_destroy": [_P],
+            "pfd_last_error": [_P],
+            "pfd_stream": [_P],
+            "pfd_sync": [_P],
+            "pfd_bytes_in_use": [_P],
+            "pfd_frame_create": [_P, ctypes.POINTER(_I), _I, _I, _P, _P, _I, _I, _I, _P, _P, _I, _P],
+            "pfd_frame_set_raw": [_P, _I, _P, _I],
+            "pfd_frame_set_raw_device": [_P, _I, _P, _I],
+            "pfd_frame_upload": [_P, ctypes.POINTER(_I), _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _I, _P],
+            "pfd_frame_free": [_P, _I],
+            "pfd_patchmatch": [_P, _I, ctypes.POINTER(PmParamsC), ctypes.c_uint64],
+            "pfd_pm_init": [_P, _I, ctypes.POINTER(PmParamsC), ctypes.c_uint64],
+            "pfd_pm_sweep": [_P, _I, ctypes.POINTER(PmParamsC), ctypes.c_uint64, _I, _I],
+            "pfd_ncc_costs": [_P, _I, ctypes.POINTER(PmParamsC), _P, _P, _P, _I, _P],
+            "pfd_download": [_P, _I, _P, _P, _P, _P],
+            "pfd_neighbors_by_baseline": [_P, _P, _I, _F, _I, _I, _P, _P],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = _I
+        L.pfd_destroy.restype = None
+        L.pfd_last_error.restype = ctypes.c_char_p
+        L.pfd_stream.restype = _P
+        L.pfd_bytes_in_use.restype = ctypes.c_size_t
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def neighbors_by_baseline(centers: np.ndarray, tilekeys: np.ndarray, pitch: float, max_nb: int,
+                          rings: int = 5) -> tuple[np.ndarray, np.ndarray]:
+    """Ordered matching neighbours per view (see include/pfd_host.h)."""
+    c = np.ascontiguousarray(centers, dtype=np.float32)
+    k = np.ascontiguousarray(tilekeys, dtype=np.int32)
+    n = c.shape[0]
+    ids = np.full((n, max_nb), -1, np.int32)
+    cnt = np.zeros(n, np.int32)
+    rc = lib().pfd_neighbors_by_baseline(_ptr(c), _ptr(k), n, float(pitch), rings, max_nb, _ptr(ids), _ptr(cnt))
+    if rc != PFD_OK:
+        raise PfdError(rc, "pfd_neighbors_by_baseline")
+    return ids, cnt
+
+
+class Context:
+    """One engine context (device, stream, frames); see include/pfd_abi.h."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self._L = lib()
+        h = _P()
+        rc = self._L.pfd_create(ctypes.byref(h), device, hbm_budget)
+        if rc != PFD_OK:
+            raise PfdError(rc, f"pfd_create(device={device})")
+        self._h = h
+        self._frames: dict[int, dict] = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.pfd_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != PFD_OK:
+            msg = self._L.pfd_last_error(self._h)
+            raise PfdError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    @property
+    def stream(self) -> int:
+        return self._L.pfd_stream(self._h)
+
+    def sync(self) -> None:
+        self._check(self._L.pfd_sync(self._h), "pfd_sync")
+
+    def bytes_in_use(self) -> int:
+        return self._L.pfd_bytes_in_use(self._h)
+
+    def frame_create(self, W: int, H: int, centers, tilekeys, mi_w: int, mi_h: int, nb_ids, nb_counts,
+                     blur=None) -> int:
+        c = np.ascontiguousarray(centers, dtype=np.float32)
+        k = np.ascontiguousarray(tilekeys, dtype=np.int32)
+        ids = np.ascontiguousarray(nb_ids, dtype=np.int32)
+        cnt = np.ascontiguousarray(nb_counts, dtype=np.int32)
+        b = None if blur is None else np.ascontiguousarray(blur, dtype=np.uint8)
+        fid = _I()
+        self._check(self._L.pfd_frame_create(self._h, ctypes.byref(fid), W, H, _ptr(c), _ptr(k), c.shape[0], mi_w,
+                                             mi_h, _ptr(ids), _ptr(cnt), ids.shape[1], _ptr(b)), "pfd_frame_create")
+        self._frames[fid.value] = dict(V=c.shape[0], mi_w=mi_w, mi_h=mi_h, K=ids.shape[1], W=W, H=H)
+        return fid.value
+
+    def frame_set_raw(self, fid: int, raw: np.ndarray) -> None:
+        r = np.ascontiguousarray(raw, dtype=np.uint8)
+        self._check(self._L.pfd_frame_set_raw(self._h, fid, _ptr(r), r.shape[1]), "pfd_frame_set_raw")
+
+    def frame_set_raw_device(self, fid: int, dev_ptr: int, pitch: int) -> None:
+        self._check(self._L.pfd_frame_set_raw_device(self._h, fid, _P(dev_ptr), pitch), "pfd_frame_set_raw_device")
+
+    def frame_upload(self, raw, centers, tilekeys, mi_w, mi_h, nb_ids, nb_counts, blur=None) -> int:
+        fid = self.frame_create(raw.shape[1], raw.shape[0], centers, tilekeys, mi_w, mi_h, nb_ids, nb_counts, blur)
+        try:
+            self.frame_set_raw(fid, raw)
+        except Exception:
+            self.frame_free(fid)
+            raise
+        return fid
+
+    def frame_free(self, fid: int) -> None:
+        self._check(self._L.pfd_frame_free(self._h, fid), "pfd_frame_free")
+        self._frames.pop(fid, None)
+
+    def patchmatch(self, fid: int, params: PmParams, seed: int) -> None:
+        p = params.c()
+        self._check(self._L.pfd_patchmatch(self._h, fid, ctypes.byref(p), seed), "pfd_patchmatch")
+
+    def pm_init(self, fid: int, params: PmParams, seed: int) -> None:
+        p = params.c()
+        self._check(self._L.pfd_pm_init(self._h, fid, ctypes.byref(p), seed), "pfd_pm_init")
+
+    def pm_sweep(self, fid: int, params: PmParams, seed: int, it: int, phase: int) -> None:
+        p = params.c()
+        self._check(self._L.pfd_pm_sweep(self._h, fid, ctypes.byref(p), seed, it, phase), "pfd_pm_sweep")
+
+    def ncc_costs(self, fid: int, params: PmParams, vids, pxy, planes) -> np.ndarray:
+        v = np.ascontiguousarray(vids, dtype=np.int32)
+        xy = np.ascontiguousarray(pxy, dtype=np.int32)
+        pl = np.ascontiguousarray(planes, dtype=np.float32)
+        K = self._frames[fid]["K"]
+        out = np.empty((v.shape[0], K), np.float32)
+        p = params.c()
+        self._check(self._L.pfd_ncc_costs(self._h, fid, ctypes.byref(p), _ptr(v), _ptr(xy), _ptr(pl), v.shape[0],
+                                          _ptr(out)), "pfd_ncc_costs")
+        return out
+
+    def download(self, fid: int):
+        f = self._frames[fid]
+        n = f["V"] * f["mi_w"] * f["mi_h"]
+        plane = np.empty((n, 4), np.float32)
+        cost = np.empty(n, np.float32)
+        disp = np.empty((n, 4), np.float32)
+        sel = np.empty(n, np.uint32)
+        self._check(self._L.pfd_download(self._h, fid, _ptr(plane), _ptr(cost), _ptr(disp), _ptr(sel)), "pfd_download")
+        return plane, cost, disp, sel
+
+
+# ---------------------------------------------------------------------------
+# synthetic frames
+# ---------------------------------------------------------------------------
+class SynthConfigC(ctypes.Structure):
+    _fields_ = [("width", _I), ("height", _I), ("pitch", _F), ("n_planes", _I), ("vd_min", _F), ("vd_max", _F),
+                ("noise_sigma", _F), ("n_lens_types", _I), ("blur_sigma", _F * 3), ("texture_cell", _F),
+                ("seed", ctypes.c_uint64)]
+
+
+def synth_lib() -> ctypes.CDLL:
+    global _synth
+    if _synth is None:
+        if not os.path.exists(SYNTH_PATH):
+            raise ImportError(f"{SYNTH_PATH} is missing: run plenoptic-for-depth_b200/build.py")
+        S = ctypes.CDLL(SYNTH_PATH)
+        S.pfd_synth_count.argtypes = [ctypes.POINTER(SynthConfigC), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                                      ctypes.POINTER(_I)]
+        S.pfd_synth_render.argtypes = [ctypes.POINTER(SynthConfigC), _P, _P, _P, _P, _P]
+        _synth = S
+    return _synth
+
+
+@dataclass
+class SynthFrame:
+    raw: np.ndarray          # [H][W] uint8
+    centers: np.ndarray      # [L][2] float32
+    tilekeys: np.ndarray     # [L][2] int32 (column, row)
+    types: np.ndarray        # [L] int32
+    vd_center: np.ndarray    # [L] float32
+    pitch: float
+    n_cols: int
+    n_rows: int
+
+
+def synth_frame(width: int, height: int, pitch: float, n_planes: int, seed: int, vd_min: float = 2.0,
+                vd_max: float = 12.0, noise_sigma: float = 2.0, n_lens_types: int = 1,
+                blur_sigma=(0.0, 0.0, 0.0), texture_cell: float = 0.0) -> SynthFrame:
+    """Seeded synthetic plenoptic raw frame (csrc/synth.c)."""
+    cfg = SynthConfigC(width, height, pitch, n_planes, vd_min, vd_max, noise_sigma, n_lens_types,
+                       (_F * 3)(*blur_sigma), texture_cell, seed)
+    S = synth_lib()
+    n, nc, nr = _I(), _I(), _I()
+    if S.pfd_synth_count(ctypes.byref(cfg), ctypes.byref(n), ctypes.byref(nc), ctypes.byref(nr)) != 0:
+        raise ValueError("bad synthetic frame configuration")
+    raw = np.empty((height, width), np.uint8)
+    cen = np.empty((n.value, 2), np.float32)
+    keys = np.empty((n.value, 2), np.int32)
+    types = np.empty(n.value, np.int32)
+    vd = np.empty(n.value, np.float32)
+    if S.pfd_synth_render(ctypes.byref(cfg), _ptr(raw), _ptr(cen), _ptr(keys), _ptr(types), _ptr(vd)) != 0:
+        raise ValueError("synthetic rendering failed")
+    return SynthFrame(raw, cen, keys, types, vd, pitch, nc.value, nr.value)
+
+
+def mi_window(pitch: float) -> int:
+    """mi_width_for_match = floor(pitch * 0.707106781186) (Common/Common.cpp:34-38)."""
+    return int(pitch * 0.707106781186)
+
+
+def window_origins(centers: np.ndarray, mi: int) -> np.ndarray:
+    """trunc(c - (mi - 1) / 2) as DepthSolver.cpp:1894-1895 and cv::Rect compute it."""
+    c = np.asarray(centers, np.float32).astype(np.float64)
+    o = (c - (mi - 1) * 0.5).astype(np.float32)
+    return np.trunc(o).astype(np.int32)
+
+
+def valid_views(frame: SynthFrame, mi: int) -> np.ndarray:
+    """Indices of lenses whose matching window lies inside the frame
+    (the abandon test of DepthSolver::CreateProblemsAndDisNormals_Frame, :1893-1903)."""
+    H, W = frame.raw.shape
+    c = frame.centers.astype(np.float64)
+    lo = (c - (mi - 1) * 0.5).astype(np.float32)
+    o = np.trunc(lo).astype(np.int64)
+    ok = (lo[:, 0] >= 0) & (lo[:, 1] >= 0) & (o[:, 0] + mi <= W) & (o[:, 1] + mi <= H)
+    return np.nonzero(ok)[0]
+
+
+def slice_views(raw: np.ndarray, centers: np.ndarray, mi: int) -> np.ndarray:
+    """Host slicing of the micro-image windows, [V][mi][mi] uint8."""
+    o = window_origins(centers, mi)
+    out = np.empty((o.shape[0], mi, mi), np.uint8)
+    for v, (x, y) in enumerate(o):
+        out[v] = raw[y:y + mi, x:x + mi]
+    return out
+
+
+@dataclass
+class Workload:
+    """A frame ready for matching: valid views, their windows, neighbour lists."""
+    frame: SynthFrame
+    mi: int
+    centers: np.ndarray
+    tilekeys: np.ndarray
+    nb_ids: np.ndarray
+    nb_counts: np.ndarray
+    gray: np.ndarray         # [V][mi][mi] uint8 (host slice, for the oracle)
+
+
+def make_workload(width: int, height: int, pitch: float, n_planes: int, seed: int, max_nb: int, **kw) -> Workload:
+    fr = synth_frame(width, height, pitch, n_planes, seed, **kw)
+    mi = mi_window(pitch)
+    keep = valid_views(fr, mi)
+    centers = np.ascontiguousarray(fr.centers[keep])
+    keys = np.ascontiguousarray(fr.tilekeys[keep])
+    ids, cnt = neighbors_by_baseline(centers, keys, pitch, max_nb)
+    return Workload(fr, mi, centers, keys, ids, cnt, slice_views(fr.raw, centers, mi))

@@ -1,0 +1,507 @@
+// pfd_abi.cu -- implementation of include/pfd_abi.h: contexts, frames and the
+// PatchMatch entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/pfd_abi.h"
+#include "pm_kernels.h"
+
+namespace {
+
+struct Frame {
+    int W = 0, H = 0;                 // raw frame
+    int V = 0, mi_w = 0, mi_h = 0, K = 0, tile_stride = 0;
+    bool has_raw = false, has_blur = false;
+    uint8_t* d_raw = nullptr;
+    uint8_t* d_gray = nullptr;
+    uint8_t* d_blur = nullptr;
+    float2* d_centers = nullptr;
+    int2* d_tilekeys = nullptr;
+    int2* d_origin = nullptr;
+    int* d_nb_ids = nullptr;
+    int* d_nb_counts = nullptr;
+    pfd::StateDev s[2] = {};
+    int cur = 0;                      // s[cur] is the latest state
+    bool has_state = false;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+};
+
+}  // namespace
+
+struct pfd_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0, used = 0;
+    int next_id = 1;
+    std::map<int, Frame> frames;
+    int* d_err = nullptr;
+    std::string last_error;
+};
+
+namespace {
+
+pfd_status fail(pfd_ctx* c, pfd_status code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->last_error = buf;
+    return code;
+}
+
+#define CU(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(ctx, PFD_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int now = -1;
+        cudaGetDevice(&now);
+        if (prev >= 0 && now != prev) cudaSetDevice(prev);
+    }
+};
+
+pfd_status frame_alloc(pfd_ctx* ctx, Frame& f, void** p, size_t bytes)
+{
+    if (ctx->budget && ctx->used + f.bytes + bytes > ctx->budget)
+        return fail(ctx, PFD_ENOMEM, "HBM budget exceeded: %zu in use + %zu requested > %zu",
+                    ctx->used + f.bytes, bytes, ctx->budget);
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, PFD_ENOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    f.allocs.push_back(*p);
+    f.bytes += bytes;
+    return PFD_OK;
+}
+
+void frame_release(Frame& f)
+{
+    for (void* p : f.allocs) cudaFree(p);
+    f.allocs.clear();
+    f.bytes = 0;
+}
+
+Frame* find_frame(pfd_ctx* ctx, int id)
+{
+    auto it = ctx->frames.find(id);
+    return it == ctx->frames.end() ? nullptr : &it->second;
+}
+
+pfd_status check_params(pfd_ctx* ctx, const Frame& f, const pfd_pm_params* p)
+{
+    if (!p) return fail(ctx, PFD_EINVAL, "params is NULL");
+    if (p->patch_size < 1 || (p->patch_size & 1) == 0 || p->patch_size > 31)
+        return fail(ctx, PFD_EINVAL, "patch_size must be odd in [1, 31], got %d", p->patch_size);
+    if (p->radius_increment < 1) return fail(ctx, PFD_EINVAL, "radius_increment must be >= 1");
+    if (!(p->sigma_spatial > 0.0f) || !(p->sigma_color > 0.0f))
+        return fail(ctx, PFD_EINVAL, "sigma_spatial and sigma_color must be > 0");
+    if (!(p->base > 0.0f)) return fail(ctx, PFD_EINVAL, "base (lens pitch) must be > 0");
+    if (p->top_k < 1) return fail(ctx, PFD_EINVAL, "top_k must be >= 1");
+    if (p->max_iterations < 0) return fail(ctx, PFD_EINVAL, "max_iterations must be >= 0");
+    if (!f.has_raw) return fail(ctx, PFD_ESTATE, "frame has no raw image yet");
+    return PFD_OK;
+}
+
+pfd::PmParams make_params(const Frame& f, const pfd_pm_params* p, uint64_t seed)
+{
+    pfd::PmParams P;
+    P.W = f.mi_w; P.H = f.mi_h; P.ppv = f.mi_w * f.mi_h;
+    P.K = f.K;
+    P.radius = p->patch_size / 2;
+    P.inc = p->radius_increment;
+    P.ntap = (2 * P.radius) / P.inc + 1;
+    P.top_k = p->top_k;
+    P.ss2 = (2.0f * p->sigma_spatial) * p->sigma_spatial;
+    P.cc2 = (2.0f * p->sigma_color) * p->sigma_color;
+    P.depth_min = p->depth_min;
+    P.depth_max = p->depth_max;
+    P.base = p->base;
+    P.inv_base = 1.0f / std::max(p->base, 1e-6f);
+    P.pert_pi = (float)((double)0.02f * 3.14159265358979323846);
+    const float fw = (float)f.mi_w, fh = (float)f.mi_h;
+    std::memcpy(&P.W_bits, &fw, 4);
+    std::memcpy(&P.H_bits, &fh, 4);
+    P.tile_stride = f.tile_stride;
+    P.seed = seed;
+    return P;
+}
+
+pfd::FrameDev frame_dev(const Frame& f)
+{
+    pfd::FrameDev F;
+    F.gray = f.d_gray;
+    F.blur = f.has_blur ? f.d_blur : nullptr;
+    F.centers = f.d_centers;
+    F.nb_ids = f.d_nb_ids;
+    F.nb_counts = f.d_nb_counts;
+    F.V = f.V;
+    return F;
+}
+
+pfd_status check_device_error(pfd_ctx* ctx)
+{
+    int h = 0;
+    CU(cudaMemcpyAsync(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+        return fail(ctx, PFD_ETIMEDOUT, "device wait timed out (flags 0x%x)", h);
+    }
+    return PFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pfd_status pfd_create(pfd_ctx** out, int device, size_t hbm_budget_bytes)
+{
+    pfd_ctx* ctx = nullptr;
+    if (!out) return PFD_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return PFD_ENODEV;
+    }
+    ctx = new (std::nothrow) pfd_ctx;
+    if (!ctx) return PFD_ENOMEM;
+    ctx->device = device;
+    ctx->budget = hbm_budget_bytes;
+    DeviceGuard g(device);
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        if (ctx->d_err) cudaFree(ctx->d_err);
+        delete ctx;
+        return PFD_ECUDA;
+    }
+    *out = ctx;
+    return PFD_OK;
+}
+
+void pfd_destroy(pfd_ctx* ctx)
+{
+    if (!ctx) return;
+    DeviceGuard g(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->frames) frame_release(kv.second);
+    ctx->frames.clear();
+    cudaFree(ctx->d_err);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* pfd_last_error(pfd_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+void* pfd_stream(pfd_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+size_t pfd_bytes_in_use(pfd_ctx* ctx) { return ctx ? ctx->used : 0; }
+
+pfd_status pfd_sync(pfd_ctx* ctx)
+{
+    if (!ctx) return PFD_EINVAL;
+    DeviceGuard g(ctx->device);
+    return check_device_error(ctx);
+}
+
+pfd_status pfd_frame_create(pfd_ctx* ctx, int* frame_id, int W, int H, const float* centers, const int* tilekeys,
+                            int n_views, int mi_w, int mi_h, const int* nb_ids, const int* nb_counts, int max_nb,
+                            const uint8_t* blur)
+{
+    if (!ctx || !frame_id) return PFD_EINVAL;
+    *frame_id = 0;
+    if (W <= 0 || H <= 0 || n_views <= 0 || !centers || !tilekeys || !nb_ids || !nb_counts)
+        return fail(ctx, PFD_EINVAL, "frame_create: bad sizes or NULL arrays");
+    if (mi_w < 2 || mi_h < 2 || mi_w > 64 || mi_h > 64)
+        return fail(ctx, PFD_EINVAL, "micro-image window %dx%d outside [2, 64]", mi_w, mi_h);
+    if (max_nb < 1 || max_nb > pfd::kMaxNb)
+        return fail(ctx, PFD_EINVAL, "max_nb %d outside [1, 32] (selected-view masks are 32 bits)", max_nb);
+    Frame f;
+    f.W = W; f.H = H; f.V = n_views; f.mi_w = mi_w; f.mi_h = mi_h; f.K = max_nb;
+    f.tile_stride = (mi_w * mi_h + 15) & ~15;
+    f.has_blur = blur != nullptr;
+    std::vector<int2> origin(n_views);
+    for (int v = 0; v < n_views; ++v) {
+        const float cx = centers[2 * v], cy = centers[2 * v + 1];
+        if (!std::isfinite(cx) || !std::isfinite(cy)) return fail(ctx, PFD_EINVAL, "view %d: centre not finite", v);
+        // DepthSolver.cpp:1894-1895 (float minus double, stored as float), then the
+        // int conversion of cv::Rect (:1977-1978)
+        const float ox = (float)((double)cx - (mi_w - 1) * 0.5);
+        const float oy = (float)((double)cy - (mi_h - 1) * 0.5);
+        if (!(ox >= 0.0f) || !(oy >= 0.0f))
+            return fail(ctx, PFD_EINVAL, "view %d: window origin (%g, %g) outside the frame", v, ox, oy);
+        const int ix = (int)ox, iy = (int)oy;
+        if (ix + mi_w > W || iy + mi_h > H)
+            return fail(ctx, PFD_EINVAL, "view %d: window [%d,%d]+%dx%d outside the %dx%d frame", v, ix, iy, mi_w, mi_h, W, H);
+        origin[v] = make_int2(ix, iy);
+        if (nb_counts[v] < 0 || nb_counts[v] > max_nb)
+            return fail(ctx, PFD_EINVAL, "view %d: neighbour count %d outside [0, %d]", v, nb_counts[v], max_nb);
+        for (int k = 0; k < nb_counts[v]; ++k) {
+            const int id = nb_ids[v * max_nb + k];
+            if (id >= n_views || id < -1 || id == v)
+                return fail(ctx, PFD_EINVAL, "view %d: neighbour %d has id %d", v, k, id);
+        }
+    }
+    DeviceGuard g(ctx->device);
+    const size_t ppv_tiles = (size_t)n_views * f.tile_stride;
+    const size_t px = (size_t)n_views * mi_w * mi_h;
+    pfd_status st = PFD_OK;
+    auto A = [&](void** p, size_t b) { if (st == PFD_OK) st = frame_alloc(ctx, f, p, b); };
+    A((void**)&f.d_raw, (size_t)W * H);
+    A((void**)&f.d_gray, ppv_tiles);
+    if (blur) A((void**)&f.d_blur, ppv_tiles);
+    A((void**)&f.d_centers, sizeof(float2) * n_views);
+    A((void**)&f.d_tilekeys, sizeof(int2) * n_views);
+    A((void**)&f.d_origin, sizeof(int2) * n_views);
+    A((void**)&f.d_nb_ids, sizeof(int) * (size_t)n_views * max_nb);
+    A((void**)&f.d_nb_counts, sizeof(int) * n_views);
+    for (int b = 0; b < 2; ++b) {
+        A((void**)&f.s[b].plane, sizeof(float4) * px);
+        A((void**)&f.s[b].cost, sizeof(float) * px);
+        A((void**)&f.s[b].disp, sizeof(float4) * px);
+        A((void**)&f.s[b].sel, sizeof(uint32_t) * px);
+    }
+    if (st != PFD_OK) { frame_release(f); return st; }
+    cudaStream_t s = ctx->stream;
+    auto H2D = [&](void* d, const void* h, size_t b) {
+        if (st == PFD_OK && cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, s) != cudaSuccess) st = PFD_ECUDA;
+    };
+    H2D(f.d_centers, centers, sizeof(float2) * n_views);
+    H2D(f.d_tilekeys, tilekeys, sizeof(int2) * n_views);
+    H2D(f.d_origin, origin.data(), sizeof(int2) * n_views);
+    H2D(f.d_nb_ids, nb_ids, sizeof(int) * (size_t)n_views * max_nb);
+    H2D(f.d_nb_counts, nb_counts, sizeof(int) * n_views);
+    if (blur) {
+        // repack [V][mi_h*mi_w] into padded tiles
+        std::vector<uint8_t> tiles(ppv_tiles, 0);
+        for (int v = 0; v < n_views; ++v)
+            std::memcpy(&tiles[(size_t)v * f.tile_stride], blur + (size_t)v * mi_w * mi_h, (size_t)mi_w * mi_h);
+        H2D(f.d_blur, tiles.data(), ppv_tiles);
+        if (st == PFD_OK && cudaStreamSynchronize(s) != cudaSuccess) st = PFD_ECUDA;
+    } else if (st == PFD_OK && cudaStreamSynchronize(s) != cudaSuccess) {
+        st = PFD_ECUDA;
+    }
+    if (st != PFD_OK) {
+        cudaGetLastError();
+        frame_release(f);
+        return fail(ctx, st, "frame_create: upload failed");
+    }
+    const int id = ctx->next_id++;
+    ctx->used += f.bytes;
+    ctx->frames.emplace(id, std::move(f));
+    *frame_id = id;
+    return PFD_OK;
+}
+
+static pfd_status set_raw(pfd_ctx* ctx, int frame_id, const uint8_t* raw, int raw_pitch, bool device_src)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!raw || raw_pitch < f->W) return fail(ctx, PFD_EINVAL, "raw is NULL or pitch %d < width %d", raw_pitch, f->W);
+    DeviceGuard g(ctx->device);
+    CU(cudaMemcpy2DAsync(f->d_raw, f->W, raw, raw_pitch, f->W, f->H,
+                         device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    CU(pfd::launch_slice(f->d_raw, f->W, f->d_origin, f->V, f->mi_w, f->mi_h, f->tile_stride, f->d_gray, ctx->stream));
+    f->has_raw = true;
+    f->has_state = false;
+    return PFD_OK;
+}
+
+pfd_status pfd_frame_set_raw(pfd_ctx* ctx, int frame_id, const uint8_t* raw, int raw_pitch)
+{
+    return set_raw(ctx, frame_id, raw, raw_pitch, false);
+}
+
+pfd_status pfd_frame_set_raw_device(pfd_ctx* ctx, int frame_id, const uint8_t* raw_dev, int raw_pitch)
+{
+    return set_raw(ctx, frame_id, raw_dev, raw_pitch, true);
+}
+
+pfd_status pfd_frame_upload(pfd_ctx* ctx, int* frame_id, const uint8_t* raw, int W, int H, int raw_pitch,
+                            const float* centers, const int* tilekeys, int n_views, int mi_w, int mi_h,
+                            const int* nb_ids, const int* nb_counts, int max_nb, const uint8_t* blur)
+{
+    pfd_status st = pfd_frame_create(ctx, frame_id, W, H, centers, tilekeys, n_views, mi_w, mi_h, nb_ids, nb_counts,
+                                     max_nb, blur);
+    if (st != PFD_OK) return st;
+    st = pfd_frame_set_raw(ctx, *frame_id, raw, raw_pitch);
+    if (st != PFD_OK) {
+        const std::string msg = ctx->last_error;
+        pfd_frame_free(ctx, *frame_id);
+        *frame_id = 0;
+        ctx->last_error = msg;
+    }
+    return st;
+}
+
+pfd_status pfd_frame_free(pfd_ctx* ctx, int frame_id)
+{
+    if (!ctx) return PFD_EINVAL;
+    auto it = ctx->frames.find(frame_id);
+    if (it == ctx->frames.end()) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    DeviceGuard g(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->used -= it->second.bytes;
+    frame_release(it->second);
+    ctx->frames.erase(it);
+    return PFD_OK;
+}
+
+pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    pfd_status st = check_params(ctx, *f, params);
+    if (st != PFD_OK) return st;
+    DeviceGuard g(ctx->device);
+    const pfd::PmParams P = make_params(*f, params, seed);
+    f->cur = 0;
+    CU(pfd::launch_init(frame_dev(*f), P, f->s[0], ctx->d_err, ctx->stream));
+    f->has_state = true;
+    return PFD_OK;
+}
+
+pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed, int iter, int phase)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    pfd_status st = check_params(ctx, *f, params);
+    if (st != PFD_OK) return st;
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "sweep before pfd_pm_init");
+    if (phase != 0 && phase != 1) return fail(ctx, PFD_EINVAL, "phase must be 0 or 1");
+    if (iter < 0) return fail(ctx, PFD_EINVAL, "iter must be >= 0");
+    DeviceGuard g(ctx->device);
+    const pfd::PmParams P = make_params(*f, params, seed);
+    if (pfd::sweep_smem_bytes(P, 32, f->has_blur) > 227 * 1024)
+        return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
+    CU(pfd::launch_sweep(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, ctx->d_err, ctx->stream));
+    f->cur ^= 1;
+    return PFD_OK;
+}
+
+pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed)
+{
+    pfd_status st = pfd_pm_init(ctx, frame_id, params, seed);
+    for (int it = 0; st == PFD_OK && it < params->max_iterations; ++it)
+        for (int ph = 0; ph < 2 && st == PFD_OK; ++ph) st = pfd_pm_sweep(ctx, frame_id, params, seed, it, ph);
+    return st;
+}
+
+pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, const int* vids, const int* pxy,
+                         const float* planes, int n, float* costs)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    pfd_status st = check_params(ctx, *f, params);
+    if (st != PFD_OK) return st;
+    if (n < 0 || (n > 0 && (!vids || !pxy || !planes || !costs))) return fail(ctx, PFD_EINVAL, "ncc_costs: bad arrays");
+    if (n == 0) return PFD_OK;
+    for (int i = 0; i < n; ++i) {
+        if (vids[i] < 0 || vids[i] >= f->V) return fail(ctx, PFD_EINVAL, "hypothesis %d: view %d", i, vids[i]);
+        if (pxy[2 * i] < 0 || pxy[2 * i] >= f->mi_w || pxy[2 * i + 1] < 0 || pxy[2 * i + 1] >= f->mi_h)
+            return fail(ctx, PFD_EINVAL, "hypothesis %d: pixel outside the window", i);
+    }
+    // group by view (stable), segments of <= npb hypotheses
+    const int npb = 128;
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return vids[a] < vids[b]; });
+    std::vector<int> seg_vid, seg_start, seg_len, h_pxy(2 * (size_t)n), h_out(n);
+    std::vector<float> h_plane(4 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        const int o = order[i];
+        h_pxy[2 * i] = pxy[2 * o]; h_pxy[2 * i + 1] = pxy[2 * o + 1];
+        std::memcpy(&h_plane[4 * (size_t)i], planes + 4 * (size_t)o, 16);
+        h_out[i] = o;
+        if (i == 0 || vids[o] != vids[order[i - 1]] || seg_len.back() == npb) {
+            seg_vid.push_back(vids[o]); seg_start.push_back(i); seg_len.push_back(0);
+        }
+        seg_len.back()++;
+    }
+    const int nseg = (int)seg_vid.size();
+    DeviceGuard g(ctx->device);
+    const size_t bytes = sizeof(int) * (3 * (size_t)nseg + 3 * (size_t)n) + sizeof(float) * 4 * (size_t)n +
+                         sizeof(float) * (size_t)n * f->K + 64;
+    char* d = nullptr;
+    CU(cudaMallocAsync((void**)&d, bytes, ctx->stream));
+    int* d_segv = (int*)d;
+    int* d_segs = d_segv + nseg;
+    int* d_segl = d_segs + nseg;
+    int* d_pxy = d_segl + nseg;
+    int* d_out = d_pxy + 2 * (size_t)n;
+    float4* d_plane = (float4*)(((uintptr_t)(d_out + n) + 15) & ~(uintptr_t)15);
+    float* d_cost = (float*)(d_plane + n);
+    cudaStream_t s = ctx->stream;
+    pfd_status rc = PFD_OK;
+    auto H2D = [&](void* dd, const void* h, size_t b) {
+        if (rc == PFD_OK && cudaMemcpyAsync(dd, h, b, cudaMemcpyHostToDevice, s) != cudaSuccess) rc = PFD_ECUDA;
+    };
+    H2D(d_segv, seg_vid.data(), sizeof(int) * nseg);
+    H2D(d_segs, seg_start.data(), sizeof(int) * nseg);
+    H2D(d_segl, seg_len.data(), sizeof(int) * nseg);
+    H2D(d_pxy, h_pxy.data(), sizeof(int) * 2 * (size_t)n);
+    H2D(d_out, h_out.data(), sizeof(int) * (size_t)n);
+    H2D(d_plane, h_plane.data(), sizeof(float) * 4 * (size_t)n);
+    const pfd::PmParams P = make_params(*f, params, 0);
+    if (rc == PFD_OK &&
+        pfd::launch_ncc(frame_dev(*f), P, nseg, npb, d_segv, d_segs, d_segl, d_pxy, d_plane, d_out, d_cost,
+                        ctx->d_err, s) != cudaSuccess)
+        rc = PFD_ECUDA;
+    if (rc == PFD_OK &&
+        cudaMemcpyAsync(costs, d_cost, sizeof(float) * (size_t)n * f->K, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        rc = PFD_ECUDA;
+    cudaFreeAsync(d, s);
+    if (rc != PFD_OK) {
+        const cudaError_t e = cudaGetLastError();
+        return fail(ctx, rc, "ncc_costs: %s", cudaGetErrorString(e));
+    }
+    return check_device_error(ctx);
+}
+
+pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane, float* cost, float* disp, uint32_t* sel)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "download before PatchMatch");
+    DeviceGuard g(ctx->device);
+    const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
+    const pfd::StateDev& s = f->s[f->cur];
+    if (plane) CU(cudaMemcpyAsync(plane, s.plane, sizeof(float4) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (cost) CU(cudaMemcpyAsync(cost, s.cost, sizeof(float) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (disp) CU(cudaMemcpyAsync(disp, s.disp, sizeof(float4) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (sel) CU(cudaMemcpyAsync(sel, s.sel, sizeof(uint32_t) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_device_error(ctx);
+}
+
+}  // extern "C"

@@ -1,0 +1,369 @@
+// pm_device.cuh -- device building blocks of the micro-image PatchMatch:
+// plane geometry, hexagonal-baseline mapping, shared-memory micro-image tiles,
+// and the bilateral NCC evaluated for one plane against a chunk of neighbour
+// micro-images at once.
+//
+// Reference: MIStereo/AdaptMIPMFrame.cu:24-317,350-471, MIStereo/CudaUtil.cu:
+// 13-170,341-361,491-507, MIStereo/AdaptMIPMUtil.cu:463-501,625-649.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "canon.cuh"
+
+namespace pfd {
+
+constexpr int kMaxNb = 32;           // selected-view bitmask width (CudaUtil.cu:13-21)
+constexpr float kCostMax = 2.0f;
+
+// Per-launch constants (PatchMatchParamsLF, LFDepthInfo.h:19-46, as the Frame
+// path sets them in AdaptMIPMFrame.cpp:126-143).
+struct PmParams {
+    int W, H, ppv;          // micro-image window (mi_width_for_match) and pixels per view
+    int K;                  // neighbour-id stride (m_max_neighbors)
+    int radius, inc, ntap;  // patch radius, radius_increment, taps per patch side
+    int top_k;
+    float ss2, cc2;         // (2 sigma_s) sigma_s and (2 sigma_c) sigma_c
+    float depth_min, depth_max;
+    float base, inv_base;   // Base and 1 / max(Base, 1e-6)
+    float pert_pi;          // (float)(0.02 * pi)
+    uint32_t W_bits, H_bits;   // __float_as_uint((float)W), ... for unsigned bound tests
+    int tile_stride;        // bytes per micro-image tile in HBM (W*H rounded up to 16)
+    uint64_t seed;
+};
+
+struct FrameDev {
+    const uint8_t* gray;    // [V][tile_stride]
+    const uint8_t* blur;    // [V][tile_stride] or nullptr
+    const float2* centers;  // [V]
+    const int* nb_ids;      // [V][K]
+    const int* nb_counts;   // [V]
+    int V;
+};
+
+struct StateDev {
+    float4* plane;          // nx, ny, nz, disparity
+    float* cost;
+    float4* disp;           // d, d_real, baseline, baseline / d_real
+    uint32_t* sel;
+};
+
+// Per (reference, neighbour) pair constants of DisparityGeometricMapOperate_Hex
+// (AdaptMIPMUtil.cu:625-649) and the NCC's source step (AdaptMIPMFrame.cu:106-108).
+struct NbGeo {
+    float bx, by;           // c_ref - c_nb
+    float baseline;         // |c_nb - c_ref|
+    float dxn, dyn;         // (c_ref - c_nb) / baseline
+    float scale;            // baseline / Base
+    float stx, sty;         // (c_ref - c_nb) * inv_base
+};
+
+__device__ __forceinline__ NbGeo make_geo(float2 c0, float2 c1, const PmParams& P)
+{
+    NbGeo g;
+    const float ey = __fsub_rn(c1.y, c0.y), ex = __fsub_rn(c1.x, c0.x);
+    g.baseline = __fsqrt_rn(__fmaf_rn(ex, ex, __fmul_rn(ey, ey)));
+    g.bx = __fsub_rn(c0.x, c1.x);
+    g.by = __fsub_rn(c0.y, c1.y);
+    g.dxn = __fdiv_rn(g.bx, g.baseline);
+    g.dyn = __fdiv_rn(g.by, g.baseline);
+    g.scale = __fdiv_rn(g.baseline, P.base);
+    g.stx = __fmul_rn(g.bx, P.inv_base);
+    g.sty = __fmul_rn(g.by, P.inv_base);
+    return g;
+}
+
+// DisparityPlane, CudaUtil.cu:158-170
+__device__ __forceinline__ float3 disparity_plane(int px, int py, float4 h)
+{
+    float3 d;
+    d.x = __fdiv_rn(-h.x, h.z);
+    d.y = __fdiv_rn(-h.y, h.z);
+    float num = __fmaf_rn(h.y, (float)py, __fmul_rn(h.x, (float)px));
+    num = __fmaf_rn(h.z, h.w, num);
+    d.z = __fdiv_rn(num, h.z);
+    return d;
+}
+
+// to_disparity, CudaUtil.cu:152-156
+__device__ __forceinline__ float to_disparity(int px, int py, float3 dp)
+{
+    return __fadd_rn(__fmaf_rn(dp.y, (float)py, __fmul_rn(dp.x, (float)px)), dp.z);
+}
+
+// NormalizeVec3, CudaUtil.cu:49-56
+__device__ __forceinline__ float4 normalize3(float4 v)
+{
+    const float n2 = __fmaf_rn(v.z, v.z, __fmaf_rn(v.y, v.y, __fmul_rn(v.x, v.x)));
+    const float inv = pfd_rsqrtf(n2);
+    v.x = __fmul_rn(v.x, inv); v.y = __fmul_rn(v.y, inv); v.z = __fmul_rn(v.z, inv);
+    return v;
+}
+
+// Anchor of p in the neighbour window (DisparityGeometricMapOperate_Hex p1).
+__device__ __forceinline__ float2 geo_anchor(const NbGeo& g, int px, int py, float d)
+{
+    return make_float2(__fmaf_rn(__fmul_rn(g.dxn, d), g.scale, (float)px),
+                       __fmaf_rn(__fmul_rn(g.dyn, d), g.scale, (float)py));
+}
+
+// disparity_basline of DisparityGeometricMapOperate_Hex (d, d_real, baseline, ratio).
+__device__ __forceinline__ float4 geo_disp(const NbGeo& g, int px, int py, float d)
+{
+    const float2 a = geo_anchor(g, px, py, d);
+    const float dr2 = __fmaf_rn(g.by, __fsub_rn((float)py, a.y), __fmul_rn(g.bx, __fsub_rn((float)px, a.x)));
+    const float d_real = __fsqrt_rn(dr2);
+    const double ratio = __ddiv_rn((double)g.baseline, __dadd_rn((double)d_real, 1e-7));
+    return make_float4(d, d_real, g.baseline, __double2float_rn(ratio));
+}
+
+// GenerateRandomNormal_MIPM (AdaptMIPMUtil.cu:463-492); the rejection loop is
+// bounded at 64 pairs (probability of reaching it ~1e-43), then +z.
+__device__ __forceinline__ float4 random_normal(DrawStream& g)
+{
+    float q1 = 1.0f, q2 = 1.0f, s = 2.0f;
+    int attempts = 0;
+    while (s >= 1.0f) {
+        if (attempts++ == 64) { q1 = 0.0f; q2 = 0.0f; s = 0.0f; break; }
+        q1 = __fmaf_rn(2.0f, g.uniform(), -1.0f);
+        q2 = __fmaf_rn(2.0f, g.uniform(), -1.0f);
+        s = __fmaf_rn(q2, q2, __fmul_rn(q1, q1));
+    }
+    const float sq = __fsqrt_rn(__fsub_rn(1.0f, s));
+    float4 n = make_float4(__fmul_rn(__fmul_rn(2.0f, q1), sq), __fmul_rn(__fmul_rn(2.0f, q2), sq),
+                           __fmaf_rn(-2.0f, s, 1.0f), 0.0f);
+    return normalize3(n);
+}
+
+// GenerateRandomPlaneHypothesis_MIPM (AdaptMIPMUtil.cu:494-501)
+__device__ __forceinline__ float4 random_plane(DrawStream& g, float dmin, float dmax)
+{
+    const float depth = __fmaf_rn(g.uniform(), __fsub_rn(dmax, dmin), dmin);
+    float4 h = random_normal(g);
+    h.w = depth;
+    return h;
+}
+
+// GeneratePerturbedNormalLF (CudaUtil.cu:105-142).  The perturbed normal keeps
+// n.w (the reference leaves .w uninitialised there).
+__device__ __forceinline__ float4 perturbed_normal(int px, int py, float4 n, DrawStream& g, float pert)
+{
+    const float X0 = (float)px, X1 = (float)py, X2 = 1.0f;
+    const float norm = __fsqrt_rn(__fmaf_rn(X2, X2, __fmaf_rn(X1, X1, __fmul_rn(X0, X0))));
+    const float vx = __fdiv_rn(X0, norm), vy = __fdiv_rn(X1, norm), vz = __fdiv_rn(X2, norm);
+    const float a1 = __fmul_rn(__fsub_rn(g.uniform(), 0.5f), pert);
+    const float a2 = __fmul_rn(__fsub_rn(g.uniform(), 0.5f), pert);
+    const float a3 = __fmul_rn(__fsub_rn(g.uniform(), 0.5f), pert);
+    const float s1 = pfd_sin_small(a1), s2 = pfd_sin_small(a2), s3 = pfd_sin_small(a3);
+    const float c1 = pfd_cos_small(a1), c2 = pfd_cos_small(a2), c3 = pfd_cos_small(a3);
+    const float R0 = __fmul_rn(c2, c3);
+    const float R1 = __fmaf_rn(-c1, s3, __fmul_rn(__fmul_rn(c3, s1), s2));
+    const float R2 = __fmaf_rn(__fmul_rn(c1, c3), s2, __fmul_rn(s1, s3));
+    const float R3 = __fmul_rn(c2, s3);
+    const float R4 = __fmaf_rn(__fmul_rn(s1, s2), s3, __fmul_rn(c1, c3));
+    const float R5 = __fmaf_rn(-c3, s1, __fmul_rn(__fmul_rn(c1, s2), s3));
+    const float R6 = -s2;
+    const float R7 = __fmul_rn(c2, s1);
+    const float R8 = __fmul_rn(c1, c2);
+    float4 q;
+    q.x = __fmaf_rn(R2, n.z, __fmaf_rn(R1, n.y, __fmul_rn(R0, n.x)));
+    q.y = __fmaf_rn(R5, n.z, __fmaf_rn(R4, n.y, __fmul_rn(R3, n.x)));
+    q.z = __fmaf_rn(R8, n.z, __fmaf_rn(R7, n.y, __fmul_rn(R6, n.x)));
+    q.w = n.w;
+    const float dot = __fmaf_rn(q.z, vz, __fmaf_rn(q.y, vy, __fmul_rn(q.x, vx)));
+    if (dot >= 0.0f) q = n;
+    return normalize3(q);
+}
+
+// EncodePlaneHypothesisFromDispPlaneDevice (AdaptMIPMFrame.cu:36-53)
+__device__ __forceinline__ float4 encode_plane(int ax, int ay, float alpha, float beta, float gamma)
+{
+    float nx = -alpha, ny = -beta, nz = 1.0f;
+    const float inv = pfd_rsqrtf(__fadd_rn(__fmaf_rn(nz, nz, __fmaf_rn(ny, ny, __fmul_rn(nx, nx))), 1e-12f));
+    nx = __fmul_rn(nx, inv); ny = __fmul_rn(ny, inv); nz = __fmul_rn(nz, inv);
+    const float d = __fadd_rn(__fmaf_rn(beta, (float)ay, __fmul_rn(alpha, (float)ax)), gamma);
+    return make_float4(nx, ny, nz, d);
+}
+
+__device__ __forceinline__ float clamp_cost(float v) { return fminf(2.0f, fmaxf(0.0f, v)); }
+
+__device__ __forceinline__ float safe_denom(float v)
+{
+    if (fabsf(v) < 1e-6f) return (v >= 0.0f) ? 1e-6f : -1e-6f;
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory image of one reference micro-image and its neighbours.
+//
+// Neighbour windows are held as "row pairs": entry (y, x), x in [0, W],
+// y in [0, H+1], is (2T - T', T' - T) with T = I(y, x), T' = I(y, x+1), indices
+// clamped to the window (the texture unit's clamp addressing).  A bilinear tap
+// at texel (ix, iy) with 8-bit fractions (ax, ay) reads entries (iy, ix) and
+// (iy+1, ix): h = fma(1 + ax/256, D, E) = T + ax/256 (T' - T) exactly, because
+// texels are integers 0..255 and every intermediate fits 24 bits.
+// ---------------------------------------------------------------------------
+struct Tiles {
+    const float* R;         // [H][W] reference texels (as floats)
+    const float* RB;        // [H][W] reference blur or nullptr
+    const float2* Q;        // [K_nb][(H+2)][(W+1)] neighbour row pairs
+    const float2* QB;       // same for blur, or nullptr
+    const NbGeo* geo;       // [K_nb]
+    const int* nb_ok;       // [K_nb] neighbour id valid (>= 0)
+    const float* a_s;       // [ntap*ntap] (-sqrt(i^2+j^2)) / ss2, i outer, j inner
+    const float* a_c;       // [256] cd / cc2
+    int q_stride;           // (H+2)*(W+1) float2 per neighbour
+};
+
+// Bilateral NCC (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:73-179) of one
+// plane against neighbours k0 .. k0+KCH-1 (those < nc).  The reference-side
+// terms of each tap (disparity, texel, bilateral weight) are evaluated once and
+// shared by the KCH neighbours; each neighbour keeps its own six moment sums,
+// accumulated in the reference's tap order (x offset outer, y offset inner).
+// Output: cost[c] for c < KCH, already including the blur penalty of
+// ComputeMultiViewCostVector_Frame (AdaptMIPMFrame.cu:219-220).
+template <int KCH, bool BLUR>
+__device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int px, int py, float3 dp, float d0,
+                                          int k0, int nc, float (&cost)[KCH])
+{
+    const int W = P.W, H = P.H;
+    float stx[KCH], sty[KCH];
+    const float2* tq[KCH];
+    const float2* tqb[KCH];
+    bool ok[KCH];
+    float sr[KCH], srr[KCH], ss[KCH], sss[KCH], srs[KCH], sw[KCH], bsx[KCH], bsy[KCH];
+#pragma unroll
+    for (int c = 0; c < KCH; ++c) {
+        const int k = k0 + c;
+        bool v = (k < nc);
+        const int kk = v ? k : 0;
+        const NbGeo g = T.geo[kk];
+        v = v && T.nb_ok[kk];
+        const float2 a = geo_anchor(g, px, py, d0);
+        v = v && (__float_as_uint(a.x) < P.W_bits) && (__float_as_uint(a.y) < P.H_bits);
+        ok[c] = v;
+        stx[c] = g.stx; sty[c] = g.sty;
+        tq[c] = T.Q + (size_t)kk * T.q_stride;
+        tqb[c] = BLUR ? T.QB + (size_t)kk * T.q_stride : nullptr;
+        sr[c] = srr[c] = ss[c] = sss[c] = srs[c] = sw[c] = 0.0f;
+        bsx[c] = bsy[c] = 0.0f;
+    }
+    bool any = false;
+#pragma unroll
+    for (int c = 0; c < KCH; ++c) any |= ok[c];
+
+    if (any) {
+        const float rc = T.R[py * W + px];
+        const int r = P.radius, inc = P.inc, ntap = P.ntap;
+        int t_row = 0;
+        for (int i = -r; i <= r; i += inc, t_row += ntap) {
+            const int xr = px + i;
+            if ((unsigned)xr >= (unsigned)W) continue;
+            const float fxr = (float)xr;
+            const float axr = __fmul_rn(dp.x, fxr);
+            int t = t_row;
+            float fyr = (float)(py - r);
+            for (int j = -r; j <= r; j += inc, ++t, fyr = __fadd_rn(fyr, (float)inc)) {
+                const int yr = py + j;
+                if ((unsigned)yr >= (unsigned)H) continue;
+                const float d = __fadd_rn(__fmaf_rn(dp.y, fyr, axr), dp.z);
+                const float rv = T.R[yr * W + xr];
+                const float cd = fabsf(__fsub_rn(rv, rc));
+                const int cdi = __float_as_int(__fadd_rn(cd, 8388608.0f)) & 0xFF;
+                const float w = pfd_expf_nonpos(__fsub_rn(T.a_s[t], T.a_c[cdi]));
+                const float wr = __fmul_rn(w, rv);
+                float rb = 0.0f;
+                if (BLUR) rb = __fdiv_rn(T.RB[yr * W + xr], 255.0f);
+#pragma unroll
+                for (int c = 0; c < KCH; ++c) {
+                    if (!ok[c]) continue;
+                    const float sx = __fmaf_rn(stx[c], d, fxr);
+                    const float sy = __fmaf_rn(sty[c], d, fyr);
+                    if (__float_as_uint(sx) < P.W_bits && __float_as_uint(sy) < P.H_bits) {
+                        const int tbx = __float_as_int(__fmaf_rn(__fadd_rn(sx, 0.5f), 256.0f, kRneMagic - 128.0f));
+                        const int tby = __float_as_int(__fmaf_rn(__fadd_rn(sy, 0.5f), 256.0f, kRneMagic - 128.0f));
+                        const int ix = (tbx >> 8) - 0x4B4000, iy = (tby >> 8) - 0x4B4000;
+                        const float fx1 = __int_as_float(0x3F800000 | ((tbx & 0xFF) << 15));
+                        const float fy1 = __int_as_float(0x3F800000 | ((tby & 0xFF) << 15));
+                        const int off = iy * (W + 1) + ix;
+                        const float2 qa = tq[c][off], qb = tq[c][off + W + 1];
+                        const float h0 = __fmaf_rn(fx1, qa.y, qa.x);
+                        const float h1 = __fmaf_rn(fx1, qb.y, qb.x);
+                        const float dh = __fsub_rn(h1, h0);
+                        const float s = __fmaf_rn(fy1, dh, __fsub_rn(h0, dh));
+                        if (BLUR) {
+                            const float2 ba = tqb[c][off], bb = tqb[c][off + W + 1];
+                            const float g0 = __fmaf_rn(fx1, ba.y, ba.x);
+                            const float g1 = __fmaf_rn(fx1, bb.y, bb.x);
+                            const float dg = __fsub_rn(g1, g0);
+                            const float sb = __fmaf_rn(fy1, dg, __fsub_rn(g0, dg));
+                            bsx[c] = __fadd_rn(bsx[c], rb);
+                            bsy[c] = __fadd_rn(bsy[c], __fdiv_rn(sb, 255.0f));
+                        }
+                        const float ws = __fmul_rn(w, s);
+                        sr[c]  = __fmaf_rn(w, rv, sr[c]);
+                        srr[c] = __fmaf_rn(wr, rv, srr[c]);
+                        ss[c]  = __fmaf_rn(w, s, ss[c]);
+                        sss[c] = __fmaf_rn(ws, s, sss[c]);
+                        srs[c] = __fmaf_rn(wr, s, srs[c]);
+                        sw[c]  = __fadd_rn(sw[c], w);
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < KCH; ++c) {
+        float v = kCostMax;
+        if (ok[c] && sw[c] > 1e-6f) {
+            const float inv = __fdiv_rn(1.0f, sw[c]);
+            const float m_r = __fmul_rn(sr[c], inv), m_rr = __fmul_rn(srr[c], inv);
+            const float m_s = __fmul_rn(ss[c], inv), m_ss = __fmul_rn(sss[c], inv);
+            const float m_rs = __fmul_rn(srs[c], inv);
+            const float var_r = __fmaf_rn(-m_r, m_r, m_rr);
+            const float var_s = __fmaf_rn(-m_s, m_s, m_ss);
+            if (!(var_r < 1e-5f || var_s < 1e-5f)) {
+                const float cov = __fmaf_rn(-m_r, m_s, m_rs);
+                const float vv = __fsqrt_rn(__fmul_rn(var_r, var_s));
+                v = clamp_cost(__fsub_rn(1.0f, __fdiv_rn(cov, vv)));
+            }
+        }
+        if (BLUR) {
+            const float tb = __fsub_rn(bsx[c], bsy[c]);
+            const float bw = pfd_expf(__fmul_rn(__fmul_rn(-0.007368f, tb), tb));
+            v = clamp_cost(__fmaf_rn(2.0f, __fsub_rn(1.0f, bw), v));
+        }
+        cost[c] = v;
+    }
+}
+
+// Cost of plane h at pixel p against every neighbour k < nc, in order; sink(k, c)
+// receives each cost (ComputeMultiViewCostVector_Frame).
+template <int KCH, bool BLUR, class Sink>
+__device__ __forceinline__ void cost_vector(const Tiles& T, const PmParams& P, int px, int py, float4 h, int nc, Sink&& sink)
+{
+    const float3 dp = disparity_plane(px, py, h);
+    const float d0 = to_disparity(px, py, dp);
+    for (int k0 = 0; k0 < nc; k0 += KCH) {
+        float c[KCH];
+        ncc_chunk<KCH, BLUR>(T, P, px, py, dp, d0, k0, nc, c);
+#pragma unroll
+        for (int j = 0; j < KCH; ++j)
+            if (k0 + j < nc) sink(k0 + j, c[j]);
+    }
+}
+
+// ComputeWeightedCost_Frame (AdaptMIPMFrame.cu:284-317), streamed: call add(k,
+// c) for k = 0..nc-1 in order, then result().
+struct WeightedCost {
+    float norm, total, min_cost;
+    int min_idx;
+    __device__ __forceinline__ WeightedCost() : norm(0.0f), total(0.0f), min_cost(2.0f), min_idx(-1) {}
+    __device__ __forceinline__ void add(int k, float c, float w)
+    {
+        if (w > 0.0f) { norm = __fadd_rn(norm, w); total = __fmaf_rn(w, c, total); }
+        if (c < min_cost) { min_cost = c; min_idx = k; }
+    }
+    __device__ __forceinline__ float result() const { return (norm <= 1e-6f) ? 2.0f : __fdiv_rn(total, norm); }
+};
+
+}  // namespace pfd

@@ -1,0 +1,22 @@
+// pm_kernels.h -- launchers of the PatchMatch kernels (pm_kernels.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "pm_device.cuh"
+
+// Device-side error flags, OR-ed into the context's error word.
+#define PFD_DEVERR_TMA_TIMEOUT 0x1
+
+namespace pfd {
+
+cudaError_t launch_slice(const uint8_t* raw, int raw_pitch, const int2* origin, int V, int W, int H,
+                         int tile_stride, uint8_t* tiles, cudaStream_t st);
+cudaError_t launch_init(const FrameDev& F, const PmParams& P, const StateDev& out, int* err, cudaStream_t st);
+cudaError_t launch_sweep(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
+                         int iter, int phase, int* err, cudaStream_t st);
+cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, const int* seg_vid,
+                       const int* seg_start, const int* seg_len, const int* hyp_pxy, const float4* hyp_plane,
+                       const int* hyp_out, float* costs, int* err, cudaStream_t st);
+int sweep_smem_bytes(const PmParams& P, int npb, bool blur);
+
+}  // namespace pfd

@@ -1,0 +1,60 @@
+"""Canonical arithmetic of the oracle (CPU): Philox known answers, exp accuracy,
+uniform draws, texture emulation."""
+import json
+import math
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_philox_known_answers(oracle):
+    # Published Philox4x32-10 known-answer vectors (Random123 distribution, kat_vectors).
+    with open(os.path.join(GOLDEN, "philox4x32_10_kat.json")) as f:
+        kat = json.load(f)
+    for case in kat:
+        ctr = [int(x, 16) for x in case["ctr"]]
+        key = [int(x, 16) for x in case["key"]]
+        want = [int(x, 16) for x in case["out"]]
+        assert oracle.philox(ctr, key) == want
+
+
+def test_expf_within_two_ulp(oracle):
+    rs = np.random.RandomState(0)
+    xs = np.concatenate([np.linspace(-103.9, 88.7, 20001, dtype=np.float32),
+                         -np.abs(rs.randn(5000).astype(np.float32)) * 3,
+                         np.float32([0.0, -0.0, -1e-30, 1e-30, -0.6931472, 0.6931472])])
+    worst = 0.0
+    for x in xs:
+        y = oracle.expf(float(x))
+        t = math.exp(float(x))
+        ulp = float(np.spacing(np.float32(t))) if t > 1.2e-38 else 2.0 ** -149
+        worst = max(worst, abs(y - t) / ulp)
+    assert worst <= 2.0
+    assert oracle.expf(-200.0) == 0.0
+    assert oracle.expf(0.0) == 1.0
+
+
+def test_uniform_range_and_stream(oracle):
+    vals = [oracle.uniform(1234, 3, 77, n) for n in range(64)]
+    assert all(0.0 < v <= 1.0 for v in vals)
+    assert len(set(vals)) > 60
+    # draws are a pure function of (seed, sweep, pixel, n)
+    assert oracle.uniform(1234, 3, 77, 5) == vals[5]
+    assert oracle.uniform(1235, 3, 77, 5) != vals[5]
+
+
+def test_tex_fetch_exact_on_texels_and_bilinear(oracle):
+    rs = np.random.RandomState(1)
+    img = rs.randint(0, 256, size=(16, 16)).astype(np.float32)
+    for _ in range(200):
+        x, y = rs.randint(0, 16), rs.randint(0, 16)
+        assert oracle.tex_fetch(img, float(x), float(y)) == img[y, x]
+    # a quantised coordinate gives the exact bilinear blend with 8-bit weights
+    x, y = 3.25, 7.75
+    a, b = 0.25, 0.75
+    want = (1 - a) * (1 - b) * img[7, 3] + a * (1 - b) * img[7, 4] + (1 - a) * b * img[8, 3] + a * b * img[8, 4]
+    assert oracle.tex_fetch(img, x, y) == np.float32(want)
+    # clamp at the right/bottom edge (wrap is unsupported for unnormalised coordinates)
+    assert oracle.tex_fetch(img, 15.5, 15.5) == img[15, 15]
