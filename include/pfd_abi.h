@@ -140,6 +140,19 @@ pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params
 pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane /*[.][4]*/, float* cost,
                         float* disp /*[.][4]*/, uint32_t* sel);
 
+/* ---- measurement --------------------------------------------------------
+ * No counterpart in the reference (it has no timers or counters on this path,
+ * see its Util/Logger only).  Tap counting switches the PatchMatch kernels to
+ * a variant that also counts in-bounds NCC taps (reference and source sample
+ * both inside their windows): the algorithmic unit of the roofline.  Timed
+ * runs leave it off. */
+pfd_status pfd_set_tap_counting(pfd_ctx* ctx, int enable);
+/* Reads and clears the tap counter (synchronises the stream). */
+pfd_status pfd_read_tap_count(pfd_ctx* ctx, unsigned long long* taps);
+/* Measured FP32 fused multiply-add throughput of the device, TFLOP/s
+ * (independent FFMA chains on every SM; best of three launches). */
+pfd_status pfd_fp32_fma_rate(pfd_ctx* ctx, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -691,22 +691,28 @@ long long orc_count_taps(const orc_frame* f, const orc_params* p, const int* vid
     return taps;
 }
 
-int orc_pm_init(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int nthreads)
+int orc_pm_init_views(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int v0, int v1,
+                      int nthreads)
 {
     if (!f || !p || f->max_nb > MAX_NB) return -1;
-    const int V = f->n_views, W = f->mi_w, H = f->mi_h;
-    const long total = (long)V * W * H;
+    const int W = f->mi_w, H = f->mi_h;
+    const long t0 = (long)v0 * W * H, t1 = (long)v1 * W * H;
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
 #endif
-    for (long t = 0; t < total; ++t) {
+    for (long t = t0; t < t1; ++t) {
         const int vid = (int)(t / ((long)W * H));
         const int rem = (int)(t % ((long)W * H));
         init_pixel(f, p, seed, vid, rem % W, rem / W, out);
     }
     (void)nthreads;
     return 0;
+}
+
+int orc_pm_init(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int nthreads)
+{
+    return orc_pm_init_views(f, p, seed, out, 0, f->n_views, nthreads);
 }
 
 int orc_pm_sweep_views(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,

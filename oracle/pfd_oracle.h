@@ -75,6 +75,10 @@ double orc_ncc_fp64(const orc_frame* f, const orc_params* p, int vid, int k, int
 /* RandomInitializationForFrame (AdaptMIPMFrame.cu:474-518) over all pixels. */
 int orc_pm_init(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int nthreads);
 
+/* Same, restricted to views [v0, v1) (the bounded CPU-baseline sample). */
+int orc_pm_init_views(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int v0, int v1,
+                      int nthreads);
+
 /* One CheckerboardUpdateFrame launch (AdaptMIPMFrame.cu:520-947): next <- update(prev). */
 int orc_pm_sweep(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
                  const orc_state* prev, orc_state* next, int nthreads);

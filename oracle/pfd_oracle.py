@@ -58,6 +58,7 @@ def lib() -> ctypes.CDLL:
         L.orc_ncc_fp64.argtypes = [FP, PP, _I, _I, _I, _I, _P]
         L.orc_ncc_fp64.restype = ctypes.c_double
         L.orc_pm_init.argtypes = [FP, PP, ctypes.c_uint64, SP, _I]
+        L.orc_pm_init_views.argtypes = [FP, PP, ctypes.c_uint64, SP, _I, _I, _I]
         L.orc_pm_sweep.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I]
         L.orc_pm_sweep_views.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I, _I, _I]
         L.orc_patchmatch.argtypes = [FP, PP, ctypes.c_uint64, SP, _I]
@@ -129,10 +130,15 @@ class Oracle:
         p = self.params(params)
         return float(lib().orc_ncc_fp64(ctypes.byref(self.f), ctypes.byref(p), vid, k, px, py, _p(pl)))
 
-    def init(self, params, seed, nthreads=0):
+    def init(self, params, seed, nthreads=0, views=None):
         arr, st = self.new_state()
         p = self.params(params)
-        assert lib().orc_pm_init(ctypes.byref(self.f), ctypes.byref(p), seed, ctypes.byref(st), nthreads) == 0
+        if views is None:
+            rc = lib().orc_pm_init(ctypes.byref(self.f), ctypes.byref(p), seed, ctypes.byref(st), nthreads)
+        else:
+            rc = lib().orc_pm_init_views(ctypes.byref(self.f), ctypes.byref(p), seed, ctypes.byref(st), views[0],
+                                         views[1], nthreads)
+        assert rc == 0
         return arr
 
     def sweep(self, params, seed, it, phase, prev, nthreads=0, views=None):

@@ -92,6 +92,9 @@ def lib() -> ctypes.CDLL:
             "pfd_ncc_costs": [_P, _I, ctypes.POINTER(PmParamsC), _P, _P, _P, _I, _P],
             "pfd_download": [_P, _I, _P, _P, _P, _P],
             "pfd_neighbors_by_baseline": [_P, _P, _I, _F, _I, _I, _P, _P],
+            "pfd_set_tap_counting": [_P, _I],
+            "pfd_read_tap_count": [_P, ctypes.POINTER(ctypes.c_ulonglong)],
+            "pfd_fp32_fma_rate": [_P, ctypes.POINTER(ctypes.c_double)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -222,6 +225,19 @@ class Context:
         self._check(self._L.pfd_ncc_costs(self._h, fid, ctypes.byref(p), _ptr(v), _ptr(xy), _ptr(pl), v.shape[0],
                                           _ptr(out)), "pfd_ncc_costs")
         return out
+
+    def set_tap_counting(self, on: bool) -> None:
+        self._check(self._L.pfd_set_tap_counting(self._h, 1 if on else 0), "pfd_set_tap_counting")
+
+    def read_tap_count(self) -> int:
+        v = ctypes.c_ulonglong()
+        self._check(self._L.pfd_read_tap_count(self._h, ctypes.byref(v)), "pfd_read_tap_count")
+        return v.value
+
+    def fp32_fma_rate(self) -> float:
+        v = ctypes.c_double()
+        self._check(self._L.pfd_fp32_fma_rate(self._h, ctypes.byref(v)), "pfd_fp32_fma_rate")
+        return v.value
 
     def download(self, fid: int):
         f = self._frames[fid]

@@ -45,6 +45,8 @@ struct pfd_ctx {
     int next_id = 1;
     std::map<int, Frame> frames;
     int* d_err = nullptr;
+    unsigned long long* d_taps = nullptr;   // tap counter of calibration runs
+    bool counting = false;
     std::string last_error;
 };
 
@@ -146,6 +148,7 @@ pfd::PmParams make_params(const Frame& f, const pfd_pm_params* p, uint64_t seed)
     std::memcpy(&P.H_bits, &fh, 4);
     P.tile_stride = f.tile_stride;
     P.seed = seed;
+    P.tap_counter = nullptr;
     return P;
 }
 
@@ -194,10 +197,13 @@ pfd_status pfd_create(pfd_ctx** out, int device, size_t hbm_budget_bytes)
     DeviceGuard g(device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess ||
-        cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess) {
+        cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_taps, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMemset(ctx->d_taps, 0, sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
         if (ctx->d_err) cudaFree(ctx->d_err);
+        if (ctx->d_taps) cudaFree(ctx->d_taps);
         delete ctx;
         return PFD_ECUDA;
     }
@@ -213,8 +219,37 @@ void pfd_destroy(pfd_ctx* ctx)
     for (auto& kv : ctx->frames) frame_release(kv.second);
     ctx->frames.clear();
     cudaFree(ctx->d_err);
+    cudaFree(ctx->d_taps);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
+}
+
+pfd_status pfd_set_tap_counting(pfd_ctx* ctx, int enable)
+{
+    if (!ctx) return PFD_EINVAL;
+    ctx->counting = enable != 0;
+    return PFD_OK;
+}
+
+pfd_status pfd_read_tap_count(pfd_ctx* ctx, unsigned long long* taps)
+{
+    if (!ctx || !taps) return PFD_EINVAL;
+    DeviceGuard g(ctx->device);
+    CU(cudaMemcpyAsync(taps, ctx->d_taps, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemsetAsync(ctx->d_taps, 0, sizeof(unsigned long long), ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return PFD_OK;
+}
+
+pfd_status pfd_fp32_fma_rate(pfd_ctx* ctx, double* tflops)
+{
+    if (!ctx || !tflops) return PFD_EINVAL;
+    DeviceGuard g(ctx->device);
+    float ms = 0.0f;
+    double flops = 0.0;
+    CU(pfd::measure_fma_rate(ctx->stream, &ms, &flops));
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return PFD_OK;
 }
 
 const char* pfd_last_error(pfd_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
@@ -238,8 +273,8 @@ pfd_status pfd_frame_create(pfd_ctx* ctx, int* frame_id, int W, int H, const flo
     *frame_id = 0;
     if (W <= 0 || H <= 0 || n_views <= 0 || !centers || !tilekeys || !nb_ids || !nb_counts)
         return fail(ctx, PFD_EINVAL, "frame_create: bad sizes or NULL arrays");
-    if (mi_w < 2 || mi_h < 2 || mi_w > 64 || mi_h > 64)
-        return fail(ctx, PFD_EINVAL, "micro-image window %dx%d outside [2, 64]", mi_w, mi_h);
+    if (mi_w < 2 || mi_h < 2 || mi_w > 32 || mi_h > 32)
+        return fail(ctx, PFD_EINVAL, "micro-image window %dx%d outside [2, 32]", mi_w, mi_h);
     if (max_nb < 1 || max_nb > pfd::kMaxNb)
         return fail(ctx, PFD_EINVAL, "max_nb %d outside [1, 32] (selected-view masks are 32 bits)", max_nb);
     Frame f;
@@ -382,7 +417,8 @@ pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, 
     pfd_status st = check_params(ctx, *f, params);
     if (st != PFD_OK) return st;
     DeviceGuard g(ctx->device);
-    const pfd::PmParams P = make_params(*f, params, seed);
+    pfd::PmParams P = make_params(*f, params, seed);
+    if (ctx->counting) P.tap_counter = ctx->d_taps;
     f->cur = 0;
     CU(pfd::launch_init(frame_dev(*f), P, f->s[0], ctx->d_err, ctx->stream));
     f->has_state = true;
@@ -400,7 +436,8 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
     if (phase != 0 && phase != 1) return fail(ctx, PFD_EINVAL, "phase must be 0 or 1");
     if (iter < 0) return fail(ctx, PFD_EINVAL, "iter must be >= 0");
     DeviceGuard g(ctx->device);
-    const pfd::PmParams P = make_params(*f, params, seed);
+    pfd::PmParams P = make_params(*f, params, seed);
+    if (ctx->counting) P.tap_counter = ctx->d_taps;
     if (pfd::sweep_smem_bytes(P, 32, f->has_blur) > 227 * 1024)
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
     CU(pfd::launch_sweep(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, ctx->d_err, ctx->stream));

@@ -29,6 +29,7 @@ struct PmParams {
     uint32_t W_bits, H_bits;   // __float_as_uint((float)W), ... for unsigned bound tests
     int tile_stride;        // bytes per micro-image tile in HBM (W*H rounded up to 16)
     uint64_t seed;
+    unsigned long long* tap_counter;   // calibration runs only: in-bounds NCC taps evaluated
 };
 
 struct FrameDev {
@@ -195,118 +196,139 @@ __device__ __forceinline__ float safe_denom(float v)
 // ---------------------------------------------------------------------------
 // Shared-memory image of one reference micro-image and its neighbours.
 //
-// Neighbour windows are held as "row pairs": entry (y, x), x in [0, W],
-// y in [0, H+1], is (2T - T', T' - T) with T = I(y, x), T' = I(y, x+1), indices
-// clamped to the window (the texture unit's clamp addressing).  A bilinear tap
-// at texel (ix, iy) with 8-bit fractions (ax, ay) reads entries (iy, ix) and
-// (iy+1, ix): h = fma(1 + ax/256, D, E) = T + ax/256 (T' - T) exactly, because
-// texels are integers 0..255 and every intermediate fits 24 bits.
+// Neighbour windows are held as integer "row pairs": entry (y, x), y in
+// [0, H+1], x in [0, S) with S even and >= W+1, is (T, T' - T) with
+// T = I(y, x), T' = I(y, x+1), indices clamped to the window.  A fetch at
+// texel (ix, iy) reads entries (iy, ix) and (iy+1, ix), which hold the four
+// texels of the bilinear footprint.
+//
+// The fetch reproduces the texture unit's linear filter as measured on B200
+// for integer texels (see the oracle's canon_tex_fetch): coordinates rounded
+// half up to 1/256 (one FFMA rounding toward -inf against 2^23 - 127.5), and
+// weights w11 = (a b + 128) >> 8, w10 = a - w11, w01 = b - w11,
+// w00 = 256 - a - b + w11, i.e.
+//   256 s = 256 T00 + a (T10-T00) + b (T01-T00) + w11 (T11-T10-T01+T00),
+// an integer below 2^16 that is turned into a float exactly.
 // ---------------------------------------------------------------------------
 struct Tiles {
     const float* R;         // [H][W] reference texels (as floats)
     const float* RB;        // [H][W] reference blur or nullptr
-    const float2* Q;        // [K_nb][(H+2)][(W+1)] neighbour row pairs
-    const float2* QB;       // same for blur, or nullptr
-    const NbGeo* geo;       // [K_nb]
-    const int* nb_ok;       // [K_nb] neighbour id valid (>= 0)
+    uint32_t q_addr;        // shared address of neighbour row pairs, [K][H+2][S] int2
+    uint32_t qb_addr;       // same for blur (0 if none)
+    int q_stride;           // S, row stride in entries
+    int q_bytes;            // bytes per neighbour tile
+    const NbGeo* geo;       // [K]
+    const int* nb_ok;       // [K] neighbour id valid (>= 0)
     const float* a_s;       // [ntap*ntap] (-sqrt(i^2+j^2)) / ss2, i outer, j inner
     const float* a_c;       // [256] cd / cc2
-    int q_stride;           // (H+2)*(W+1) float2 per neighbour
 };
 
-// Bilateral NCC (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:73-179) of one
-// plane against neighbours k0 .. k0+KCH-1 (those < nc).  The reference-side
-// terms of each tap (disparity, texel, bilateral weight) are evaluated once and
-// shared by the KCH neighbours; each neighbour keeps its own six moment sums,
-// accumulated in the reference's tap order (x offset outer, y offset inner).
-// Output: cost[c] for c < KCH, already including the blur penalty of
-// ComputeMultiViewCostVector_Frame (AdaptMIPMFrame.cu:219-220).
-template <int KCH, bool BLUR>
-__device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int px, int py, float3 dp, float d0,
-                                          int k0, int nc, float (&cost)[KCH])
+constexpr uint32_t kFullMask = 0xffffffffu;
+
+__device__ __forceinline__ int2 lds_int2(uint32_t addr)
 {
-    const int W = P.W, H = P.H;
+    int2 v;
+    asm volatile("ld.shared.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(addr));
+    return v;
+}
+
+// 2^23 + floor(256 (s + 0.5) - 127.5), as float bits: the texel index in the
+// upper bits, the 8-bit fraction in the low byte.
+__device__ __forceinline__ int tex_coord_bits(float s)
+{
+    return __float_as_int(__fmaf_rd(__fadd_rn(s, 0.5f), 256.0f, 8388480.5f));
+}
+
+__device__ __forceinline__ float tex_blend(int tbx, int tby, int2 p0, int2 p1)
+{
+    const int a = tbx & 0xFF, b = tby & 0xFF;
+    const int w11 = (a * b + 128) >> 8;
+    const int s256 = (p0.x << 8) + a * p0.y + b * (p1.x - p0.x) + w11 * (p1.y - p0.y);
+    return __fsub_rn(__int_as_float(s256 | 0x47000000), 32768.0f);
+}
+
+// Bilateral NCC (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:73-179) of each
+// lane's plane against the neighbours ks[0..nks) (warp-uniform list).  The
+// reference-side work of a tap (disparity, texel, bilateral weight) is done
+// once and shared by the chunk; every neighbour keeps its own six moment sums
+// in the reference's tap order (x offset outer, y offset inner).  The body is
+// branch-free: a tap that falls outside either window contributes exact
+// zeros (fma(0, s, acc) == acc), so the sums equal the reference's skipping.
+// okmask: per lane, bit k set when neighbour k's anchor lies in the window.
+template <int KCH, bool BLUR, bool COUNT>
+__device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int px, int py, float3 dp,
+                                          const int (&ks)[16], int nks, uint32_t okmask, float (&cost)[KCH],
+                                          unsigned& ntaps)
+{
+    const int W = P.W, H = P.H, S = T.q_stride;
+    const uint32_t fold = (uint32_t)0x4B0000u * (uint32_t)(S + 1) * 8u;
     float stx[KCH], sty[KCH];
-    const float2* tq[KCH];
-    const float2* tqb[KCH];
-    bool ok[KCH];
+    uint32_t base[KCH], bbase[KCH];
+    bool okc[KCH];
     float sr[KCH], srr[KCH], ss[KCH], sss[KCH], srs[KCH], sw[KCH], bsx[KCH], bsy[KCH];
 #pragma unroll
     for (int c = 0; c < KCH; ++c) {
-        const int k = k0 + c;
-        bool v = (k < nc);
-        const int kk = v ? k : 0;
-        const NbGeo g = T.geo[kk];
-        v = v && T.nb_ok[kk];
-        const float2 a = geo_anchor(g, px, py, d0);
-        v = v && (__float_as_uint(a.x) < P.W_bits) && (__float_as_uint(a.y) < P.H_bits);
-        ok[c] = v;
-        stx[c] = g.stx; sty[c] = g.sty;
-        tq[c] = T.Q + (size_t)kk * T.q_stride;
-        tqb[c] = BLUR ? T.QB + (size_t)kk * T.q_stride : nullptr;
+        const int k = (c < nks) ? ks[c] : ks[0];
+        okc[c] = (c < nks) && ((okmask >> k) & 1u);
+        stx[c] = T.geo[k].stx;
+        sty[c] = T.geo[k].sty;
+        base[c] = T.q_addr + (uint32_t)(k * T.q_bytes) - fold;
+        bbase[c] = BLUR ? T.qb_addr + (uint32_t)(k * T.q_bytes) - fold : 0u;
         sr[c] = srr[c] = ss[c] = sss[c] = srs[c] = sw[c] = 0.0f;
         bsx[c] = bsy[c] = 0.0f;
     }
-    bool any = false;
+    const float rc = T.R[py * W + px];
+    const int r = P.radius, inc = P.inc, ntap = P.ntap;
+    int t_row = 0;
+    for (int i = -r; i <= r; i += inc, t_row += ntap) {
+        const int xr = px + i;
+        const bool rowok = (unsigned)xr < (unsigned)W;
+        if (!__any_sync(kFullMask, rowok)) continue;
+        const int xrc = min(max(xr, 0), W - 1);
+        const float fxr = (float)xr;
+        const float axr = __fmul_rn(dp.x, fxr);
+        int t = t_row;
+        float fyr = (float)(py - r);
+        for (int j = -r; j <= r; j += inc, ++t, fyr = __fadd_rn(fyr, (float)inc)) {
+            const int yr = py + j;
+            const bool refok = rowok && ((unsigned)yr < (unsigned)H);
+            if (!__any_sync(kFullMask, refok)) continue;
+            const int yrc = min(max(yr, 0), H - 1);
+            const float rv = T.R[yrc * W + xrc];
+            const float cd = fabsf(__fsub_rn(rv, rc));
+            const int cdi = __float_as_int(__fadd_rn(cd, 8388608.0f)) & 0xFF;
+            const float w = refok ? pfd_expf_nonpos(__fsub_rn(T.a_s[t], T.a_c[cdi])) : 0.0f;
+            const float wr = __fmul_rn(w, rv);
+            const float d = __fadd_rn(__fmaf_rn(dp.y, fyr, axr), dp.z);
+            float rb = 0.0f;
+            if (BLUR) rb = __fdiv_rn(T.RB[yrc * W + xrc], 255.0f);
 #pragma unroll
-    for (int c = 0; c < KCH; ++c) any |= ok[c];
-
-    if (any) {
-        const float rc = T.R[py * W + px];
-        const int r = P.radius, inc = P.inc, ntap = P.ntap;
-        int t_row = 0;
-        for (int i = -r; i <= r; i += inc, t_row += ntap) {
-            const int xr = px + i;
-            if ((unsigned)xr >= (unsigned)W) continue;
-            const float fxr = (float)xr;
-            const float axr = __fmul_rn(dp.x, fxr);
-            int t = t_row;
-            float fyr = (float)(py - r);
-            for (int j = -r; j <= r; j += inc, ++t, fyr = __fadd_rn(fyr, (float)inc)) {
-                const int yr = py + j;
-                if ((unsigned)yr >= (unsigned)H) continue;
-                const float d = __fadd_rn(__fmaf_rn(dp.y, fyr, axr), dp.z);
-                const float rv = T.R[yr * W + xr];
-                const float cd = fabsf(__fsub_rn(rv, rc));
-                const int cdi = __float_as_int(__fadd_rn(cd, 8388608.0f)) & 0xFF;
-                const float w = pfd_expf_nonpos(__fsub_rn(T.a_s[t], T.a_c[cdi]));
-                const float wr = __fmul_rn(w, rv);
-                float rb = 0.0f;
-                if (BLUR) rb = __fdiv_rn(T.RB[yr * W + xr], 255.0f);
-#pragma unroll
-                for (int c = 0; c < KCH; ++c) {
-                    if (!ok[c]) continue;
-                    const float sx = __fmaf_rn(stx[c], d, fxr);
-                    const float sy = __fmaf_rn(sty[c], d, fyr);
-                    if (__float_as_uint(sx) < P.W_bits && __float_as_uint(sy) < P.H_bits) {
-                        const int tbx = __float_as_int(__fmaf_rn(__fadd_rn(sx, 0.5f), 256.0f, kRneMagic - 128.0f));
-                        const int tby = __float_as_int(__fmaf_rn(__fadd_rn(sy, 0.5f), 256.0f, kRneMagic - 128.0f));
-                        const int ix = (tbx >> 8) - 0x4B4000, iy = (tby >> 8) - 0x4B4000;
-                        const float fx1 = __int_as_float(0x3F800000 | ((tbx & 0xFF) << 15));
-                        const float fy1 = __int_as_float(0x3F800000 | ((tby & 0xFF) << 15));
-                        const int off = iy * (W + 1) + ix;
-                        const float2 qa = tq[c][off], qb = tq[c][off + W + 1];
-                        const float h0 = __fmaf_rn(fx1, qa.y, qa.x);
-                        const float h1 = __fmaf_rn(fx1, qb.y, qb.x);
-                        const float dh = __fsub_rn(h1, h0);
-                        const float s = __fmaf_rn(fy1, dh, __fsub_rn(h0, dh));
-                        if (BLUR) {
-                            const float2 ba = tqb[c][off], bb = tqb[c][off + W + 1];
-                            const float g0 = __fmaf_rn(fx1, ba.y, ba.x);
-                            const float g1 = __fmaf_rn(fx1, bb.y, bb.x);
-                            const float dg = __fsub_rn(g1, g0);
-                            const float sb = __fmaf_rn(fy1, dg, __fsub_rn(g0, dg));
-                            bsx[c] = __fadd_rn(bsx[c], rb);
-                            bsy[c] = __fadd_rn(bsy[c], __fdiv_rn(sb, 255.0f));
-                        }
-                        const float ws = __fmul_rn(w, s);
-                        sr[c]  = __fmaf_rn(w, rv, sr[c]);
-                        srr[c] = __fmaf_rn(wr, rv, srr[c]);
-                        ss[c]  = __fmaf_rn(w, s, ss[c]);
-                        sss[c] = __fmaf_rn(ws, s, sss[c]);
-                        srs[c] = __fmaf_rn(wr, s, srs[c]);
-                        sw[c]  = __fadd_rn(sw[c], w);
-                    }
+            for (int c = 0; c < KCH; ++c) {
+                const float sx = __fmaf_rn(stx[c], d, fxr);
+                const float sy = __fmaf_rn(sty[c], d, fyr);
+                const bool v = okc[c] && (__float_as_uint(sx) < P.W_bits) && (__float_as_uint(sy) < P.H_bits);
+                if (COUNT) ntaps += (v && refok) ? 1u : 0u;
+                const int tbx = tex_coord_bits(sx), tby = tex_coord_bits(sy);
+                const uint32_t rel = (uint32_t)(((tby >> 8) * S + (tbx >> 8)) << 3);
+                const uint32_t addr = v ? base[c] + rel : T.q_addr;
+                const int2 p0 = lds_int2(addr), p1 = lds_int2(addr + (uint32_t)S * 8u);
+                const float s = tex_blend(tbx, tby, p0, p1);
+                const float wv = v ? w : 0.0f;
+                const float wrv = v ? wr : 0.0f;
+                const float ws = __fmul_rn(wv, s);
+                sr[c]  = __fmaf_rn(wv, rv, sr[c]);
+                srr[c] = __fmaf_rn(wrv, rv, srr[c]);
+                ss[c]  = __fmaf_rn(wv, s, ss[c]);
+                sss[c] = __fmaf_rn(ws, s, sss[c]);
+                srs[c] = __fmaf_rn(wrv, s, srs[c]);
+                sw[c]  = __fadd_rn(sw[c], wv);
+                if (BLUR) {
+                    const uint32_t baddr = v ? bbase[c] + rel : T.qb_addr;
+                    const int2 b0 = lds_int2(baddr), b1 = lds_int2(baddr + (uint32_t)S * 8u);
+                    const float sb = tex_blend(tbx, tby, b0, b1);
+                    const bool vr = v && refok;       // blur sums skip taps outside either window
+                    bsx[c] = __fadd_rn(bsx[c], vr ? rb : 0.0f);
+                    bsy[c] = __fadd_rn(bsy[c], vr ? __fdiv_rn(sb, 255.0f) : 0.0f);
                 }
             }
         }
@@ -314,7 +336,7 @@ __device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int
 #pragma unroll
     for (int c = 0; c < KCH; ++c) {
         float v = kCostMax;
-        if (ok[c] && sw[c] > 1e-6f) {
+        if (okc[c] && sw[c] > 1e-6f) {
             const float inv = __fdiv_rn(1.0f, sw[c]);
             const float m_r = __fmul_rn(sr[c], inv), m_rr = __fmul_rn(srr[c], inv);
             const float m_s = __fmul_rn(ss[c], inv), m_ss = __fmul_rn(sss[c], inv);
@@ -336,19 +358,61 @@ __device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int
     }
 }
 
-// Cost of plane h at pixel p against every neighbour k < nc, in order; sink(k, c)
-// receives each cost (ComputeMultiViewCostVector_Frame).
-template <int KCH, bool BLUR, class Sink>
-__device__ __forceinline__ void cost_vector(const Tiles& T, const PmParams& P, int px, int py, float4 h, int nc, Sink&& sink)
+// ComputeMultiViewCostVector_Frame (AdaptMIPMFrame.cu:181-225) for the plane of
+// every lane of the warp; must be called by all 32 lanes together.  Lanes with
+// active == false only keep the warp company.  Cost of neighbour k (k < nc)
+// goes to out[k * out_stride]; neighbours whose anchor leaves the window for
+// every lane are not evaluated (their cost is 2, as the reference returns).
+template <bool BLUR, bool COUNT>
+__device__ __noinline__ void cost_vector(const Tiles& T, const PmParams& P, int px, int py, bool active,
+                                            float4 h, int nc, float* out, int out_stride)
 {
+    if (!active) h = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
     const float3 dp = disparity_plane(px, py, h);
     const float d0 = to_disparity(px, py, dp);
-    for (int k0 = 0; k0 < nc; k0 += KCH) {
-        float c[KCH];
-        ncc_chunk<KCH, BLUR>(T, P, px, py, dp, d0, k0, nc, c);
+    uint32_t okmask = 0;
+    for (int k = 0; k < nc; ++k) {
+        const float2 a = geo_anchor(T.geo[k], px, py, d0);
+        const bool ok = active && T.nb_ok[k] && (__float_as_uint(a.x) < P.W_bits) && (__float_as_uint(a.y) < P.H_bits);
+        okmask |= ok ? (1u << k) : 0u;
+    }
+    uint32_t todo = __reduce_or_sync(kFullMask, okmask);
+    unsigned ntaps = 0;
+    for (int k = 0; k < nc; ++k)
+        if (!((todo >> k) & 1u)) out[k * out_stride] = kCostMax;
+    while (todo) {
+        int ks[16];
+        int nks = 0;
 #pragma unroll
-        for (int j = 0; j < KCH; ++j)
-            if (k0 + j < nc) sink(k0 + j, c[j]);
+        for (int c = 0; c < 16; ++c) {
+            ks[c] = todo ? (__ffs(todo) - 1) : 0;
+            if (todo) { ++nks; todo &= todo - 1; }
+        }
+        if (nks > 12) {
+            float c16[16];
+            ncc_chunk<16, BLUR, COUNT>(T, P, px, py, dp, ks, nks, okmask, c16, ntaps);
+#pragma unroll
+            for (int c = 0; c < 16; ++c) if (c < nks) out[ks[c] * out_stride] = c16[c];
+        } else if (nks > 8) {
+            float c12[12];
+            ncc_chunk<12, BLUR, COUNT>(T, P, px, py, dp, ks, nks, okmask, c12, ntaps);
+#pragma unroll
+            for (int c = 0; c < 12; ++c) if (c < nks) out[ks[c] * out_stride] = c12[c];
+        } else if (nks > 4) {
+            float c8[8];
+            ncc_chunk<8, BLUR, COUNT>(T, P, px, py, dp, ks, nks, okmask, c8, ntaps);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) if (c < nks) out[ks[c] * out_stride] = c8[c];
+        } else {
+            float c4[4];
+            ncc_chunk<4, BLUR, COUNT>(T, P, px, py, dp, ks, nks, okmask, c4, ntaps);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) if (c < nks) out[ks[c] * out_stride] = c4[c];
+        }
+    }
+    if (COUNT) {
+        const unsigned tot = __reduce_add_sync(kFullMask, ntaps);
+        if ((threadIdx.x & 31) == 0 && tot) atomicAdd(P.tap_counter, (unsigned long long)tot);
     }
 }
 

@@ -24,18 +24,23 @@ namespace pfd {
 // --------------------------------------------------------------------------
 __host__ __device__ inline int align16(int v) { return (v + 15) & ~15; }
 
+// Row stride of the neighbour row pairs: even (conflict-free 8-byte loads for
+// two rows of checkerboard pixels) and at least W + 1.
+__host__ __device__ inline int pair_stride(int W) { return (W + 2) & ~1; }
+
 struct SmemPlan {
     int off_Q, off_QB, off_R, off_RB, off_geo, off_ok, off_as, off_ac;
-    int off_prevc, off_prevs, off_pix, off_vw, off_cost, off_stage, off_bar, total;
+    int off_prevc, off_prevs, off_vw, off_cost, off_stage, off_bar, total;
+    int q_bytes;
 
     __host__ __device__ static SmemPlan make(int W, int H, int K, int npb, int ntap, bool blur,
                                              int cost_slots, bool sweep, int tile_stride)
     {
         SmemPlan p;
         int o = 0;
-        const int q = K * (H + 2) * (W + 1) * 8;
-        p.off_Q = o;    o += align16(q);
-        p.off_QB = o;   o += blur ? align16(q) : 0;
+        p.q_bytes = (H + 2) * pair_stride(W) * 8;
+        p.off_Q = o;    o += align16(K * p.q_bytes);
+        p.off_QB = o;   o += blur ? align16(K * p.q_bytes) : 0;
         p.off_R = o;    o += align16(H * W * 4);
         p.off_RB = o;   o += blur ? align16(H * W * 4) : 0;
         p.off_geo = o;  o += align16(K * (int)sizeof(NbGeo));
@@ -44,7 +49,6 @@ struct SmemPlan {
         p.off_ac = o;   o += 256 * 4;
         p.off_prevc = o; o += sweep ? align16(W * H * 4) : 0;
         p.off_prevs = o; o += sweep ? align16(W * H * 4) : 0;
-        p.off_pix = o;  o += align16(2 * npb * 4);
         p.off_vw = o;   o += sweep ? align16(K * npb * 4) : 0;
         p.off_bar = o;  o += 16;
         p.off_cost = o;
@@ -143,37 +147,38 @@ __device__ __forceinline__ bool stage_tiles(unsigned char* smem, const SmemPlan&
     if (__syncthreads_or(!ok)) return false;
 
     float* R = (float*)(smem + L.off_R);
-    float2* Q = (float2*)(smem + L.off_Q);
     for (int e = threadIdx.x; e < W * H; e += blockDim.x) R[e] = (float)stage[e];
     if (BLUR) {
         float* RB = (float*)(smem + L.off_RB);
         for (int e = threadIdx.x; e < W * H; e += blockDim.x) RB[e] = (float)stage[nt * ts + e];
     }
-    const int qs = (H + 2) * (W + 1);
+    const int S = pair_stride(W);
+    const int qs = (H + 2) * S;
+    int2* Q = (int2*)(smem + L.off_Q);
+    int2* QB = (int2*)(smem + L.off_QB);
     for (int e = threadIdx.x; e < nc * qs; e += blockDim.x) {
         const int k = e / qs, r = e % qs;
-        const int y = r / (W + 1), x = r % (W + 1);
-        const int yy = y < H ? y : H - 1;
-        const int x0 = x < W ? x : W - 1, x1 = (x + 1) < W ? (x + 1) : W - 1;
+        const int y = r / S, x = r % S;
+        const int yy = min(y, H - 1);
+        const int x0 = min(x, W - 1), x1 = min(x + 1, W - 1);
         const uint8_t* src = stage + (1 + k) * ts + yy * W;
-        const float t0 = (float)src[x0], t1 = (float)src[x1];
-        Q[e] = make_float2(__fsub_rn(__fmul_rn(2.0f, t0), t1), __fsub_rn(t1, t0));
+        Q[e] = make_int2((int)src[x0], (int)src[x1] - (int)src[x0]);
         if (BLUR) {
             const uint8_t* sb = stage + (nt + 1 + k) * ts + yy * W;
-            const float b0 = (float)sb[x0], b1 = (float)sb[x1];
-            ((float2*)(smem + L.off_QB))[e] = make_float2(__fsub_rn(__fmul_rn(2.0f, b0), b1), __fsub_rn(b1, b0));
+            QB[e] = make_int2((int)sb[x0], (int)sb[x1] - (int)sb[x0]);
         }
     }
     __syncthreads();
     T.R = R;
     T.RB = BLUR ? (const float*)(smem + L.off_RB) : nullptr;
-    T.Q = Q;
-    T.QB = BLUR ? (const float2*)(smem + L.off_QB) : nullptr;
+    T.q_addr = smem_u32(smem + L.off_Q);
+    T.qb_addr = BLUR ? smem_u32(smem + L.off_QB) : 0u;
+    T.q_stride = S;
+    T.q_bytes = L.q_bytes;
     T.geo = geo;
     T.nb_ok = okk;
     T.a_s = a_s;
     T.a_c = a_c;
-    T.q_stride = qs;
     return true;
 }
 
@@ -208,37 +213,40 @@ __global__ void pm_slice_kernel(const uint8_t* raw, int raw_pitch, const int2* o
 }
 
 // --------------------------------------------------------------------------
-// RandomInitializationForFrame
+// RandomInitializationForFrame.  One thread per pixel; every lane of a warp
+// takes part in the warp-collective cost evaluation.
 // --------------------------------------------------------------------------
-template <int KCH, bool BLUR>
+template <bool BLUR, bool COUNT>
 __global__ void __launch_bounds__(256) pm_init_kernel(FrameDev F, PmParams P, StateDev out, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int vid = blockIdx.x;
     const int npb = blockDim.x;
+    const int t = threadIdx.x;
     const int nc = min(F.nb_counts[vid], P.K);
     const SmemPlan L = SmemPlan::make(P.W, P.H, P.K, npb, P.ntap, BLUR, 1, false, P.tile_stride);
     Tiles T;
     if (!stage_tiles<BLUR>(smem, L, F, P, vid, nc, T, err)) return;
 
-    const int e = blockIdx.y * npb + threadIdx.x;
-    if (e >= P.ppv) return;
-    const int x = e % P.W, y = e / P.W;
-    const size_t idx = (size_t)vid * P.ppv + e;
+    const int e = blockIdx.y * npb + t;
+    const bool act = e < P.ppv;
+    const int x = act ? e % P.W : 0, y = act ? e / P.W : 0;
+    const size_t idx = (size_t)vid * P.ppv + (act ? e : 0);
     DrawStream g;
     g.init(P.seed, 0u, (uint32_t)idx);
-    const float4 h = random_plane(g, P.depth_min, P.depth_max);
-    float* cs = (float*)(smem + L.off_cost);
-    const int t = threadIdx.x;
-    cost_vector<KCH, BLUR>(T, P, x, y, h, nc, [&](int k, float c) { cs[k * npb + t] = c; });
+    float4 h = make_float4(0.f, 0.f, 1.f, 0.f);
+    if (act) h = random_plane(g, P.depth_min, P.depth_max);
+    float* cs = (float*)(smem + L.off_cost) + t;           // [k][npb]
+    cost_vector<BLUR, COUNT>(T, P, x, y, act, h, nc, cs, npb);
+    if (!act) return;
 
     // ComputeSelectedViewsTopK_Frame (AdaptMIPMFrame.cu:227-282)
     int best_idx = -1, valid = 0;
     for (int i = 0; i < nc; ++i) {
-        const float c = cs[i * npb + t];
+        const float c = cs[i * npb];
         if (c < 2.0f) {
             ++valid;
-            if (best_idx < 0 || c < cs[best_idx * npb + t]) best_idx = i;
+            if (best_idx < 0 || c < cs[best_idx * npb]) best_idx = i;
         }
     }
     float mean = 2.0f;
@@ -246,7 +254,7 @@ __global__ void __launch_bounds__(256) pm_init_kernel(FrameDev F, PmParams P, St
     if (valid > 0) {
         const int kk = min(valid, P.top_k);
         float tmp[kMaxNb];
-        for (int i = 0; i < kMaxNb; ++i) tmp[i] = (i < nc) ? cs[i * npb + t] : 2.0f;
+        for (int i = 0; i < kMaxNb; ++i) tmp[i] = (i < nc) ? cs[i * npb] : 2.0f;
         for (int i = 0; i < kk; ++i)
             for (int j = i + 1; j < nc; ++j)
                 if (tmp[j] < tmp[i]) { const float s = tmp[i]; tmp[i] = tmp[j]; tmp[j] = s; }
@@ -255,7 +263,7 @@ __global__ void __launch_bounds__(256) pm_init_kernel(FrameDev F, PmParams P, St
         mean = __fdiv_rn(m, (float)kk);
         const float thr = tmp[kk - 1];
         for (int i = 0; i < nc && i < 32; ++i)
-            if (cs[i * npb + t] <= thr) mask |= (1u << i);
+            if (cs[i * npb] <= thr) mask |= (1u << i);
     }
     float4 disp = make_float4(0.f, 0.f, 0.f, 0.f);
     if (best_idx >= 0) disp = geo_disp(T.geo[best_idx], x, y, to_disparity(x, y, disparity_plane(x, y, h)));
@@ -333,7 +341,19 @@ __device__ __forceinline__ void find_candidates(const float* pc, int x, int y, i
     if (x >= W - 3 && x < W - 1) { C.flag[7] = 1; C.pos[7] = C.pos[6]; C.src[7] = 6; }
 }
 
-template <int KCH, bool BLUR>
+// Position of the n-th (0-based) set bit of m, or -1.
+__device__ __forceinline__ int nth_set_bit(uint32_t m, int n)
+{
+    for (int i = 0; i < n && m; ++i) m &= m - 1;
+    return m ? __ffs(m) - 1 : -1;
+}
+
+// One red or black half-sweep.  Every lane of a warp reaches each cost
+// evaluation together (lanes without a pixel, or whose candidate slot is
+// empty, ride along inactive); per-lane logic between evaluations is free to
+// diverge.  Cross-view proposals and refinement candidates are walked by a
+// warp-uniform loop in which every lane takes its own next hypothesis.
+template <bool BLUR, bool COUNT>
 __global__ void __launch_bounds__(256) pm_sweep_kernel(FrameDev F, PmParams P, StateDev prev, StateDev next,
                                                        int iter, int phase, int* err)
 {
@@ -346,7 +366,6 @@ __global__ void __launch_bounds__(256) pm_sweep_kernel(FrameDev F, PmParams P, S
     const SmemPlan L = SmemPlan::make(W, H, K, npb, P.ntap, BLUR, 9, true, P.tile_stride);
     const size_t vbase = (size_t)vid * P.ppv;
 
-    // this batch's pixels of each colour
     int ux = 0, uy = 0, cx = 0, cy = 0;
     const bool has_u = nth_pixel(blockIdx.y * npb + t, phase, W, H, ux, uy);
     const bool has_c = nth_pixel(blockIdx.y * npb + t, phase ^ 1, W, H, cx, cy);
@@ -372,132 +391,145 @@ __global__ void __launch_bounds__(256) pm_sweep_kernel(FrameDev F, PmParams P, S
     uint32_t* ps = (uint32_t*)(smem + L.off_prevs);
     for (int e = t; e < P.ppv; e += npb) { pc[e] = prev.cost[vbase + e]; ps[e] = prev.sel[vbase + e]; }
     __syncthreads();
-    if (!has_u) return;
 
     const int x = ux, y = uy;
     const int center = y * W + x;
     const size_t idx = vbase + center;
-    float* cA = (float*)(smem + L.off_cost);          // [slot][k][npb]
-    float* vws = (float*)(smem + L.off_vw);           // [k][npb]
-#define COSTA(slot, k) cA[((slot) * K + (k)) * npb + t]
-#define VW(k) vws[(k) * npb + t]
+    float* cA = (float*)(smem + L.off_cost) + t;       // [slot][k][npb]
+    float* vws = (float*)(smem + L.off_vw) + t;        // [k][npb]
+#define COSTA(slot, k) cA[((slot) * K + (k)) * npb]
+#define VW(k) vws[(k) * npb]
 
     // ---- propagation candidates and the current plane --------------------
     Cands C;
-    find_candidates(pc, x, y, W, H, C);
+    if (has_u) find_candidates(pc, x, y, W, H, C);
+    else for (int a = 0; a < 8; ++a) { C.flag[a] = 0; C.pos[a] = 0; C.src[a] = -1; }
     for (int s = 0; s < 8; ++s) {
-        if (!C.flag[s] || C.src[s] >= 0) continue;
-        const float4 h = prev.plane[vbase + C.pos[s]];
-        cost_vector<KCH, BLUR>(T, P, x, y, h, nc, [&](int k, float c) { COSTA(s, k) = c; });
+        const bool act = has_u && C.flag[s] && C.src[s] < 0;
+        const float4 h = act ? prev.plane[vbase + C.pos[s]] : make_float4(0.f, 0.f, 1.f, 0.f);
+        cost_vector<BLUR, COUNT>(T, P, x, y, act, h, nc, &COSTA(s, 0), npb);
     }
     for (int s = 0; s < 8; ++s) {
-        if (!C.flag[s] || C.src[s] < 0) continue;
+        if (!has_u || !C.flag[s] || C.src[s] < 0) continue;
         for (int k = 0; k < nc; ++k) COSTA(s, k) = COSTA(C.src[s], k);
     }
-    float4 best_plane = prev.plane[idx];
-    cost_vector<KCH, BLUR>(T, P, x, y, best_plane, nc, [&](int k, float c) { COSTA(8, k) = c; });
+    float4 best_plane = has_u ? prev.plane[idx] : make_float4(0.f, 0.f, 1.f, 0.f);
+    cost_vector<BLUR, COUNT>(T, P, x, y, has_u, best_plane, nc, &COSTA(8, 0), npb);
 
     // ---- view-selection priors and sampling (AdaptMIPMFrame.cu:797-875) ----
     DrawStream g;
     g.init(P.seed, (uint32_t)(1 + 2 * iter + phase), (uint32_t)idx);
-    const int dpos[4] = { (y > 0) ? center - W : -1, (y < H - 1) ? center + W : -1,
-                          (x > 0) ? center - 1 : -1, (x < W - 1) ? center + 1 : -1 };
-    const float thr = __fmul_rn(0.8f, pfd_expf(__fdiv_rn((float)(iter * iter), -90.0f)));
-    const float p_default = pfd_expf(__fdiv_rn(__fmul_rn(thr, thr), -0.32f));
-    float psum = 0.0f;
-    for (int i = 0; i < nc; ++i) {
-        float prior = 0.0f;
-        for (int ii = 0; ii < 4; ++ii) {
-            if (dpos[ii] < 0 || !C.flag[2 * ii]) continue;
-            prior = __fadd_rn(prior, ((ps[dpos[ii]] >> i) & 1u) ? 0.9f : 0.1f);
-        }
-        float count = 0.0f, tmpw = 0.0f;
-        int count_false = 0;
-        for (int j = 0; j < 8; ++j) {
-            if (!C.flag[j]) continue;
-            const float c = COSTA(j, i);
-            if (c < thr) { tmpw = __fadd_rn(tmpw, pfd_expf(__fdiv_rn(__fmul_rn(c, c), -0.18f))); count = __fadd_rn(count, 1.0f); }
-            if (c > 1.2f) count_false++;
-        }
-        float pr = 0.0f;
-        if (count > 2.0f && count_false < 3) pr = __fdiv_rn(tmpw, count);
-        else if (count_false < 3) pr = p_default;
-        pr = __fmul_rn(pr, prior);
-        VW(i) = pr;                       // probabilities live in the weight slots until the draws
-        psum = __fadd_rn(psum, pr);
-    }
-    {   // TransformPDFToCDF (CudaUtil.cu:491-507)
-        const float inv = __fdiv_rn(1.0f, psum);
-        float cum = 0.0f;
-        for (int i = 0; i < nc; ++i) { cum = __fmaf_rn(VW(i), inv, cum); VW(i) = cum; }
-    }
-    uint32_t counts[kMaxNb / 8];          // 4-bit draw counts per view
-    for (int i = 0; i < kMaxNb / 8; ++i) counts[i] = 0;
-    for (int sample = 0; sample < 15; ++sample) {
-        const float rp = __fsub_rn(g.uniform(), 1.1920928955078125e-07f);
-        for (int id = 0; id < nc; ++id)
-            if (VW(id) > rp) { counts[id >> 3] += 1u << ((id & 7) * 4); break; }
-    }
     uint32_t tsel = 0;
-    for (int i = 0; i < nc; ++i) {
-        const uint32_t cnt = (counts[i >> 3] >> ((i & 7) * 4)) & 15u;
-        VW(i) = (float)cnt;
-        if (cnt) tsel |= 1u << i;
-    }
-    if (tsel == 0) {
-        for (int i = 0; i < nc; ++i) { VW(i) = 1.0f; tsel |= 1u << i; }
-    }
+    float best_cost = kCostMax;
+    int best_min = -1;
+    if (has_u) {
+        const int dpos[4] = { (y > 0) ? center - W : -1, (y < H - 1) ? center + W : -1,
+                              (x > 0) ? center - 1 : -1, (x < W - 1) ? center + 1 : -1 };
+        const float thr = __fmul_rn(0.8f, pfd_expf(__fdiv_rn((float)(iter * iter), -90.0f)));
+        const float p_default = pfd_expf(__fdiv_rn(__fmul_rn(thr, thr), -0.32f));
+        float psum = 0.0f;
+        for (int i = 0; i < nc; ++i) {
+            float prior = 0.0f;
+            for (int ii = 0; ii < 4; ++ii) {
+                if (dpos[ii] < 0 || !C.flag[2 * ii]) continue;
+                prior = __fadd_rn(prior, ((ps[dpos[ii]] >> i) & 1u) ? 0.9f : 0.1f);
+            }
+            float count = 0.0f, tmpw = 0.0f;
+            int count_false = 0;
+            for (int j = 0; j < 8; ++j) {
+                if (!C.flag[j]) continue;
+                const float c = COSTA(j, i);
+                if (c < thr) { tmpw = __fadd_rn(tmpw, pfd_expf(__fdiv_rn(__fmul_rn(c, c), -0.18f))); count = __fadd_rn(count, 1.0f); }
+                if (c > 1.2f) count_false++;
+            }
+            float pr = 0.0f;
+            if (count > 2.0f && count_false < 3) pr = __fdiv_rn(tmpw, count);
+            else if (count_false < 3) pr = p_default;
+            pr = __fmul_rn(pr, prior);
+            VW(i) = pr;                   // probabilities live in the weight slots until the draws
+            psum = __fadd_rn(psum, pr);
+        }
+        {   // TransformPDFToCDF (CudaUtil.cu:491-507)
+            const float inv = __fdiv_rn(1.0f, psum);
+            float cum = 0.0f;
+            for (int i = 0; i < nc; ++i) { cum = __fmaf_rn(VW(i), inv, cum); VW(i) = cum; }
+        }
+        uint32_t counts[kMaxNb / 8];      // 4-bit draw counts per view
+        for (int i = 0; i < kMaxNb / 8; ++i) counts[i] = 0;
+        for (int sample = 0; sample < 15; ++sample) {
+            const float rp = __fsub_rn(g.uniform(), 1.1920928955078125e-07f);
+            for (int id = 0; id < nc; ++id)
+                if (VW(id) > rp) { counts[id >> 3] += 1u << ((id & 7) * 4); break; }
+        }
+        for (int i = 0; i < nc; ++i) {
+            const uint32_t cnt = (counts[i >> 3] >> ((i & 7) * 4)) & 15u;
+            VW(i) = (float)cnt;
+            if (cnt) tsel |= 1u << i;
+        }
+        if (tsel == 0)
+            for (int i = 0; i < nc; ++i) { VW(i) = 1.0f; tsel |= 1u << i; }
 
-    // ---- weighted costs: current plane, then the 8 candidates -----------
-    float best_cost;
-    int best_min;
-    {
-        WeightedCost wc;
-        for (int k = 0; k < nc; ++k) wc.add(k, COSTA(8, k), VW(k));
-        best_cost = wc.result();
-        best_min = wc.min_idx;
+        // weighted costs: current plane, then the 8 candidates
+        {
+            WeightedCost wc;
+            for (int k = 0; k < nc; ++k) wc.add(k, COSTA(8, k), VW(k));
+            best_cost = wc.result();
+            best_min = wc.min_idx;
+        }
+        for (int s = 0; s < 8; ++s) {
+            if (!C.flag[s]) continue;
+            WeightedCost wc;
+            for (int k = 0; k < nc; ++k) wc.add(k, COSTA(s, k), VW(k));
+            const float c = wc.result();
+            if (c < best_cost) { best_cost = c; best_plane = prev.plane[vbase + C.pos[s]]; best_min = wc.min_idx; }
+        }
     }
-    for (int s = 0; s < 8; ++s) {
-        if (!C.flag[s]) continue;
-        WeightedCost wc;
-        for (int k = 0; k < nc; ++k) wc.add(k, COSTA(s, k), VW(k));
-        const float c = wc.result();
-        if (c < best_cost) { best_cost = c; best_plane = prev.plane[vbase + C.pos[s]]; best_min = wc.min_idx; }
-    }
+    float* scratch = &COSTA(0, 0);                    // candidate costs are dead from here on
 
     // ---- cross-view proposals (AdaptMIPMFrame.cu:907-936) ----------------
-    for (int k = 0; k < nc; ++k) {
-        if (!((tsel >> k) & 1u)) continue;
-        const int nvid = F.nb_ids[vid * K + k];
-        if (nvid < 0) continue;
-        const NbGeo& gk = T.geo[k];
-        const float dcur = to_disparity(x, y, disparity_plane(x, y, best_plane));
-        const float2 qf = geo_anchor(gk, x, y, dcur);
-        const float fqx = floorf(__fadd_rn(qf.x, 0.5f)), fqy = floorf(__fadd_rn(qf.y, 0.5f));
-        if (!(fqx >= 0.0f && fqx < (float)W && fqy >= 0.0f && fqy < (float)H)) continue;
-        const int qx = (int)fqx, qy = (int)fqy;
-        const float4 hn = prev.plane[(size_t)nvid * P.ppv + qy * W + qx];
-        const float3 dpn = disparity_plane(qx, qy, hn);
-        float denom = __fmaf_rn(dpn.y, gk.by, __fmaf_rn(dpn.x, gk.bx, 1.0f));
-        denom = safe_denom(denom);
-        const float4 proxy = encode_plane(x, y, __fdiv_rn(dpn.x, denom), __fdiv_rn(dpn.y, denom), __fdiv_rn(dpn.z, denom));
-        WeightedCost wc;
-        cost_vector<KCH, BLUR>(T, P, x, y, proxy, nc, [&](int kk, float c) { wc.add(kk, c, VW(kk)); });
-        const float c = wc.result();
-        if (c < best_cost) { best_cost = c; best_plane = proxy; best_min = wc.min_idx; }
+    const int nsel = __popc(tsel);
+    const int nmax = __reduce_max_sync(kFullMask, nsel);
+    for (int n = 0; n < nmax; ++n) {
+        const int k = (n < nsel) ? nth_set_bit(tsel, n) : -1;
+        bool act = false;
+        float4 proxy = make_float4(0.f, 0.f, 1.f, 0.f);
+        if (k >= 0) {
+            const int nvid = F.nb_ids[vid * K + k];
+            if (nvid >= 0) {
+                const NbGeo& gk = T.geo[k];
+                const float dcur = to_disparity(x, y, disparity_plane(x, y, best_plane));
+                const float2 qf = geo_anchor(gk, x, y, dcur);
+                const float fqx = floorf(__fadd_rn(qf.x, 0.5f)), fqy = floorf(__fadd_rn(qf.y, 0.5f));
+                if (fqx >= 0.0f && fqx < (float)W && fqy >= 0.0f && fqy < (float)H) {
+                    const int qx = (int)fqx, qy = (int)fqy;
+                    const float4 hn = prev.plane[(size_t)nvid * P.ppv + qy * W + qx];
+                    const float3 dpn = disparity_plane(qx, qy, hn);
+                    float denom = __fmaf_rn(dpn.y, gk.by, __fmaf_rn(dpn.x, gk.bx, 1.0f));
+                    denom = safe_denom(denom);
+                    proxy = encode_plane(x, y, __fdiv_rn(dpn.x, denom), __fdiv_rn(dpn.y, denom), __fdiv_rn(dpn.z, denom));
+                    act = true;
+                }
+            }
+        }
+        cost_vector<BLUR, COUNT>(T, P, x, y, act, proxy, nc, scratch, npb);
+        if (act) {
+            WeightedCost wc;
+            for (int kk = 0; kk < nc; ++kk) wc.add(kk, scratch[kk * npb], VW(kk));
+            const float c = wc.result();
+            if (c < best_cost) { best_cost = c; best_plane = proxy; best_min = wc.min_idx; }
+        }
     }
 
     // ---- refinement (PlaneHypothesisRefinement_Frame, :400-471) ---------
-    {
+    float4 cand[5];
+    if (has_u) {
         const float depth_now = best_plane.w;
-        if (best_cost < 0.1f) (void)g.uniform();   // depth_rand: drawn, unused
-        else (void)g.uniform();
+        (void)g.uniform();                           // depth_rand: drawn, never used
         const float4 rn = random_normal(g);
         const float4 pn = perturbed_normal(x, y, best_plane, g, P.pert_pi);
         const float dmin_p = __fmul_rn(__fsub_rn(1.0f, 0.02f), depth_now);
         const float dmax_p = __fmul_rn(__fadd_rn(1.0f, 0.02f), depth_now);
         const float depth_perturbed = __fmaf_rn(g.uniform(), __fsub_rn(dmax_p, dmin_p), dmin_p);
-        float4 cand[5];
         cand[0] = random_plane(g, P.depth_min, P.depth_max);
         cand[1] = rn;
         cand[2] = pn;
@@ -505,15 +537,21 @@ __global__ void __launch_bounds__(256) pm_sweep_kernel(FrameDev F, PmParams P, S
         cand[4] = best_plane;
         cand[4].w = depth_perturbed;
         for (int i = 1; i < 5; ++i) cand[i].w = to_disparity(x, y, disparity_plane(x, y, cand[i]));
-        for (int i = 0; i < 5; ++i) {
+    } else {
+        for (int i = 0; i < 5; ++i) cand[i] = make_float4(0.f, 0.f, 1.f, 0.f);
+    }
+    for (int i = 0; i < 5; ++i) {
+        cost_vector<BLUR, COUNT>(T, P, x, y, has_u, cand[i], nc, scratch, npb);
+        if (has_u) {
             WeightedCost wc;
-            cost_vector<KCH, BLUR>(T, P, x, y, cand[i], nc, [&](int kk, float c) { wc.add(kk, c, VW(kk)); });
+            for (int kk = 0; kk < nc; ++kk) wc.add(kk, scratch[kk * npb], VW(kk));
             const float c = wc.result();
             if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = wc.min_idx; }
         }
     }
 #undef COSTA
 #undef VW
+    if (!has_u) return;
     float4 best_disp = make_float4(0.f, 0.f, 0.f, 0.f);
     if (best_min >= 0) best_disp = geo_disp(T.geo[best_min], x, y, to_disparity(x, y, disparity_plane(x, y, best_plane)));
     next.plane[idx] = best_plane;
@@ -525,7 +563,7 @@ __global__ void __launch_bounds__(256) pm_sweep_kernel(FrameDev F, PmParams P, S
 // --------------------------------------------------------------------------
 // Per-hypothesis cost vectors.  Segments group hypotheses of one view.
 // --------------------------------------------------------------------------
-template <int KCH, bool BLUR>
+template <bool BLUR, bool COUNT>
 __global__ void __launch_bounds__(256) pm_ncc_kernel(FrameDev F, PmParams P, const int* seg_vid, const int* seg_start,
                                                      const int* seg_len, const int* hyp_pxy, const float4* hyp_plane,
                                                      const int* hyp_out, float* costs, int* err)
@@ -534,35 +572,22 @@ __global__ void __launch_bounds__(256) pm_ncc_kernel(FrameDev F, PmParams P, con
     const int s = blockIdx.x;
     const int vid = seg_vid[s];
     const int nc = min(F.nb_counts[vid], P.K);
-    const SmemPlan L = SmemPlan::make(P.W, P.H, P.K, blockDim.x, P.ntap, BLUR, 0, false, P.tile_stride);
+    const SmemPlan L = SmemPlan::make(P.W, P.H, P.K, blockDim.x, P.ntap, BLUR, 1, false, P.tile_stride);
     Tiles T;
     if (!stage_tiles<BLUR>(smem, L, F, P, vid, nc, T, err)) return;
-    if ((int)threadIdx.x >= seg_len[s]) return;
-    const int h = seg_start[s] + threadIdx.x;
-    const int px = hyp_pxy[2 * h], py = hyp_pxy[2 * h + 1];
+    const bool act = (int)threadIdx.x < seg_len[s];
+    const int h = seg_start[s] + (act ? threadIdx.x : 0);
+    const int px = act ? hyp_pxy[2 * h] : 0, py = act ? hyp_pxy[2 * h + 1] : 0;
+    float* cs = (float*)(smem + L.off_cost) + threadIdx.x;
+    cost_vector<BLUR, COUNT>(T, P, px, py, act, act ? hyp_plane[h] : make_float4(0.f, 0.f, 1.f, 0.f), nc, cs, blockDim.x);
+    if (!act) return;
     float* out = costs + (size_t)hyp_out[h] * P.K;
-    for (int k = 0; k < P.K; ++k) out[k] = 2.0f;
-    cost_vector<KCH, BLUR>(T, P, px, py, hyp_plane[h], nc, [&](int k, float c) { out[k] = c; });
+    for (int k = 0; k < P.K; ++k) out[k] = (k < nc) ? cs[k * blockDim.x] : 2.0f;
 }
 
 // --------------------------------------------------------------------------
 // Host launchers
 // --------------------------------------------------------------------------
-static int pick_kch(int K)
-{
-    if (K % 6 == 0) return 6;
-    if (K % 4 == 0) return 4;
-    return 6;
-}
-
-template <class F4, class F6, class F8>
-static cudaError_t dispatch_kch(int kch, F4 f4, F6 f6, F8 f8)
-{
-    if (kch == 4) return f4();
-    if (kch == 8) return f8();
-    return f6();
-}
-
 int sweep_smem_bytes(const PmParams& P, int npb, bool blur)
 {
     return SmemPlan::make(P.W, P.H, P.K, npb, P.ntap, blur, 9, true, P.tile_stride).total;
@@ -602,16 +627,11 @@ cudaError_t launch_init(const FrameDev& F, const PmParams& P, const StateDev& ou
     dim3 grid(F.V, (P.ppv + npb - 1) / npb);
     FrameDev f = F; PmParams p = P; StateDev o = out; int* e = err;
     void* args[] = { &f, &p, &o, &e };
-    const int kch = pick_kch(P.K);
-    if (blur)
-        return dispatch_kch(kch,
-            [&] { return launch(pm_init_kernel<4, true>, grid, npb, smem, st, args); },
-            [&] { return launch(pm_init_kernel<6, true>, grid, npb, smem, st, args); },
-            [&] { return launch(pm_init_kernel<8, true>, grid, npb, smem, st, args); });
-    return dispatch_kch(kch,
-        [&] { return launch(pm_init_kernel<4, false>, grid, npb, smem, st, args); },
-        [&] { return launch(pm_init_kernel<6, false>, grid, npb, smem, st, args); },
-        [&] { return launch(pm_init_kernel<8, false>, grid, npb, smem, st, args); });
+    if (P.tap_counter)
+        return blur ? launch(pm_init_kernel<true, true>, grid, npb, smem, st, args)
+                    : launch(pm_init_kernel<false, true>, grid, npb, smem, st, args);
+    return blur ? launch(pm_init_kernel<true, false>, grid, npb, smem, st, args)
+                : launch(pm_init_kernel<false, false>, grid, npb, smem, st, args);
 }
 
 cudaError_t launch_sweep(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
@@ -625,16 +645,11 @@ cudaError_t launch_sweep(const FrameDev& F, const PmParams& P, const StateDev& p
     dim3 grid(F.V, (updated + npb - 1) / npb);
     FrameDev f = F; PmParams p = P; StateDev a = prev, b = next; int it = iter, ph = phase; int* e = err;
     void* args[] = { &f, &p, &a, &b, &it, &ph, &e };
-    const int kch = pick_kch(P.K);
-    if (blur)
-        return dispatch_kch(kch,
-            [&] { return launch(pm_sweep_kernel<4, true>, grid, npb, smem, st, args); },
-            [&] { return launch(pm_sweep_kernel<6, true>, grid, npb, smem, st, args); },
-            [&] { return launch(pm_sweep_kernel<8, true>, grid, npb, smem, st, args); });
-    return dispatch_kch(kch,
-        [&] { return launch(pm_sweep_kernel<4, false>, grid, npb, smem, st, args); },
-        [&] { return launch(pm_sweep_kernel<6, false>, grid, npb, smem, st, args); },
-        [&] { return launch(pm_sweep_kernel<8, false>, grid, npb, smem, st, args); });
+    if (P.tap_counter)
+        return blur ? launch(pm_sweep_kernel<true, true>, grid, npb, smem, st, args)
+                    : launch(pm_sweep_kernel<false, true>, grid, npb, smem, st, args);
+    return blur ? launch(pm_sweep_kernel<true, false>, grid, npb, smem, st, args)
+                : launch(pm_sweep_kernel<false, false>, grid, npb, smem, st, args);
 }
 
 cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, const int* seg_vid, const int* seg_start,
@@ -643,20 +658,12 @@ cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, 
 {
     if (nseg <= 0) return cudaSuccess;
     const bool blur = F.blur != nullptr;
-    const int smem = SmemPlan::make(P.W, P.H, P.K, npb, P.ntap, blur, 0, false, P.tile_stride).total;
+    const int smem = SmemPlan::make(P.W, P.H, P.K, npb, P.ntap, blur, 1, false, P.tile_stride).total;
     FrameDev f = F; PmParams p = P;
     void* args[] = { &f, &p, (void*)&seg_vid, (void*)&seg_start, (void*)&seg_len, (void*)&hyp_pxy,
                      (void*)&hyp_plane, (void*)&hyp_out, &costs, &err };
-    const int kch = pick_kch(P.K);
-    if (blur)
-        return dispatch_kch(kch,
-            [&] { return launch(pm_ncc_kernel<4, true>, nseg, npb, smem, st, args); },
-            [&] { return launch(pm_ncc_kernel<6, true>, nseg, npb, smem, st, args); },
-            [&] { return launch(pm_ncc_kernel<8, true>, nseg, npb, smem, st, args); });
-    return dispatch_kch(kch,
-        [&] { return launch(pm_ncc_kernel<4, false>, nseg, npb, smem, st, args); },
-        [&] { return launch(pm_ncc_kernel<6, false>, nseg, npb, smem, st, args); },
-        [&] { return launch(pm_ncc_kernel<8, false>, nseg, npb, smem, st, args); });
+    return blur ? launch(pm_ncc_kernel<true, false>, nseg, npb, smem, st, args)
+                : launch(pm_ncc_kernel<false, false>, nseg, npb, smem, st, args);
 }
 
 }  // namespace pfd

@@ -18,5 +18,7 @@ cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, 
                        const int* seg_start, const int* seg_len, const int* hyp_pxy, const float4* hyp_plane,
                        const int* hyp_out, float* costs, int* err, cudaStream_t st);
 int sweep_smem_bytes(const PmParams& P, int npb, bool blur);
+// FP32 FFMA throughput probe (diag.cu): best of three timed launches.
+cudaError_t measure_fma_rate(cudaStream_t st, float* ms, double* flops);
 
 }  // namespace pfd
