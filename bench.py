@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the plenoptic depth hot path on B200.
+
+One step = one 4080x3068 8-bit raw frame (pitch 23.2 px, three lens types with
+blur sigma 0.6/1.0/1.4, 12 slanted planes, ~26.6 k micro-images) through the
+engine: micro-image slicing, random initialisation and 8 red-black PatchMatch
+iterations with 12 neighbours and a 15x15 bilateral NCC, FP32.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Prints one JSON line (rank 0).  Under torchrun each rank processes its own
+frame (frames are independent: weak scaling, replicas only); ranks meet only
+for the barrier and the max-over-ranks timing.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "plenoptic-for-depth_b200")
+
+WORKLOAD = dict(width=4080, height=3068, pitch=23.2, n_planes=12, max_nb=12, patch_size=15, iterations=8,
+                sigma_spatial=3.0, sigma_color=12.0, n_lens_types=3, blur_sigma=(0.6, 1.0, 1.4), seed=2026)
+METRIC = "4080x3068 depth frames/s"
+FLOPS_PER_TAP = 24      # per in-bounds NCC tap: disparity 4, source coords 4, fractions 2, bilinear 6, moments 8
+
+
+def load_pfd():
+    name = "pfd_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pfd_oracle
+    pfd_oracle.build()
+    return pfd_oracle
+
+
+def make_workload(pfd, rank: int):
+    w = WORKLOAD
+    return pfd.make_workload(w["width"], w["height"], w["pitch"], w["n_planes"], seed=w["seed"] + rank,
+                             max_nb=w["max_nb"], n_lens_types=w["n_lens_types"], blur_sigma=w["blur_sigma"])
+
+
+def pm_params(pfd):
+    w = WORKLOAD
+    return pfd.PmParams(base=w["pitch"], patch_size=w["patch_size"], max_iterations=w["iterations"],
+                        sigma_spatial=w["sigma_spatial"], sigma_color=w["sigma_color"])
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the oracle restatement of the reference, on a bounded sample
+# --------------------------------------------------------------------------
+class CpuSample:
+    """The oracle's RandomInitializationForFrame + one CheckerboardUpdateFrame
+    half-sweep, timed on a contiguous block of micro-images and extrapolated
+    to one frame (init of every view + 2 x iterations half-sweeps).  The
+    neighbourhood the half-sweep reads (cross-view proposals) is initialised
+    once, outside the timed region."""
+
+    def __init__(self, oracle, w, params, seed, nthreads):
+        self.orc = oracle.Oracle(w.gray, w.centers, w.nb_ids, w.nb_counts)
+        self.params, self.seed, self.nthreads = params, seed, nthreads
+        self.V = w.centers.shape[0]
+        self.v0 = self.V // 2
+        self.max_views = min(2048, self.V - self.v0)
+        self.state = self.orc.init(params, seed, nthreads=nthreads,
+                                   views=(max(0, self.v0 - 400), min(self.V, self.v0 + 400 + self.max_views)))
+        self.nv = 2
+
+    def time_block(self, nv):
+        t0 = time.perf_counter()
+        self.orc.init(self.params, self.seed, nthreads=self.nthreads, views=(self.v0, self.v0 + nv))
+        t1 = time.perf_counter()
+        self.orc.sweep(self.params, self.seed, 0, 0, self.state, nthreads=self.nthreads, views=(self.v0, self.v0 + nv))
+        t2 = time.perf_counter()
+        return t1 - t0, t2 - t1
+
+    def calibrate(self, budget_s):
+        nv = 2
+        while True:
+            ti, ts = self.time_block(nv)
+            if ti + ts >= 0.5 * budget_s or nv >= self.max_views:
+                break
+            nv = min(self.max_views, max(2 * nv, int(nv * 0.7 * budget_s / max(ti + ts, 1e-3))))
+        self.nv = nv
+
+    def run(self) -> dict:
+        ti, ts = self.time_block(self.nv)
+        frame_s = (ti + 2 * self.params.max_iterations * ts) * self.V / self.nv
+        return {"frame_s": frame_s, "views": self.nv, "t_init": ti, "t_sweep": ts}
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------------
+# engine arm
+# --------------------------------------------------------------------------
+def run_engine(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    pfd = load_pfd()
+    torch.cuda.set_device(local_rank)
+    w = make_workload(pfd, rank)
+    params = pm_params(pfd)
+    V = w.centers.shape[0]
+    ctx = pfd.Context(local_rank)
+    fid = ctx.frame_create(w.frame.raw.shape[1], w.frame.raw.shape[0], w.centers, w.tilekeys, w.mi, w.mi,
+                           w.nb_ids, w.nb_counts)
+    raw_dev = torch.from_numpy(w.frame.raw).to(f"cuda:{local_rank}")
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local_rank}")
+    seed = WORKLOAD["seed"]
+    launches_per_step = 1 + 1 + 2 * params.max_iterations     # slice, init, sweeps
+
+    def step(ev=None):
+        ctx.frame_set_raw_device(fid, raw_dev.data_ptr(), raw_dev.shape[1])
+        ctx.pm_init(fid, params, seed)
+        for it in range(params.max_iterations):
+            for ph in range(2):
+                if ev is not None:
+                    ev[0].append(torch.cuda.Event(enable_timing=True))
+                    ev[0][-1].record(stream)
+                ctx.pm_sweep(fid, params, seed, it, ph)
+                if ev is not None:
+                    ev[1].append(torch.cuda.Event(enable_timing=True))
+                    ev[1][-1].record(stream)
+
+    # calibration pass: in-bounds NCC taps per sweep launch (identical trajectory: same seed)
+    ctx.set_tap_counting(True)
+    ctx.frame_set_raw_device(fid, raw_dev.data_ptr(), raw_dev.shape[1])
+    ctx.pm_init(fid, params, seed)
+    ctx.read_tap_count()
+    sweep_taps = []
+    for it in range(params.max_iterations):
+        for ph in range(2):
+            ctx.pm_sweep(fid, params, seed, it, ph)
+            sweep_taps.append(ctx.read_tap_count())
+    ctx.set_tap_counting(False)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.sync()
+    fp32_tflops = ctx.fp32_fma_rate()
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ev_sweep = ([], [])
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for _ in range(args.steps):
+        step(ev_sweep)
+    t_end.record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = t_start.elapsed_time(t_end)
+    sweep_ms = [a.elapsed_time(b) for a, b in zip(*ev_sweep)]
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # e2e through the public API with host buffers: pinned raw in, per-pixel
+    # state (plane, cost, selected views) out, every step
+    pinned_raw = torch.from_numpy(w.frame.raw).pin_memory()
+    px = V * w.mi * w.mi
+    out_plane = torch.empty((px, 4), dtype=torch.float32).pin_memory()
+    out_cost = torch.empty(px, dtype=torch.float32).pin_memory()
+    out_sel = torch.empty(px, dtype=torch.int32).pin_memory()
+    import ctypes
+    L = pfd.lib()
+
+    def e2e_step():
+        ctx._check(L.pfd_frame_set_raw(ctx._h, fid, ctypes.c_void_p(pinned_raw.data_ptr()), pinned_raw.shape[1]),
+                   "pfd_frame_set_raw")
+        ctx.patchmatch(fid, params, seed)
+        ctx._check(L.pfd_download(ctx._h, fid, ctypes.c_void_p(out_plane.data_ptr()), ctypes.c_void_p(out_cost.data_ptr()),
+                                  None, ctypes.c_void_p(out_sel.data_ptr())), "pfd_download")
+
+    e2e_step()
+    e2e_steps = max(1, min(args.steps, 3))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    result = None
+    if rank == 0:
+        frames = world * args.steps
+        value = frames / (ms / 1e3)
+        # roofline of the dominant kernel (the red-black sweep)
+        avg_sweep_ms = statistics.mean(sweep_ms)
+        taps_per_launch = statistics.mean(sweep_taps)
+        achieved = taps_per_launch * FLOPS_PER_TAP / (avg_sweep_ms * 1e-3) / 1e12
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "pm_sweep_traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                tj = json.load(f)
+            if tj.get("workload") == "4080x3068 pitch 23.2 K12 P15":
+                traffic = tj.get("bytes_per_launch")
+        result = {
+            "metric": METRIC, "value": round(value, 4), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plenoptic raw frame)",
+            "config": {"workload": "%dx%d raw, pitch %.1f px, 3 lens types, %d planes, %d micro-images, "
+                                   "K=%d neighbours, %dx%d bilateral NCC, %d PatchMatch iterations, FP32" %
+                                   (WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["pitch"], WORKLOAD["n_planes"], V,
+                                    WORKLOAD["max_nb"], WORKLOAD["patch_size"], WORKLOAD["patch_size"],
+                                    WORKLOAD["iterations"]),
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "per-step working set %.2f GB > 126 MB L2 (state + tiles)" %
+                             (px * 40 * 2 / 1e9),
+                       "stages": "slice + init + 16 half-sweeps"},
+            "e2e": {"value": round(world * e2e_steps / e2e_s, 4), "unit": "frames/s",
+                    "h2d_bytes_per_step": int(w.frame.raw.nbytes),
+                    "d2h_bytes_per_step": int(out_plane.numel() * 4 + out_cost.numel() * 4 + out_sel.numel() * 4)},
+            "roofline": {"bound": "fp32", "kernel": "pm_sweep_kernel", "achieved": round(achieved, 3),
+                         "peak": round(fp32_tflops, 2), "unit": "TFLOP/s", "frac": round(achieved / fp32_tflops, 4),
+                         "peak_source": "measured FP32 FFMA rate on this device (pfd_fp32_fma_rate); "
+                                        "MEASURED_PEAKS.json has no FP32 figure",
+                         "algorithmic": "%d flops x %.3g in-bounds NCC taps per launch" %
+                                        (FLOPS_PER_TAP, taps_per_launch),
+                         "avg_launch_ms": round(avg_sweep_ms, 3), "traffic": traffic},
+            "clocks": clk,
+            "gpu_launches": launches_per_step * args.steps,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            oracle = load_oracle()
+            nth = cpu_threads()
+            cs = CpuSample(oracle, w, params, seed, nth)
+            cs.calibrate(15.0)
+            s = cs.run()
+            result["cpu_baseline"] = {"value": round(1.0 / s["frame_s"], 8), "unit": "frames/s", "cores": nth,
+                                      "kind": "port",
+                                      "sample": "oracle init + one half-sweep on %d of %d micro-images "
+                                                "(%.1f s + %.1f s), extrapolated to init + 16 half-sweeps" %
+                                                (s["views"], V, s["t_init"], s["t_sweep"])}
+    ctx.frame_free(fid)
+    ctx.close()
+    return result
+
+
+def run_reference(args, rank, world):
+    """The reference's algorithm on host cores: the oracle restatement (the
+    reference's own code needs OpenCV/Eigen/Boost and does not build here),
+    each step a bounded sample of the same workload."""
+    if rank != 0:
+        return None
+    pfd = load_pfd()
+    oracle = load_oracle()
+    w = make_workload(pfd, 0)
+    params = pm_params(pfd)
+    nth = cpu_threads()
+    cs = CpuSample(oracle, w, params, WORKLOAD["seed"], nth)
+    cs.calibrate(6.0)
+    vals = []
+    samples = []
+    for i in range(args.warmup + args.steps):
+        s = cs.run()
+        if i >= args.warmup:
+            vals.append(1.0 / s["frame_s"])
+            samples.append(s)
+    value = statistics.median(vals)
+    V = w.centers.shape[0]
+    s = samples[0]
+    return {
+        "metric": METRIC, "value": round(value, 8), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "dtype": "f32",
+        "data": "synthetic (seeded plenoptic raw frame)",
+        "config": {"workload": "%dx%d raw, pitch %.1f px, %d micro-images, K=%d, %dx%d NCC, %d iterations" %
+                   (WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["pitch"], V, WORKLOAD["max_nb"],
+                    WORKLOAD["patch_size"], WORKLOAD["patch_size"], WORKLOAD["iterations"])},
+        "cpu_baseline": {"value": round(value, 8), "unit": "frames/s", "cores": nth, "kind": "port",
+                         "sample": "oracle init + one half-sweep on %d micro-images per step, extrapolated to a "
+                                   "frame" % s["views"]},
+        "e2e": {"value": round(value, 8), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--frame", default=None, help="WxH override (profiling captures of a smaller frame)")
+    ap.add_argument("--iterations", type=int, default=None, help="PatchMatch iterations override (profiling)")
+    args = ap.parse_args()
+    if args.frame:
+        wdt, hgt = args.frame.lower().split("x")
+        WORKLOAD["width"], WORKLOAD["height"] = int(wdt), int(hgt)
+    if args.iterations is not None:
+        WORKLOAD["iterations"] = args.iterations
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    res = run_engine(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

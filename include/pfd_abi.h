@@ -140,6 +140,51 @@ pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params
 pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane /*[.][4]*/, float* cost,
                         float* disp /*[.][4]*/, uint32_t* sel);
 
+/* ---- consistency pass -------------------------------------------------------
+ * MIDisparityFilterConfig (CheckModule/MIDisparityFilter.h:24-57).  The values
+ * MIStereoMatch::FilterAndStatic passes (MIStereoMatch.cpp:759-778):
+ * max_triplet 4, min_valid_disp 0, selected views only, clear views when
+ * invalid, cost filter 1.8, geo 0.5 px, photo 0.5, 2 good neighbours, spike
+ * filter 1.0 with 3 neighbours. */
+typedef struct {
+    int   max_triplet;
+    float min_valid_disp;
+    int   use_selected_views_only;
+    int   clear_selected_views_when_invalid;
+    int   enable_cost_filter;
+    float max_cost;
+    int   enable_cycle_geo_filter;
+    float max_geo_err_px;
+    int   enable_cycle_photo_filter;
+    float max_photo_err_u;
+    int   min_good_neighbors;
+    int   enable_spike_filter;
+    float spike_abs_diff;
+    int   spike_min_neighbors;
+} pfd_filter_cfg;
+
+/* Reject reasons written to the reason map (MIDisparityFilter.h:102-109). */
+#define PFD_PR_KEEP       0
+#define PFD_PR_COST       80
+#define PFD_PR_NOSUPPORT  140
+#define PFD_PR_CYCLE      200
+#define PFD_PR_SPIKE      255
+
+/* MIDisparityFilterCPU::FilterGlobal (MIDisparityFilter.cpp:962-986): filters
+ * the frame's current PatchMatch state in place, view by view in key order,
+ * with the reference's in-place dependency between views kept exactly.
+ * baseline_unit is LightFieldParams::baseline.  reason (host, [V*mi_w*mi_h],
+ * may be NULL) receives the reject reasons; stats (may be NULL) the counters
+ * total, valid_in, kept, removed, by_cost, by_no_support, by_cycle, by_spike. */
+pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, float baseline_unit,
+                      uint8_t* reason, long long* stats);
+/* ComputeTileReprojectionErrorMap (MIDisparityFilter.cpp:695-842) over the
+ * frame: per-pixel median cycle reprojection error (-1 where fewer than
+ * min_good_neighbors views support it).  err: host [V*mi_w*mi_h], or NULL to
+ * keep the map on the device only. */
+pfd_status pfd_reprojection_error(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, float baseline_unit,
+                                  float* err);
+
 /* ---- measurement --------------------------------------------------------
  * No counterpart in the reference (it has no timers or counters on this path,
  * see its Util/Logger only).  Tap counting switches the PatchMatch kernels to

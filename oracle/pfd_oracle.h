@@ -91,6 +91,44 @@ int orc_pm_sweep_views(const orc_frame* f, const orc_params* p, uint64_t seed, i
  * max_iterations x (phase 0, phase 1).  Result in out. */
 int orc_patchmatch(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int nthreads);
 
+/* ---- consistency pass (oracle/checks.c) ---- */
+
+/* MIDisparityFilterConfig (CheckModule/MIDisparityFilter.h:24-57); the values
+ * MIStereoMatch::FilterAndStatic uses are in MIStereoMatch.cpp:759-778. */
+typedef struct {
+    int   max_triplet;
+    float min_valid_disp;
+    int   use_selected_views_only;
+    int   clear_selected_views_when_invalid;
+    int   enable_cost_filter;
+    float max_cost;
+    int   enable_cycle_geo_filter;
+    float max_geo_err_px;
+    int   enable_cycle_photo_filter;
+    float max_photo_err_u;
+    int   min_good_neighbors;
+    int   enable_spike_filter;
+    float spike_abs_diff;
+    int   spike_min_neighbors;
+} orc_filter_cfg;
+
+/* PixelRejectReason (MIDisparityFilter.h:102-109) */
+enum { ORC_PR_KEEP = 0, ORC_PR_COST = 80, ORC_PR_NOSUPPORT = 140, ORC_PR_CYCLE = 200, ORC_PR_SPIKE = 255 };
+/* MIDisparityFilterStats counters (MIDisparityFilter.h:59-77) */
+enum { ORC_FS_TOTAL = 0, ORC_FS_VALID_IN, ORC_FS_KEPT, ORC_FS_REMOVED, ORC_FS_COST, ORC_FS_NOSUPPORT,
+       ORC_FS_CYCLE, ORC_FS_SPIKE, ORC_FS_COUNT };
+
+/* MIDisparityFilterCPU::FilterGlobal (MIDisparityFilter.cpp:962-986): filters
+ * the views in order, invalidating rejected pixels of st in place; reason
+ * [V*mi_w*mi_h] receives the reject reasons, stats[ORC_FS_COUNT] the counters. */
+int orc_filter_global(const orc_frame* f, const orc_filter_cfg* cfg, float baseline_unit, orc_state* st,
+                      uint8_t* reason, long long* stats);
+
+/* ComputeTileReprojectionErrorMap (MIDisparityFilter.cpp:695-842) for all
+ * views: per-pixel median cycle error, -1 where undefined. */
+int orc_reprojection_error(const orc_frame* f, const orc_filter_cfg* cfg, float baseline_unit, const orc_state* st,
+                           float* err);
+
 /* Scalar hooks for unit tests of the canonical arithmetic. */
 float orc_expf(float x);
 float orc_uniform(uint64_t seed, uint32_t sweep, uint32_t pixel, uint32_t n);

@@ -1,6 +1,7 @@
 // pfd_abi.cu -- implementation of include/pfd_abi.h: contexts, frames and the
 // PatchMatch entry points.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -14,6 +15,7 @@
 
 #include "../../include/pfd_abi.h"
 #include "pm_kernels.h"
+#include "check_kernels.h"
 
 namespace {
 
@@ -33,7 +35,14 @@ struct Frame {
     int cur = 0;                      // s[cur] is the latest state
     bool has_state = false;
     size_t bytes = 0;
+    bool registered = false;          // bytes already counted in the context's total
     std::vector<void*> allocs;
+    // host copies for scheduling the consistency pass
+    std::vector<int> h_keys, h_nb_ids, h_nb_counts;
+    uint8_t* d_reason = nullptr;      // filter reject reasons, allocated on first use
+    float* d_err = nullptr;           // reprojection-error map, allocated on first use
+    int* d_steps = nullptr;           // views grouped by wavefront step
+    std::vector<int> step_start;      // [n_steps + 1] offsets into d_steps
 };
 
 }  // namespace
@@ -47,6 +56,8 @@ struct pfd_ctx {
     int* d_err = nullptr;
     unsigned long long* d_taps = nullptr;   // tap counter of calibration runs
     bool counting = false;
+    float* d_scratch = nullptr;             // sweep candidate costs, per resident CTA
+    size_t scratch_bytes = 0;
     std::string last_error;
 };
 
@@ -86,9 +97,10 @@ struct DeviceGuard {
 
 pfd_status frame_alloc(pfd_ctx* ctx, Frame& f, void** p, size_t bytes)
 {
-    if (ctx->budget && ctx->used + f.bytes + bytes > ctx->budget)
+    const size_t pending = f.registered ? 0 : f.bytes;
+    if (ctx->budget && ctx->used + pending + bytes > ctx->budget)
         return fail(ctx, PFD_ENOMEM, "HBM budget exceeded: %zu in use + %zu requested > %zu",
-                    ctx->used + f.bytes, bytes, ctx->budget);
+                    ctx->used + pending, bytes, ctx->budget);
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -96,6 +108,7 @@ pfd_status frame_alloc(pfd_ctx* ctx, Frame& f, void** p, size_t bytes)
     }
     f.allocs.push_back(*p);
     f.bytes += bytes;
+    if (f.registered) ctx->used += bytes;
     return PFD_OK;
 }
 
@@ -149,6 +162,7 @@ pfd::PmParams make_params(const Frame& f, const pfd_pm_params* p, uint64_t seed)
     P.tile_stride = f.tile_stride;
     P.seed = seed;
     P.tap_counter = nullptr;
+    P.cost_scratch = nullptr;
     return P;
 }
 
@@ -220,6 +234,7 @@ void pfd_destroy(pfd_ctx* ctx)
     ctx->frames.clear();
     cudaFree(ctx->d_err);
     cudaFree(ctx->d_taps);
+    if (ctx->d_scratch) cudaFree(ctx->d_scratch);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -347,8 +362,12 @@ pfd_status pfd_frame_create(pfd_ctx* ctx, int* frame_id, int W, int H, const flo
         frame_release(f);
         return fail(ctx, st, "frame_create: upload failed");
     }
+    f.h_keys.assign(tilekeys, tilekeys + 2 * (size_t)n_views);
+    f.h_nb_ids.assign(nb_ids, nb_ids + (size_t)n_views * max_nb);
+    f.h_nb_counts.assign(nb_counts, nb_counts + n_views);
     const int id = ctx->next_id++;
     ctx->used += f.bytes;
+    f.registered = true;
     ctx->frames.emplace(id, std::move(f));
     *frame_id = id;
     return PFD_OK;
@@ -438,9 +457,29 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
     DeviceGuard g(ctx->device);
     pfd::PmParams P = make_params(*f, params, seed);
     if (ctx->counting) P.tap_counter = ctx->d_taps;
-    if (pfd::sweep_smem_bytes(P, 32, f->has_blur) > 227 * 1024)
+    if (pfd::sweep_smem_bytes(P, 128, f->has_blur) > 227 * 1024)
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
-    CU(pfd::launch_sweep(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, ctx->d_err, ctx->stream));
+    int n_ctas = 0;
+    CU(pfd::sweep_grid(P, f->has_blur, &n_ctas));
+    const size_t need = pfd::sweep_scratch_bytes(P, n_ctas, 1);
+    if (need > ctx->scratch_bytes) {
+        if (ctx->budget && ctx->used - ctx->scratch_bytes + need > ctx->budget)
+            return fail(ctx, PFD_ENOMEM, "HBM budget exceeded by %zu bytes of sweep scratch", need);
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (ctx->d_scratch) cudaFree(ctx->d_scratch);
+        ctx->used -= ctx->scratch_bytes;
+        ctx->d_scratch = nullptr;
+        ctx->scratch_bytes = 0;
+        if (cudaMalloc(&ctx->d_scratch, need) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, PFD_ENOMEM, "cudaMalloc(%zu) for sweep scratch failed", need);
+        }
+        ctx->scratch_bytes = need;
+        ctx->used += need;
+    }
+    P.cost_scratch = ctx->d_scratch;
+    CU(pfd::launch_sweep(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
+                         ctx->stream));
     f->cur ^= 1;
     return PFD_OK;
 }
@@ -523,6 +562,139 @@ pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params
         return fail(ctx, rc, "ncc_costs: %s", cudaGetErrorString(e));
     }
     return check_device_error(ctx);
+}
+
+static pfd::CheckFrame check_frame(const Frame& f, float baseline_unit)
+{
+    pfd::CheckFrame F;
+    F.V = f.V; F.W = f.mi_w; F.H = f.mi_h; F.K = f.K; F.tile_stride = f.tile_stride;
+    F.gray = f.d_gray; F.centers = f.d_centers; F.nb_ids = f.d_nb_ids; F.nb_counts = f.d_nb_counts;
+    F.baseline_unit = baseline_unit;
+    return F;
+}
+
+static pfd_status check_filter_cfg(pfd_ctx* ctx, const pfd_filter_cfg* cfg, float baseline_unit)
+{
+    if (!cfg) return fail(ctx, PFD_EINVAL, "filter config is NULL");
+    if (cfg->max_triplet < 0 || cfg->max_triplet > 32) return fail(ctx, PFD_EINVAL, "max_triplet outside [0, 32]");
+    if (!(baseline_unit > 0.0f)) return fail(ctx, PFD_EINVAL, "baseline_unit must be > 0");
+    return PFD_OK;
+}
+
+// Groups the views into wavefront steps col + c * row such that every
+// neighbour that precedes a view in key order (row, col) lands in an earlier
+// step and every one that follows it in a later step.
+static pfd_status build_steps(pfd_ctx* ctx, Frame& f)
+{
+    if (!f.step_start.empty()) return PFD_OK;
+    const int V = f.V;
+    long long c = 1;
+    for (int v = 0; v < V; ++v) {
+        const int cv = f.h_keys[2 * v], rv = f.h_keys[2 * v + 1];
+        for (int k = 0; k < f.h_nb_counts[v]; ++k) {
+            const int u = f.h_nb_ids[(size_t)v * f.K + k];
+            if (u < 0) continue;
+            const int cu = f.h_keys[2 * u], ru = f.h_keys[2 * u + 1];
+            if (ru == rv) continue;
+            // earlier row: c (rv - ru) > cu - cv; later row: c (ru - rv) > cv - cu
+            const long long num = (ru < rv) ? (long long)cu - cv : (long long)cv - cu;
+            const long long den = (ru < rv) ? (long long)rv - ru : (long long)ru - rv;
+            long long need = (num >= 0) ? num / den + 1 : 1;
+            if (need > c) c = need;
+        }
+    }
+    std::vector<long long> step(V);
+    long long smin = LLONG_MAX, smax = LLONG_MIN;
+    for (int v = 0; v < V; ++v) {
+        step[v] = (long long)f.h_keys[2 * v] + c * (long long)f.h_keys[2 * v + 1];
+        smin = std::min(smin, step[v]);
+        smax = std::max(smax, step[v]);
+    }
+    const long long ns = smax - smin + 1;
+    if (ns > 100000000LL) return fail(ctx, PFD_EINVAL, "tile keys too sparse for the filter schedule");
+    std::vector<int> counts((size_t)ns + 1, 0), order(V);
+    for (int v = 0; v < V; ++v) counts[(size_t)(step[v] - smin) + 1]++;
+    for (size_t i = 1; i < counts.size(); ++i) counts[i] += counts[i - 1];
+    std::vector<int> fill(counts.begin(), counts.end() - 1);
+    for (int v = 0; v < V; ++v) order[fill[(size_t)(step[v] - smin)]++] = v;
+    // compact away empty steps
+    f.step_start.clear();
+    for (size_t s = 0; s + 1 < counts.size(); ++s)
+        if (counts[s + 1] > counts[s]) f.step_start.push_back(counts[s]);
+    f.step_start.push_back(V);
+    void* p = nullptr;
+    pfd_status st = frame_alloc(ctx, f, &p, sizeof(int) * (size_t)V);
+    if (st != PFD_OK) { f.step_start.clear(); return st; }
+    f.d_steps = (int*)p;
+    CU(cudaMemcpyAsync(f.d_steps, order.data(), sizeof(int) * (size_t)V, cudaMemcpyHostToDevice, ctx->stream));
+    return PFD_OK;
+}
+
+pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, float baseline_unit, uint8_t* reason,
+                      long long* stats)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    pfd_status st = check_filter_cfg(ctx, cfg, baseline_unit);
+    if (st != PFD_OK) return st;
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "filter before PatchMatch");
+    DeviceGuard g(ctx->device);
+    if ((st = build_steps(ctx, *f)) != PFD_OK) return st;
+    const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
+    if (!f->d_reason) {
+        void* p = nullptr;
+        if ((st = frame_alloc(ctx, *f, &p, px)) != PFD_OK) return st;
+        f->d_reason = (uint8_t*)p;
+    }
+    pfd::FilterCfg fc;
+    static_assert(sizeof(fc) == sizeof(pfd_filter_cfg), "filter config layouts differ");
+    std::memcpy(&fc, cfg, sizeof(fc));
+    const pfd::CheckFrame F = check_frame(*f, baseline_unit);
+    if (pfd::filter_smem_bytes(F) > 227 * 1024) return fail(ctx, PFD_EINVAL, "filter tile does not fit shared memory");
+    unsigned long long* d_stats = nullptr;
+    CU(cudaMallocAsync((void**)&d_stats, 8 * sizeof(unsigned long long), ctx->stream));
+    CU(cudaMemsetAsync(d_stats, 0, 8 * sizeof(unsigned long long), ctx->stream));
+    const pfd::StateDev& S = f->s[f->cur];
+    for (size_t s = 0; s + 1 < f->step_start.size(); ++s) {
+        const int a = f->step_start[s], b = f->step_start[s + 1];
+        cudaError_t e = pfd::launch_filter_step(F, fc, S, f->d_steps + a, b - a, f->d_reason, d_stats, ctx->stream);
+        if (e != cudaSuccess) { cudaFreeAsync(d_stats, ctx->stream); return fail(ctx, PFD_ECUDA, "filter step: %s", cudaGetErrorString(e)); }
+    }
+    unsigned long long h[8] = {};
+    if (stats) CU(cudaMemcpyAsync(h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    if (reason) CU(cudaMemcpyAsync(reason, f->d_reason, px, cudaMemcpyDeviceToHost, ctx->stream));
+    cudaFreeAsync(d_stats, ctx->stream);
+    if (stats || reason) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (stats) for (int i = 0; i < 8; ++i) stats[i] = (long long)h[i];
+    }
+    return PFD_OK;
+}
+
+pfd_status pfd_reprojection_error(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, float baseline_unit, float* err)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    pfd_status st = check_filter_cfg(ctx, cfg, baseline_unit);
+    if (st != PFD_OK) return st;
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "reprojection error before PatchMatch");
+    DeviceGuard g(ctx->device);
+    const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
+    if (!f->d_err) {
+        void* p = nullptr;
+        if ((st = frame_alloc(ctx, *f, &p, px * sizeof(float))) != PFD_OK) return st;
+        f->d_err = (float*)p;
+    }
+    pfd::FilterCfg fc;
+    std::memcpy(&fc, cfg, sizeof(fc));
+    CU(pfd::launch_reproj(check_frame(*f, baseline_unit), fc, f->s[f->cur], f->d_err, ctx->stream));
+    if (err) {
+        CU(cudaMemcpyAsync(err, f->d_err, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+    }
+    return PFD_OK;
 }
 
 pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane, float* cost, float* disp, uint32_t* sel)

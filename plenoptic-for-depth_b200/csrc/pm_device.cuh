@@ -30,6 +30,7 @@ struct PmParams {
     int tile_stride;        // bytes per micro-image tile in HBM (W*H rounded up to 16)
     uint64_t seed;
     unsigned long long* tap_counter;   // calibration runs only: in-bounds NCC taps evaluated
+    float* cost_scratch;    // sweep: per resident CTA, [9][K][block] candidate costs
 };
 
 struct FrameDev {
@@ -279,35 +280,50 @@ __device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int
     }
     const float rc = T.R[py * W + px];
     const int r = P.radius, inc = P.inc, ntap = P.ntap;
-    int t_row = 0;
-    for (int i = -r; i <= r; i += inc, t_row += ntap) {
-        const int xr = px + i;
-        const bool rowok = (unsigned)xr < (unsigned)W;
+    // Taps are visited by absolute window position (X, Y), X outer, Y inner,
+    // over the union of the warp's patches.  Each lane keeps only positions
+    // inside its own patch, so it accumulates its taps in exactly the
+    // reference order (x offset outer, y offset inner), while the warp's lanes
+    // see nearly the same source-window validity and read the same texels.
+    bool any_ok = false;
+#pragma unroll
+    for (int c = 0; c < KCH; ++c) any_ok |= okc[c];
+    const int x_lo = max(0, __reduce_min_sync(kFullMask, any_ok ? px : W) - r);
+    const int x_hi = min(W - 1, (int)__reduce_max_sync(kFullMask, any_ok ? px : -r - 1) + r);
+    const int y_lo = max(0, __reduce_min_sync(kFullMask, any_ok ? py : H) - r);
+    const int y_hi = min(H - 1, (int)__reduce_max_sync(kFullMask, any_ok ? py : -r - 1) + r);
+    for (int X = x_lo; X <= x_hi; ++X) {
+        const int i = X - px;
+        const bool rowok = any_ok && i >= -r && i <= r && (inc == 1 || (i + r) % inc == 0);
         if (!__any_sync(kFullMask, rowok)) continue;
-        const int xrc = min(max(xr, 0), W - 1);
-        const float fxr = (float)xr;
+        const int xr = X, xrc = X;
+        const float fxr = (float)X;
         const float axr = __fmul_rn(dp.x, fxr);
-        int t = t_row;
-        float fyr = (float)(py - r);
-        for (int j = -r; j <= r; j += inc, ++t, fyr = __fadd_rn(fyr, (float)inc)) {
-            const int yr = py + j;
-            const bool refok = rowok && ((unsigned)yr < (unsigned)H);
+        const int ii = (inc == 1) ? (i + r) : (i + r) / inc;
+        float fyr = (float)y_lo;
+        for (int Y = y_lo; Y <= y_hi; ++Y, fyr = __fadd_rn(fyr, 1.0f)) {
+            const int j = Y - py;
+            const bool refok = rowok && j >= -r && j <= r && (inc == 1 || (j + r) % inc == 0);
             if (!__any_sync(kFullMask, refok)) continue;
-            const int yrc = min(max(yr, 0), H - 1);
-            const float rv = T.R[yrc * W + xrc];
+            const int t = refok ? ii * ntap + ((inc == 1) ? (j + r) : (j + r) / inc) : 0;
+            const int yrc = Y;
+            const float rv = T.R[Y * W + X];
             const float cd = fabsf(__fsub_rn(rv, rc));
             const int cdi = __float_as_int(__fadd_rn(cd, 8388608.0f)) & 0xFF;
             const float w = refok ? pfd_expf_nonpos(__fsub_rn(T.a_s[t], T.a_c[cdi])) : 0.0f;
             const float wr = __fmul_rn(w, rv);
             const float d = __fadd_rn(__fmaf_rn(dp.y, fyr, axr), dp.z);
+            (void)xr;
             float rb = 0.0f;
             if (BLUR) rb = __fdiv_rn(T.RB[yrc * W + xrc], 255.0f);
 #pragma unroll
             for (int c = 0; c < KCH; ++c) {
                 const float sx = __fmaf_rn(stx[c], d, fxr);
                 const float sy = __fmaf_rn(sty[c], d, fyr);
-                const bool v = okc[c] && (__float_as_uint(sx) < P.W_bits) && (__float_as_uint(sy) < P.H_bits);
-                if (COUNT) ntaps += (v && refok) ? 1u : 0u;
+                const bool v = okc[c] && refok && (__float_as_uint(sx) < P.W_bits) && (__float_as_uint(sy) < P.H_bits);
+                // a tap that no lane of the warp keeps for this neighbour is skipped whole
+                if (!__any_sync(kFullMask, v)) continue;
+                if (COUNT) ntaps += v ? 1u : 0u;
                 const int tbx = tex_coord_bits(sx), tby = tex_coord_bits(sy);
                 const uint32_t rel = (uint32_t)(((tby >> 8) * S + (tbx >> 8)) << 3);
                 const uint32_t addr = v ? base[c] + rel : T.q_addr;
@@ -326,9 +342,8 @@ __device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int
                     const uint32_t baddr = v ? bbase[c] + rel : T.qb_addr;
                     const int2 b0 = lds_int2(baddr), b1 = lds_int2(baddr + (uint32_t)S * 8u);
                     const float sb = tex_blend(tbx, tby, b0, b1);
-                    const bool vr = v && refok;       // blur sums skip taps outside either window
-                    bsx[c] = __fadd_rn(bsx[c], vr ? rb : 0.0f);
-                    bsy[c] = __fadd_rn(bsy[c], vr ? __fdiv_rn(sb, 255.0f) : 0.0f);
+                    bsx[c] = __fadd_rn(bsx[c], v ? rb : 0.0f);
+                    bsy[c] = __fadd_rn(bsy[c], v ? __fdiv_rn(sb, 255.0f) : 0.0f);
                 }
             }
         }
@@ -384,25 +399,15 @@ __device__ __noinline__ void cost_vector(const Tiles& T, const PmParams& P, int 
         int ks[16];
         int nks = 0;
 #pragma unroll
-        for (int c = 0; c < 16; ++c) {
+        for (int c = 0; c < 6; ++c) {
             ks[c] = todo ? (__ffs(todo) - 1) : 0;
             if (todo) { ++nks; todo &= todo - 1; }
         }
-        if (nks > 12) {
-            float c16[16];
-            ncc_chunk<16, BLUR, COUNT>(T, P, px, py, dp, ks, nks, okmask, c16, ntaps);
+        if (nks > 4) {
+            float c6[6];
+            ncc_chunk<6, BLUR, COUNT>(T, P, px, py, dp, ks, nks, okmask, c6, ntaps);
 #pragma unroll
-            for (int c = 0; c < 16; ++c) if (c < nks) out[ks[c] * out_stride] = c16[c];
-        } else if (nks > 8) {
-            float c12[12];
-            ncc_chunk<12, BLUR, COUNT>(T, P, px, py, dp, ks, nks, okmask, c12, ntaps);
-#pragma unroll
-            for (int c = 0; c < 12; ++c) if (c < nks) out[ks[c] * out_stride] = c12[c];
-        } else if (nks > 4) {
-            float c8[8];
-            ncc_chunk<8, BLUR, COUNT>(T, P, px, py, dp, ks, nks, okmask, c8, ntaps);
-#pragma unroll
-            for (int c = 0; c < 8; ++c) if (c < nks) out[ks[c] * out_stride] = c8[c];
+            for (int c = 0; c < 6; ++c) if (c < nks) out[ks[c] * out_stride] = c6[c];
         } else {
             float c4[4];
             ncc_chunk<4, BLUR, COUNT>(T, P, px, py, dp, ks, nks, okmask, c4, ntaps);
