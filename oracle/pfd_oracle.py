@@ -30,6 +30,14 @@ class OrcParams(ctypes.Structure):
                 ("sigma_spatial", _F), ("sigma_color", _F), ("depth_min", _F), ("depth_max", _F), ("base", _F)]
 
 
+class OrcFilterCfg(ctypes.Structure):
+    _fields_ = [("max_triplet", _I), ("min_valid_disp", _F), ("use_selected_views_only", _I),
+                ("clear_selected_views_when_invalid", _I), ("enable_cost_filter", _I), ("max_cost", _F),
+                ("enable_cycle_geo_filter", _I), ("max_geo_err_px", _F), ("enable_cycle_photo_filter", _I),
+                ("max_photo_err_u", _F), ("min_good_neighbors", _I), ("enable_spike_filter", _I),
+                ("spike_abs_diff", _F), ("spike_min_neighbors", _I)]
+
+
 class OrcState(ctypes.Structure):
     _fields_ = [("plane", _P), ("cost", _P), ("disp", _P), ("sel", _P)]
 
@@ -69,6 +77,9 @@ def lib() -> ctypes.CDLL:
         L.orc_tex_fetch.argtypes = [_P, _I, _I, _F, _F]
         L.orc_tex_fetch.restype = _F
         L.orc_philox.argtypes = [_P, _P, _P]
+        CP = ctypes.POINTER(OrcFilterCfg)
+        L.orc_filter_global.argtypes = [FP, CP, _F, SP, _P, _P]
+        L.orc_reprojection_error.argtypes = [FP, CP, _F, SP, _P]
         _lib = L
     return _lib
 
@@ -159,6 +170,37 @@ class Oracle:
         p = self.params(params)
         assert lib().orc_patchmatch(ctypes.byref(self.f), ctypes.byref(p), seed, ctypes.byref(st), nthreads) == 0
         return arr
+
+
+def _fcfg(cfg) -> OrcFilterCfg:
+    c = cfg.c()
+    return OrcFilterCfg(*[getattr(c, n) for n, _ in OrcFilterCfg._fields_])
+
+
+def _state_struct(arr):
+    return OrcState(_p(arr["plane"]), _p(arr["cost"]), _p(arr["disp"]), _p(arr["sel"]))
+
+
+def filter_global(orc: "Oracle", cfg, baseline_unit: float, state: dict):
+    """MIDisparityFilterCPU::FilterGlobal on `state` (modified in place).
+    Returns (reason map, stats array of 8 counters)."""
+    n = orc.V * orc.h * orc.w
+    reason = np.zeros(n, np.uint8)
+    stats = np.zeros(8, np.int64)
+    st = _state_struct(state)
+    c = _fcfg(cfg)
+    assert lib().orc_filter_global(ctypes.byref(orc.f), ctypes.byref(c), float(baseline_unit), ctypes.byref(st),
+                                   _p(reason), _p(stats)) == 0
+    return reason, stats
+
+
+def reprojection_error(orc: "Oracle", cfg, baseline_unit: float, state: dict) -> np.ndarray:
+    err = np.zeros(orc.V * orc.h * orc.w, np.float32)
+    st = _state_struct(state)
+    c = _fcfg(cfg)
+    assert lib().orc_reprojection_error(ctypes.byref(orc.f), ctypes.byref(c), float(baseline_unit), ctypes.byref(st),
+                                        _p(err)) == 0
+    return err
 
 
 def expf(x: float) -> float:

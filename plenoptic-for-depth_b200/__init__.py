@@ -59,6 +59,45 @@ class PmParams:
                          self.sigma_spatial, self.sigma_color, self.depth_min, dmax, self.base)
 
 
+class FilterCfgC(ctypes.Structure):
+    _fields_ = [("max_triplet", ctypes.c_int), ("min_valid_disp", ctypes.c_float),
+                ("use_selected_views_only", ctypes.c_int), ("clear_selected_views_when_invalid", ctypes.c_int),
+                ("enable_cost_filter", ctypes.c_int), ("max_cost", ctypes.c_float),
+                ("enable_cycle_geo_filter", ctypes.c_int), ("max_geo_err_px", ctypes.c_float),
+                ("enable_cycle_photo_filter", ctypes.c_int), ("max_photo_err_u", ctypes.c_float),
+                ("min_good_neighbors", ctypes.c_int), ("enable_spike_filter", ctypes.c_int),
+                ("spike_abs_diff", ctypes.c_float), ("spike_min_neighbors", ctypes.c_int)]
+
+
+@dataclass
+class FilterCfg:
+    """MIDisparityFilterConfig with the values of MIStereoMatch::FilterAndStatic
+    (MIStereoMatch.cpp:759-778)."""
+    max_triplet: int = 4
+    min_valid_disp: float = 0.0
+    use_selected_views_only: bool = True
+    clear_selected_views_when_invalid: bool = True
+    enable_cost_filter: bool = True
+    max_cost: float = 1.8
+    enable_cycle_geo_filter: bool = True
+    max_geo_err_px: float = 0.5
+    enable_cycle_photo_filter: bool = True
+    max_photo_err_u: float = 0.5
+    min_good_neighbors: int = 2
+    enable_spike_filter: bool = True
+    spike_abs_diff: float = 1.0
+    spike_min_neighbors: int = 3
+
+    def c(self) -> FilterCfgC:
+        return FilterCfgC(self.max_triplet, self.min_valid_disp, int(self.use_selected_views_only),
+                          int(self.clear_selected_views_when_invalid), int(self.enable_cost_filter), self.max_cost,
+                          int(self.enable_cycle_geo_filter), self.max_geo_err_px, int(self.enable_cycle_photo_filter),
+                          self.max_photo_err_u, self.min_good_neighbors, int(self.enable_spike_filter),
+                          self.spike_abs_diff, self.spike_min_neighbors)
+
+
+FILTER_STATS = ("total", "valid_in", "kept", "removed", "by_cost", "by_no_support", "by_cycle", "by_spike")
+
 _lib = None
 _synth = None
 
@@ -95,6 +134,8 @@ def lib() -> ctypes.CDLL:
             "pfd_set_tap_counting": [_P, _I],
             "pfd_read_tap_count": [_P, ctypes.POINTER(ctypes.c_ulonglong)],
             "pfd_fp32_fma_rate": [_P, ctypes.POINTER(ctypes.c_double)],
+            "pfd_filter": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P, _P],
+            "pfd_reprojection_error": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -238,6 +279,25 @@ class Context:
         v = ctypes.c_double()
         self._check(self._L.pfd_fp32_fma_rate(self._h, ctypes.byref(v)), "pfd_fp32_fma_rate")
         return v.value
+
+    def filter(self, fid: int, cfg: FilterCfg, baseline_unit: float):
+        """MIDisparityFilterCPU::FilterGlobal on the frame's state, in place.
+        Returns (reason map [V*mi*mi] uint8, stats dict)."""
+        f = self._frames[fid]
+        reason = np.empty(f["V"] * f["mi_w"] * f["mi_h"], np.uint8)
+        stats = np.zeros(8, np.int64)
+        c = cfg.c()
+        self._check(self._L.pfd_filter(self._h, fid, ctypes.byref(c), float(baseline_unit), _ptr(reason), _ptr(stats)),
+                    "pfd_filter")
+        return reason, dict(zip(FILTER_STATS, (int(x) for x in stats)))
+
+    def reprojection_error(self, fid: int, cfg: FilterCfg, baseline_unit: float) -> np.ndarray:
+        f = self._frames[fid]
+        err = np.empty(f["V"] * f["mi_w"] * f["mi_h"], np.float32)
+        c = cfg.c()
+        self._check(self._L.pfd_reprojection_error(self._h, fid, ctypes.byref(c), float(baseline_unit), _ptr(err)),
+                    "pfd_reprojection_error")
+        return err
 
     def download(self, fid: int):
         f = self._frames[fid]
