@@ -124,6 +124,22 @@ pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* param
 pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed);
 pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed,
                         int iter, int phase);
+/* pfd_pm_sweep without any device allocation; no counterpart in the reference.
+ * For callers that cannot allocate device memory once frames are streaming: an
+ * application whose memory pool claimed all free HBM at start-up, or a
+ * real-time loop that forbids cudaMalloc/cudaFree because they can synchronise
+ * the whole device.  The candidate-cost scratch is a fixed 16 MiB array in the
+ * library's device image (held by every GPU that loads the library, until
+ * exit) instead of a cudaMalloc'd buffer; inputs and outputs are the frame's
+ * state exactly as for pfd_pm_sweep, and the results are the same bit for bit.
+ * Limit: the array must hold one CTA's scratch (9 x max_nb x 128 floats) for
+ * every SM, so max_nb <= 24 on a 148-SM B200; larger frames get PFD_EINVAL.
+ * The first call on a device looks up the array's device address, so make
+ * that call before any stream capture.  All calls on a device share the one
+ * array (nothing in it has to start at zero): calls whose kernels overlap on
+ * the GPU, from other streams or other contexts, race and corrupt each other. */
+pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed,
+                                int iter, int phase);
 
 /* Per-hypothesis cost vectors: ComputeMultiViewCostVector_Frame
  * (AdaptMIPMFrame.cu:181-225) for n (view, pixel, plane) hypotheses.

@@ -128,6 +128,7 @@ def lib() -> ctypes.CDLL:
             "pfd_patchmatch": [_P, _I, ctypes.POINTER(PmParamsC), ctypes.c_uint64],
             "pfd_pm_init": [_P, _I, ctypes.POINTER(PmParamsC), ctypes.c_uint64],
             "pfd_pm_sweep": [_P, _I, ctypes.POINTER(PmParamsC), ctypes.c_uint64, _I, _I],
+            "pfd_pm_sweep_noalloc": [_P, _I, ctypes.POINTER(PmParamsC), ctypes.c_uint64, _I, _I],
             "pfd_ncc_costs": [_P, _I, ctypes.POINTER(PmParamsC), _P, _P, _P, _I, _P],
             "pfd_download": [_P, _I, _P, _P, _P, _P],
             "pfd_neighbors_by_baseline": [_P, _P, _I, _F, _I, _I, _P, _P],
@@ -255,6 +256,13 @@ class Context:
     def pm_sweep(self, fid: int, params: PmParams, seed: int, it: int, phase: int) -> None:
         p = params.c()
         self._check(self._L.pfd_pm_sweep(self._h, fid, ctypes.byref(p), seed, it, phase), "pfd_pm_sweep")
+
+    def pm_sweep_noalloc(self, fid: int, params: PmParams, seed: int, it: int, phase: int) -> None:
+        """pfd_pm_sweep on the library's fixed scratch array: for callers that may
+        not allocate device memory while frames stream (max_nb <= 24 on B200)."""
+        p = params.c()
+        self._check(self._L.pfd_pm_sweep_noalloc(self._h, fid, ctypes.byref(p), seed, it, phase),
+                    "pfd_pm_sweep_noalloc")
 
     def ncc_costs(self, fid: int, params: PmParams, vids, pxy, planes) -> np.ndarray:
         v = np.ascontiguousarray(vids, dtype=np.int32)

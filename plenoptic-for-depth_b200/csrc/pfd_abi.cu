@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -714,3 +715,90 @@ pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane, float* cost, f
 }
 
 }  // extern "C"
+
+// ---- PatchMatch sweep without allocation --------------------------------------
+//
+// pfd_pm_sweep takes its candidate-cost scratch from cudaMalloc, grown on the
+// first sweep of a larger grid.  Some callers cannot allocate device memory
+// once frames are streaming: an application whose memory pool claimed all free
+// HBM at start-up (a cudaMalloc then fails, or takes memory the pool counts
+// on), or a real-time camera loop that forbids cudaMalloc/cudaFree because they
+// can synchronise the whole device and stall its other streams.
+// pfd_pm_sweep_noalloc runs the same kernel on a fixed array that is part of
+// the library's device image instead.
+
+// 16 MiB, held by every GPU that loads the library until the process exits.
+// One CTA uses 9 x max_nb x 128 floats; the array must hold at least one CTA
+// per SM, so max_nb <= 24 on a 148-SM B200.  Nothing in it needs to start at
+// zero: a sweep writes every entry it reads, earlier in the same work item.
+static __device__ __align__(256) float g_noalloc_scratch[(size_t(16) << 20) / sizeof(float)];
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = sizeof(g_noalloc_scratch);
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `dev`, which must be the current
+// device.  In host code the array's name stands for a host-side shadow, so the
+// kernel gets the address from cudaGetSymbolAddress, looked up once per device.
+pfd_status noalloc_scratch(pfd_ctx* ctx, int dev, float** out)
+{
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(ctx, PFD_EINVAL, "pfd_pm_sweep_noalloc: device %d outside [0, %d)", dev, kNoAllocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        float* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return fail(ctx, PFD_ECUDA, "pfd_pm_sweep_noalloc: cudaGetSymbolAddress of the scratch array: %s",
+                        cudaGetErrorString(e));
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return PFD_OK;
+}
+
+}  // namespace
+
+extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed,
+                                           int iter, int phase)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    pfd_status st = check_params(ctx, *f, params);
+    if (st != PFD_OK) return st;
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "sweep before pfd_pm_init");
+    if (phase != 0 && phase != 1) return fail(ctx, PFD_EINVAL, "phase must be 0 or 1");
+    if (iter < 0) return fail(ctx, PFD_EINVAL, "iter must be >= 0");
+    DeviceGuard g(ctx->device);
+    pfd::PmParams P = make_params(*f, params, seed);
+    if (ctx->counting) P.tap_counter = ctx->d_taps;
+    if (pfd::sweep_smem_bytes(P, 128, f->has_blur) > 227 * 1024)
+        return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
+    int sms = 0;
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    const size_t per_cta = pfd::sweep_scratch_bytes(P, 1, 1);
+    const size_t fit = kNoAllocScratchBytes / per_cta;
+    if (fit < (size_t)sms)
+        return fail(ctx, PFD_EINVAL,
+                    "pfd_pm_sweep_noalloc: %d neighbours need %zu bytes of scratch per CTA; the fixed %zu-byte "
+                    "scratch holds %zu CTAs, fewer than the %d SMs (at most %zu neighbours on this device)",
+                    f->K, per_cta, kNoAllocScratchBytes, fit, sms,
+                    kNoAllocScratchBytes / ((size_t)sms * (per_cta / (size_t)f->K)));
+    int n_ctas = 0;
+    CU(pfd::sweep_grid(P, f->has_blur, &n_ctas));
+    n_ctas = (int)std::min<size_t>((size_t)n_ctas, fit);
+    float* scratch = nullptr;
+    st = noalloc_scratch(ctx, ctx->device, &scratch);
+    if (st != PFD_OK) return st;
+    P.cost_scratch = scratch;
+    CU(pfd::launch_sweep(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
+                         ctx->stream));
+    f->cur ^= 1;
+    return PFD_OK;
+}

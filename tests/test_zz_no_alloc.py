@@ -1,0 +1,70 @@
+"""pfd_pm_sweep_noalloc: the PatchMatch half-sweep on the library's fixed scratch
+array, for callers that may not allocate device memory once frames stream (an
+application whose memory pool owns all free HBM, or a real-time loop in which
+cudaMalloc/cudaFree, which can synchronise the device, are forbidden).
+
+Its results must equal pfd_pm_sweep's bit for bit, the tolerance of every sweep
+parity test here, on two calls in a row: the second call finds the first one's
+leftovers in the shared array.  This file is collected last on purpose.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.dtype.kind == "f":
+        return bool(np.all((a == b) | (np.isnan(a) & np.isnan(b))))
+    return bool(np.array_equal(a, b))
+
+
+def _upload(ctx, w, blur=None):
+    return ctx.frame_upload(w.frame.raw, w.centers, w.tilekeys, w.mi, w.mi, w.nb_ids, w.nb_counts, blur=blur)
+
+
+@pytest.mark.parametrize("pitch,K,patch,blur", [(23.2, 12, 15, False), (23.0, 6, 11, True)])
+def test_noalloc_sweep_matches_pfd_pm_sweep(pfd, pitch, K, patch, blur):
+    w = pfd.make_workload(260, 200, pitch, 4, seed=5, max_nb=K)
+    bl = None
+    if blur:
+        rs = np.random.RandomState(K)
+        bl = rs.randint(0, 256, size=(w.centers.shape[0], w.mi, w.mi)).astype(np.uint8)
+    P = pfd.PmParams(base=pitch, patch_size=patch, max_iterations=1)
+    seed = 41
+    with pfd.Context(0) as ctx:
+        fa = _upload(ctx, w, bl)          # pfd_pm_sweep (cudaMalloc'd scratch)
+        fb = _upload(ctx, w, bl)          # pfd_pm_sweep_noalloc (fixed scratch)
+        ctx.pm_init(fa, P, seed)
+        ctx.pm_init(fb, P, seed)
+        for phase in (0, 1):
+            ctx.pm_sweep(fa, P, seed, 0, phase)
+            ctx.pm_sweep_noalloc(fb, P, seed, 0, phase)
+            a = ctx.download(fa)
+            b = ctx.download(fb)
+            for name, x, y in zip(("plane", "cost", "disp", "sel"), a, b):
+                assert _same(x, y), f"call {phase + 1}: {name} differs at {np.count_nonzero(x != y)} entries"
+        assert np.mean(a[1] < 2.0) > 0.3, "too few valid costs for a meaningful comparison"
+        ctx.frame_free(fa)
+        ctx.frame_free(fb)
+
+
+def test_noalloc_sweep_rejects_too_many_neighbours(pfd):
+    """32 neighbours need 147 KB of scratch per CTA: the 16 MiB array cannot
+    give every SM one CTA, so the call fails before launching anything."""
+    w = pfd.make_workload(260, 200, 23.0, 4, seed=5, max_nb=32)
+    P = pfd.PmParams(base=23.0, patch_size=11, max_iterations=1)
+    with pfd.Context(0) as ctx:
+        fid = ctx.frame_create(260, 200, w.centers, w.tilekeys, w.mi, w.mi, w.nb_ids, w.nb_counts)
+        ctx.frame_set_raw(fid, w.frame.raw)
+        ctx.pm_init(fid, P, 1)
+        before = ctx.download(fid)
+        with pytest.raises(pfd.PfdError) as e:
+            ctx.pm_sweep_noalloc(fid, P, 1, 0, 0)
+        assert e.value.code == -1
+        assert "scratch" in str(e.value)
+        after = ctx.download(fid)
+        assert all(_same(x, y) for x, y in zip(before, after))
+        ctx.frame_free(fid)
