@@ -201,6 +201,48 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
 pfd_status pfd_reprojection_error(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, float baseline_unit,
                                   float* err);
 
+/* MICycleClampConfig (CheckModule/MICycleCheck.h:54-78) and the texture-mask
+ * parameters MICycleMaskParams (:44-50).  The reference's doubles are floats
+ * here (every use casts them to float); bools are ints. */
+typedef struct pfd_cycle_cfg {
+    int   max_triplet;              /* selected views checked per pixel (CheckGlobal argument, 4) */
+    int   clamp_photo;              /* 1 */
+    float photo_u;                  /* 3.0 */
+    int   clamp_geo;                /* 1 in MIStereoMatch.cpp:571 */
+    float geo_u_px;                 /* 2.0 */
+    int   pixel_gate_enabled;       /* 0 */
+    int   gate_min_good_neighbors;  /* 2 */
+    float gate_geo_px;              /* 0.5 */
+    float gate_photo_u;             /* 0.5 */
+    int   gate_use_clamped;         /* 0 */
+    float sobel_thresh;             /* 8.0 (fixed in CheckTile, MICycleCheck.cpp:317-322) */
+    float var_thresh;               /* 60.0 */
+    int   use_and;                  /* 1 */
+} pfd_cycle_cfg;
+
+/* MICycleCheckStats (MICycleCheck.h:24-42) followed by the texture-masked
+ * figures CheckGlobal logs (MICycleCheck.cpp:834-880). */
+typedef struct pfd_cycle_stats {
+    double    mean_geo_err_px, median_geo_err_px, p90_geo_err_px, mean_photo_err;
+    long long num_samples;
+    double    rmse_geo_err_px, rmse_photo_err;
+    double    completeness, completeness_geo, completeness_photo;
+    long long completeness_masked_pixels, completeness_good_pixels, completeness_good_pixels_geo,
+              completeness_good_pixels_photo;
+    long long masked_count, all_count;
+    double    masked_geo_mean, masked_photo_mean, masked_geo_rmse, masked_photo_rmse, coverage;
+    double    masked_geo_median_approx, masked_geo_p90_approx, masked_geo_min, masked_geo_max;
+} pfd_cycle_stats;
+
+/* MICycleCheckerCPU::CheckGlobal (MICycleCheck.cpp:727-893, tiles by CheckTile
+ * :282-725) on the frame's current state; read-only.  stats receives the
+ * global figures, folded over the views in key order as the reference does.
+ * geo_err / pho_err (host float [V*mi_w*mi_h]) receive the per-pixel maximum
+ * geometric and photometric errors, texmask (host u8) the 0/255 texture mask;
+ * each may be NULL. */
+pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg, float baseline_unit,
+                           pfd_cycle_stats* stats, float* geo_err, float* pho_err, uint8_t* texmask);
+
 /* ---- measurement --------------------------------------------------------
  * No counterpart in the reference (it has no timers or counters on this path,
  * see its Util/Logger only).  Tap counting switches the PatchMatch kernels to

@@ -129,6 +129,53 @@ int orc_filter_global(const orc_frame* f, const orc_filter_cfg* cfg, float basel
 int orc_reprojection_error(const orc_frame* f, const orc_filter_cfg* cfg, float baseline_unit, const orc_state* st,
                            float* err);
 
+/* MICycleClampConfig (MICycleCheck.h:54-78) and MICycleMaskParams (:44-50);
+ * doubles of the reference become floats here because every use casts them
+ * to float first. */
+typedef struct orc_cycle_cfg {
+    int   max_triplet;
+    int   clamp_photo;
+    float photo_u;
+    int   clamp_geo;
+    float geo_u_px;
+    int   pixel_gate_enabled;
+    int   gate_min_good_neighbors;
+    float gate_geo_px;
+    float gate_photo_u;
+    int   gate_use_clamped;
+    float sobel_thresh;
+    float var_thresh;
+    int   use_and;
+} orc_cycle_cfg;
+
+/* MICycleCheckStats (MICycleCheck.h:24-42) plus the texture-masked figures that
+ * CheckGlobal logs (MICycleCheck.cpp:805-880). */
+typedef struct orc_cycle_stats {
+    double  mean_geo_err_px, median_geo_err_px, p90_geo_err_px, mean_photo_err;
+    long long num_samples;
+    double  rmse_geo_err_px, rmse_photo_err;
+    double  completeness, completeness_geo, completeness_photo;
+    long long completeness_masked_pixels, completeness_good_pixels, completeness_good_pixels_geo,
+              completeness_good_pixels_photo;
+    long long masked_count, all_count;
+    double  masked_geo_mean, masked_photo_mean, masked_geo_rmse, masked_photo_rmse, coverage;
+    double  masked_geo_median_approx, masked_geo_p90_approx, masked_geo_min, masked_geo_max;
+} orc_cycle_stats;
+
+/* BuildTextureMaskAndViz (MICycleCheck.cpp:186-213) on one W x H float image:
+ * Sobel magnitude, 7x7 variance (reflect-101 borders) and the 0/255 mask. */
+int orc_texture_mask(const float* gray, int W, int H, const orc_cycle_cfg* cfg, float* grad, float* var,
+                     uint8_t* mask);
+
+/* MICycleCheckerCPU::CheckGlobal (MICycleCheck.cpp:727-893) with CheckTile
+ * (:282-725): read-only.  geo_err / pho_err / texmask ([V*mi_w*mi_h], each
+ * nullable) receive the per-tile maps. */
+int orc_cycle_check(const orc_frame* f, const orc_cycle_cfg* cfg, float baseline_unit, const orc_state* st,
+                    orc_cycle_stats* out, float* geo_err, float* pho_err, uint8_t* texmask);
+
+/* cv::meanStdDev of the 3x3 window with top-left (x0, y0) (test hook). */
+void orc_mean_std_3x3(const float* img, int W, int x0, int y0, float* mean, float* stdv);
+
 /* Scalar hooks for unit tests of the canonical arithmetic. */
 float orc_expf(float x);
 float orc_uniform(uint64_t seed, uint32_t sweep, uint32_t pixel, uint32_t n);

@@ -38,6 +38,27 @@ class OrcFilterCfg(ctypes.Structure):
                 ("spike_abs_diff", _F), ("spike_min_neighbors", _I)]
 
 
+class OrcCycleCfg(ctypes.Structure):
+    _fields_ = [("max_triplet", _I), ("clamp_photo", _I), ("photo_u", _F), ("clamp_geo", _I), ("geo_u_px", _F),
+                ("pixel_gate_enabled", _I), ("gate_min_good_neighbors", _I), ("gate_geo_px", _F),
+                ("gate_photo_u", _F), ("gate_use_clamped", _I), ("sobel_thresh", _F), ("var_thresh", _F),
+                ("use_and", _I)]
+
+
+CYCLE_STAT_FIELDS = ["mean_geo_err_px", "median_geo_err_px", "p90_geo_err_px", "mean_photo_err", "num_samples",
+                     "rmse_geo_err_px", "rmse_photo_err", "completeness", "completeness_geo", "completeness_photo",
+                     "completeness_masked_pixels", "completeness_good_pixels", "completeness_good_pixels_geo",
+                     "completeness_good_pixels_photo", "masked_count", "all_count", "masked_geo_mean",
+                     "masked_photo_mean", "masked_geo_rmse", "masked_photo_rmse", "coverage",
+                     "masked_geo_median_approx", "masked_geo_p90_approx", "masked_geo_min", "masked_geo_max"]
+_INT_STATS = {"num_samples", "completeness_masked_pixels", "completeness_good_pixels", "completeness_good_pixels_geo",
+              "completeness_good_pixels_photo", "masked_count", "all_count"}
+
+
+class OrcCycleStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_longlong if n in _INT_STATS else ctypes.c_double) for n in CYCLE_STAT_FIELDS]
+
+
 class OrcState(ctypes.Structure):
     _fields_ = [("plane", _P), ("cost", _P), ("disp", _P), ("sel", _P)]
 
@@ -80,6 +101,10 @@ def lib() -> ctypes.CDLL:
         CP = ctypes.POINTER(OrcFilterCfg)
         L.orc_filter_global.argtypes = [FP, CP, _F, SP, _P, _P]
         L.orc_reprojection_error.argtypes = [FP, CP, _F, SP, _P]
+        YP = ctypes.POINTER(OrcCycleCfg)
+        L.orc_texture_mask.argtypes = [_P, _I, _I, YP, _P, _P, _P]
+        L.orc_cycle_check.argtypes = [FP, YP, _F, SP, ctypes.POINTER(OrcCycleStats), _P, _P, _P]
+        L.orc_mean_std_3x3.argtypes = [_P, _I, _I, _I, _P, _P]
         _lib = L
     return _lib
 
@@ -201,6 +226,45 @@ def reprojection_error(orc: "Oracle", cfg, baseline_unit: float, state: dict) ->
     assert lib().orc_reprojection_error(ctypes.byref(orc.f), ctypes.byref(c), float(baseline_unit), ctypes.byref(st),
                                         _p(err)) == 0
     return err
+
+
+def _ycfg(cfg) -> OrcCycleCfg:
+    c = cfg.c()
+    return OrcCycleCfg(*[getattr(c, n) for n, _ in OrcCycleCfg._fields_])
+
+
+def texture_mask(gray, cfg):
+    """BuildTextureMaskAndViz on one float image: (grad magnitude, 7x7 var, mask)."""
+    g = np.ascontiguousarray(gray, np.float32)
+    H, W = g.shape
+    grad = np.zeros_like(g)
+    var = np.zeros_like(g)
+    mask = np.zeros(g.shape, np.uint8)
+    c = _ycfg(cfg)
+    assert lib().orc_texture_mask(_p(g), W, H, ctypes.byref(c), _p(grad), _p(var), _p(mask)) == 0
+    return grad, var, mask
+
+
+def cycle_check(orc: "Oracle", cfg, baseline_unit: float, state: dict):
+    """MICycleCheckerCPU::CheckGlobal: (stats dict, geo_err, pho_err, texture mask)."""
+    n = orc.V * orc.h * orc.w
+    geo = np.zeros(n, np.float32)
+    pho = np.zeros(n, np.float32)
+    tm = np.zeros(n, np.uint8)
+    st = _state_struct(state)
+    out = OrcCycleStats()
+    c = _ycfg(cfg)
+    assert lib().orc_cycle_check(ctypes.byref(orc.f), ctypes.byref(c), float(baseline_unit), ctypes.byref(st),
+                                 ctypes.byref(out), _p(geo), _p(pho), _p(tm)) == 0
+    return {k: getattr(out, k) for k in CYCLE_STAT_FIELDS}, geo, pho, tm
+
+
+def mean_std_3x3(img, x0: int, y0: int):
+    a = np.ascontiguousarray(img, np.float32)
+    m = np.zeros(1, np.float32)
+    s = np.zeros(1, np.float32)
+    lib().orc_mean_std_3x3(_p(a), a.shape[1], x0, y0, _p(m), _p(s))
+    return float(m[0]), float(s[0])
 
 
 def expf(x: float) -> float:

@@ -96,6 +96,54 @@ class FilterCfg:
                           self.spike_abs_diff, self.spike_min_neighbors)
 
 
+class CycleCfgC(ctypes.Structure):
+    _fields_ = [("max_triplet", ctypes.c_int), ("clamp_photo", ctypes.c_int), ("photo_u", ctypes.c_float),
+                ("clamp_geo", ctypes.c_int), ("geo_u_px", ctypes.c_float), ("pixel_gate_enabled", ctypes.c_int),
+                ("gate_min_good_neighbors", ctypes.c_int), ("gate_geo_px", ctypes.c_float),
+                ("gate_photo_u", ctypes.c_float), ("gate_use_clamped", ctypes.c_int),
+                ("sobel_thresh", ctypes.c_float), ("var_thresh", ctypes.c_float), ("use_and", ctypes.c_int)]
+
+
+@dataclass
+class CycleCfg:
+    """MICycleClampConfig + MICycleMaskParams with the values of the call in
+    MIStereoMatch::StereoMatchingForMIA_SoftProxyRepair (MIStereoMatch.cpp:565-583)
+    and CheckTile's fixed texture-mask parameters (MICycleCheck.cpp:317-322)."""
+    max_triplet: int = 4
+    clamp_photo: bool = True
+    photo_u: float = 3.0
+    clamp_geo: bool = True
+    geo_u_px: float = 2.0
+    pixel_gate_enabled: bool = False
+    gate_min_good_neighbors: int = 2
+    gate_geo_px: float = 0.5
+    gate_photo_u: float = 0.5
+    gate_use_clamped: bool = False
+    sobel_thresh: float = 8.0
+    var_thresh: float = 60.0
+    use_and: bool = True
+
+    def c(self) -> CycleCfgC:
+        return CycleCfgC(self.max_triplet, int(self.clamp_photo), self.photo_u, int(self.clamp_geo), self.geo_u_px,
+                         int(self.pixel_gate_enabled), self.gate_min_good_neighbors, self.gate_geo_px,
+                         self.gate_photo_u, int(self.gate_use_clamped), self.sobel_thresh, self.var_thresh,
+                         int(self.use_and))
+
+
+CYCLE_STATS = ("mean_geo_err_px", "median_geo_err_px", "p90_geo_err_px", "mean_photo_err", "num_samples",
+               "rmse_geo_err_px", "rmse_photo_err", "completeness", "completeness_geo", "completeness_photo",
+               "completeness_masked_pixels", "completeness_good_pixels", "completeness_good_pixels_geo",
+               "completeness_good_pixels_photo", "masked_count", "all_count", "masked_geo_mean",
+               "masked_photo_mean", "masked_geo_rmse", "masked_photo_rmse", "coverage",
+               "masked_geo_median_approx", "masked_geo_p90_approx", "masked_geo_min", "masked_geo_max")
+_CYCLE_INT = {"num_samples", "completeness_masked_pixels", "completeness_good_pixels",
+              "completeness_good_pixels_geo", "completeness_good_pixels_photo", "masked_count", "all_count"}
+
+
+class CycleStatsC(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_longlong if n in _CYCLE_INT else ctypes.c_double) for n in CYCLE_STATS]
+
+
 FILTER_STATS = ("total", "valid_in", "kept", "removed", "by_cost", "by_no_support", "by_cycle", "by_spike")
 
 _lib = None
@@ -137,6 +185,7 @@ def lib() -> ctypes.CDLL:
             "pfd_fp32_fma_rate": [_P, ctypes.POINTER(ctypes.c_double)],
             "pfd_filter": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P, _P],
             "pfd_reprojection_error": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P],
+            "pfd_cycle_check": [_P, _I, ctypes.POINTER(CycleCfgC), _F, ctypes.POINTER(CycleStatsC), _P, _P, _P],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -298,6 +347,22 @@ class Context:
         self._check(self._L.pfd_filter(self._h, fid, ctypes.byref(c), float(baseline_unit), _ptr(reason), _ptr(stats)),
                     "pfd_filter")
         return reason, dict(zip(FILTER_STATS, (int(x) for x in stats)))
+
+    def cycle_check(self, fid: int, cfg: CycleCfg, baseline_unit: float, maps: bool = True):
+        """MICycleCheckerCPU::CheckGlobal on the frame's state (read-only).
+        Returns (stats dict, geo_err, pho_err, texture mask); maps are None
+        unless maps=True."""
+        f = self._frames[fid]
+        n = f["V"] * f["mi_w"] * f["mi_h"]
+        geo = np.empty(n, np.float32) if maps else None
+        pho = np.empty(n, np.float32) if maps else None
+        tm = np.empty(n, np.uint8) if maps else None
+        out = CycleStatsC()
+        c = cfg.c()
+        self._check(self._L.pfd_cycle_check(self._h, fid, ctypes.byref(c), float(baseline_unit), ctypes.byref(out),
+                                            _ptr(geo) if maps else None, _ptr(pho) if maps else None,
+                                            _ptr(tm) if maps else None), "pfd_cycle_check")
+        return {k: getattr(out, k) for k in CYCLE_STATS}, geo, pho, tm
 
     def reprojection_error(self, fid: int, cfg: FilterCfg, baseline_unit: float) -> np.ndarray:
         f = self._frames[fid]

@@ -20,7 +20,7 @@ NVCC = os.environ.get("PFD_NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
     "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
-    "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2", "-ccbin", "/usr/bin/g++",
+    "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "-ccbin", "/usr/bin/g++",
 ]
 
 CU_SOURCES = ["pm_kernels.cu", "check_kernels.cu", "pfd_abi.cu", "diag.cu"]

@@ -44,6 +44,10 @@ struct Frame {
     float* d_err = nullptr;           // reprojection-error map, allocated on first use
     int* d_steps = nullptr;           // views grouped by wavefront step
     std::vector<int> step_start;      // [n_steps + 1] offsets into d_steps
+    pfd::CycleTileRec* d_cyc_recs = nullptr;   // cycle check: per-view sums, allocated on first use
+    unsigned int* d_cyc_hist = nullptr;        // cycle check: masked geometric-error histogram
+    float* d_cyc_maps = nullptr;               // cycle check: geo and photo error maps
+    uint8_t* d_cyc_tm = nullptr;               // cycle check: texture mask
 };
 
 }  // namespace
@@ -695,6 +699,125 @@ pfd_status pfd_reprojection_error(pfd_ctx* ctx, int frame_id, const pfd_filter_c
         CU(cudaMemcpyAsync(err, f->d_err, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
     }
+    return PFD_OK;
+}
+
+pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg, float baseline_unit,
+                           pfd_cycle_stats* stats, float* geo_err, float* pho_err, uint8_t* texmask)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!cfg) return fail(ctx, PFD_EINVAL, "cycle config is NULL");
+    if (cfg->max_triplet < 0 || cfg->max_triplet > 32) return fail(ctx, PFD_EINVAL, "max_triplet outside [0, 32]");
+    if (!(baseline_unit > 0.0f)) return fail(ctx, PFD_EINVAL, "baseline_unit must be > 0");
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "cycle check before PatchMatch");
+    DeviceGuard g(ctx->device);
+    const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
+    pfd_status st;
+    void* p = nullptr;
+    if (!f->d_cyc_recs) {
+        const size_t rec_bytes = sizeof(pfd::CycleTileRec) * (size_t)f->V;
+        if ((st = frame_alloc(ctx, *f, &p, rec_bytes + sizeof(unsigned int) * pfd::kCycleHistBins)) != PFD_OK)
+            return st;
+        f->d_cyc_recs = (pfd::CycleTileRec*)p;
+        f->d_cyc_hist = (unsigned int*)((char*)p + rec_bytes);
+    }
+    const bool maps = geo_err || pho_err || texmask;
+    if (maps && !f->d_cyc_maps) {
+        if ((st = frame_alloc(ctx, *f, &p, 2 * sizeof(float) * px + px)) != PFD_OK) return st;
+        f->d_cyc_maps = (float*)p;
+        f->d_cyc_tm = (uint8_t*)(f->d_cyc_maps + 2 * px);
+    }
+    pfd::CycleCfg cc;
+    static_assert(sizeof(cc) == sizeof(pfd_cycle_cfg), "cycle config layouts differ");
+    std::memcpy(&cc, cfg, sizeof(cc));
+    const pfd::CheckFrame F = check_frame(*f, baseline_unit);
+    if (pfd::cycle_smem_bytes(F) > 227 * 1024) return fail(ctx, PFD_EINVAL, "cycle-check tile does not fit shared memory");
+    CU(cudaMemsetAsync(f->d_cyc_hist, 0, sizeof(unsigned int) * pfd::kCycleHistBins, ctx->stream));
+    CU(pfd::launch_cycle(F, cc, f->s[f->cur], maps ? f->d_cyc_maps : nullptr, maps ? f->d_cyc_maps + px : nullptr,
+                         maps ? f->d_cyc_tm : nullptr, f->d_cyc_recs, f->d_cyc_hist, ctx->stream));
+    std::vector<pfd::CycleTileRec> rec(f->V);
+    unsigned int hist[pfd::kCycleHistBins];
+    CU(cudaMemcpyAsync(rec.data(), f->d_cyc_recs, sizeof(pfd::CycleTileRec) * rec.size(), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaMemcpyAsync(hist, f->d_cyc_hist, sizeof(hist), cudaMemcpyDeviceToHost, ctx->stream));
+    if (geo_err) CU(cudaMemcpyAsync(geo_err, f->d_cyc_maps, sizeof(float) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (pho_err)
+        CU(cudaMemcpyAsync(pho_err, f->d_cyc_maps + px, sizeof(float) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (texmask) CU(cudaMemcpyAsync(texmask, f->d_cyc_tm, px, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if ((st = check_device_error(ctx)) != PFD_OK) return st;
+    if (!stats) return PFD_OK;
+
+    // CheckGlobal's fold over the tiles in key order (MICycleCheck.cpp:541-600, 742-832)
+    pfd_cycle_stats o;
+    std::memset(&o, 0, sizeof(o));
+    double io_mean_geo = 0.0, io_mean_photo = 0.0, io_sq_geo = 0.0, io_sq_photo = 0.0;
+    long long io_num = 0;
+    double m_sq_geo = 0.0, m_sq_photo = 0.0, m_sum_geo = 0.0, m_sum_photo = 0.0;
+    long long m_count = 0, all_count = 0, c_total = 0, c_good = 0, c_geo = 0, c_photo = 0;
+    double geo_min = INFINITY, geo_max = 0.0;
+    for (int v = 0; v < f->V; ++v) {
+        const pfd::CycleTileRec& r = rec[v];
+        if (r.n > 0) {
+            const double mg = r.sum_geo / (double)r.n, mp = r.sum_photo / (double)r.n;
+            const long long N0 = io_num + r.n;
+            const double den = (double)(N0 > 1 ? N0 : 1);
+            io_mean_geo = (io_mean_geo * (double)io_num + mg * (double)r.n) / den;
+            io_mean_photo = (io_mean_photo * (double)io_num + mp * (double)r.n) / den;
+            io_num = N0;
+            io_sq_geo += r.sq_geo;
+            io_sq_photo += r.sq_photo;
+        }
+        m_sq_geo += r.sq_geo_m;
+        m_sq_photo += r.sq_photo_m;
+        m_sum_geo += r.sum_geo_m;
+        m_sum_photo += r.sum_photo_m;
+        c_total += r.comp_total;
+        c_good += r.comp_good;
+        c_geo += r.comp_good_geo;
+        c_photo += r.comp_good_photo;
+        if ((double)r.min_geo_m < geo_min) geo_min = r.min_geo_m;
+        if ((double)r.max_geo_m > geo_max) geo_max = r.max_geo_m;
+        m_count += r.n_masked;
+        all_count += r.n;
+    }
+    o.num_samples = io_num;
+    o.mean_geo_err_px = io_mean_geo;
+    o.mean_photo_err = io_mean_photo;
+    o.completeness = c_total > 0 ? (double)c_good / (double)c_total : 0.0;
+    o.completeness_geo = c_total > 0 ? (double)c_geo / (double)c_total : 0.0;
+    o.completeness_photo = c_total > 0 ? (double)c_photo / (double)c_total : 0.0;
+    o.completeness_masked_pixels = c_total;
+    o.completeness_good_pixels = c_good;
+    o.completeness_good_pixels_geo = c_geo;
+    o.completeness_good_pixels_photo = c_photo;
+    if (io_num > 0) {
+        o.rmse_geo_err_px = std::sqrt(io_sq_geo / (double)io_num);
+        o.rmse_photo_err = std::sqrt(io_sq_photo / (double)io_num);
+    }
+    o.median_geo_err_px = o.mean_geo_err_px;          // as CheckGlobal reports them
+    o.p90_geo_err_px = o.mean_geo_err_px;
+    o.masked_count = m_count;
+    o.all_count = all_count;
+    o.masked_geo_mean = m_count > 0 ? m_sum_geo / (double)m_count : 0.0;
+    o.masked_photo_mean = m_count > 0 ? m_sum_photo / (double)m_count : 0.0;
+    o.masked_geo_rmse = m_count > 0 ? std::sqrt(m_sq_geo / (double)m_count) : 0.0;
+    o.masked_photo_rmse = m_count > 0 ? std::sqrt(m_sq_photo / (double)m_count) : 0.0;
+    o.coverage = all_count > 0 ? (double)m_count / (double)all_count : 0.0;
+    if (m_count > 0) {
+        long long cum = 0;
+        bool med = false, p90 = false;
+        for (int i = 0; i < pfd::kCycleHistBins && !(med && p90); ++i) {
+            cum += hist[i];
+            if (!med && cum >= (long long)std::ceil(0.5 * (double)m_count)) { o.masked_geo_median_approx = (i + 0.5) * 0.5; med = true; }
+            if (!p90 && cum >= (long long)std::ceil(0.9 * (double)m_count)) { o.masked_geo_p90_approx = (i + 0.5) * 0.5; p90 = true; }
+        }
+    }
+    o.masked_geo_min = std::isfinite(geo_min) ? geo_min : 0.0;
+    o.masked_geo_max = geo_max;
+    *stats = o;
     return PFD_OK;
 }
 
