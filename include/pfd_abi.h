@@ -243,6 +243,20 @@ typedef struct pfd_cycle_stats {
 pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg, float baseline_unit,
                            pfd_cycle_stats* stats, float* geo_err, float* pho_err, uint8_t* texmask);
 
+/* ---- focal stack ----------------------------------------------------------
+ * Renders n_slices refocused images of out_w x out_h from the frame's gray
+ * micro-images.  The reference has no multi-slice render; this one is built
+ * on its back-projection LFRefocus::BackProject2MI (FocalStack/LFRefocus.cpp:
+ * 2119-2125): output pixel (ox, oy) of slice s sits at raw coordinates
+ * X = (ox + 0.5) * (W / out_w) - 0.5 (Y likewise), micro-image i sees it at
+ * u = (X - c_i) / slice_vd[s] + ((m-1)/2 + 1) (the micro-image centre of
+ * FuseVirtualDepth_BackProject, :1635-1636), and every micro-image with u in
+ * [0, m-1]^2 contributes its bilinear sample; the pixel is their mean (0 when
+ * none), summed in view order.  The stack stays on the device; out (host,
+ * float [n_slices][out_h][out_w]) receives a copy unless it is NULL. */
+pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_slices, int out_w, int out_h,
+                       float* out);
+
 /* ---- measurement --------------------------------------------------------
  * No counterpart in the reference (it has no timers or counters on this path,
  * see its Util/Logger only).  Tap counting switches the PatchMatch kernels to

@@ -176,6 +176,24 @@ int orc_cycle_check(const orc_frame* f, const orc_cycle_cfg* cfg, float baseline
 /* cv::meanStdDev of the 3x3 window with top-left (x0, y0) (test hook). */
 void orc_mean_std_3x3(const float* img, int W, int x0, int y0, float* mean, float* stdv);
 
+/* Focal-stack render (no multi-slice render exists in the reference; it is
+ * defined from the reference's own back-projection, LFRefocus::BackProject2MI,
+ * FocalStack/LFRefocus.cpp:2119-2125, with the micro-image centre
+ * ((m-1)/2 + 1) of FuseVirtualDepth_BackProject, :1635-1636).  Output pixel
+ * (ox, oy) of slice s sits at raw coordinates X = (ox + 0.5) * (W / out_w) - 0.5
+ * (Y likewise); every view i, in index order, whose back-projection
+ * u = (X - c_i) / vd_s + (m-1)/2 + 1 lies in [0, m-1]^2 contributes the
+ * bilinear sample of its gray micro-image at u:
+ *   top = fma(ax, T01 - T00, T00), bot = fma(ax, T11 - T10, T10),
+ *   val = fma(ay, bot - top, top)        (T01 = the texel right of T00)
+ * and the output is the mean of the contributions (0 when there are none).
+ * out: [n_slices][out_h][out_w]. */
+int orc_refocus(const orc_frame* f, int raw_w, int raw_h, const float* slice_vd, int n_slices, int out_w, int out_h,
+                float* out);
+/* Number of (slice, output pixel, view) contributions, the render's work unit. */
+long long orc_refocus_samples(const orc_frame* f, int raw_w, int raw_h, const float* slice_vd, int n_slices,
+                              int out_w, int out_h);
+
 /* Scalar hooks for unit tests of the canonical arithmetic. */
 float orc_expf(float x);
 float orc_uniform(uint64_t seed, uint32_t sweep, uint32_t pixel, uint32_t n);

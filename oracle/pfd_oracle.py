@@ -105,6 +105,9 @@ def lib() -> ctypes.CDLL:
         L.orc_texture_mask.argtypes = [_P, _I, _I, YP, _P, _P, _P]
         L.orc_cycle_check.argtypes = [FP, YP, _F, SP, ctypes.POINTER(OrcCycleStats), _P, _P, _P]
         L.orc_mean_std_3x3.argtypes = [_P, _I, _I, _I, _P, _P]
+        L.orc_refocus.argtypes = [FP, _I, _I, _P, _I, _I, _I, _P]
+        L.orc_refocus_samples.argtypes = [FP, _I, _I, _P, _I, _I, _I]
+        L.orc_refocus_samples.restype = ctypes.c_longlong
         _lib = L
     return _lib
 
@@ -257,6 +260,19 @@ def cycle_check(orc: "Oracle", cfg, baseline_unit: float, state: dict):
     assert lib().orc_cycle_check(ctypes.byref(orc.f), ctypes.byref(c), float(baseline_unit), ctypes.byref(st),
                                  ctypes.byref(out), _p(geo), _p(pho), _p(tm)) == 0
     return {k: getattr(out, k) for k in CYCLE_STAT_FIELDS}, geo, pho, tm
+
+
+def refocus(orc: "Oracle", raw_w: int, raw_h: int, slice_vd, out_w: int, out_h: int) -> np.ndarray:
+    """Focal-stack render [n_slices][out_h][out_w] (see orc_refocus)."""
+    vd = np.ascontiguousarray(slice_vd, np.float32)
+    out = np.zeros((vd.shape[0], out_h, out_w), np.float32)
+    assert lib().orc_refocus(ctypes.byref(orc.f), raw_w, raw_h, _p(vd), vd.shape[0], out_w, out_h, _p(out)) == 0
+    return out
+
+
+def refocus_samples(orc: "Oracle", raw_w: int, raw_h: int, slice_vd, out_w: int, out_h: int) -> int:
+    vd = np.ascontiguousarray(slice_vd, np.float32)
+    return int(lib().orc_refocus_samples(ctypes.byref(orc.f), raw_w, raw_h, _p(vd), vd.shape[0], out_w, out_h))
 
 
 def mean_std_3x3(img, x0: int, y0: int):

@@ -185,6 +185,7 @@ def lib() -> ctypes.CDLL:
             "pfd_fp32_fma_rate": [_P, ctypes.POINTER(ctypes.c_double)],
             "pfd_filter": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P, _P],
             "pfd_reprojection_error": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P],
+            "pfd_refocus": [_P, _I, _P, _I, _I, _I, _P],
             "pfd_cycle_check": [_P, _I, ctypes.POINTER(CycleCfgC), _F, ctypes.POINTER(CycleStatsC), _P, _P, _P],
         }
         for name, args in sig.items():
@@ -363,6 +364,15 @@ class Context:
                                             _ptr(geo) if maps else None, _ptr(pho) if maps else None,
                                             _ptr(tm) if maps else None), "pfd_cycle_check")
         return {k: getattr(out, k) for k in CYCLE_STATS}, geo, pho, tm
+
+    def refocus(self, fid: int, slice_vd, out_w: int, out_h: int, download: bool = True):
+        """Focal stack [n_slices][out_h][out_w] of the frame (pfd_refocus); with
+        download=False the stack stays on the device and None is returned."""
+        vd = np.ascontiguousarray(slice_vd, dtype=np.float32)
+        out = np.empty((vd.shape[0], out_h, out_w), np.float32) if download else None
+        self._check(self._L.pfd_refocus(self._h, fid, _ptr(vd), vd.shape[0], out_w, out_h,
+                                        _ptr(out) if download else None), "pfd_refocus")
+        return out
 
     def reprojection_error(self, fid: int, cfg: FilterCfg, baseline_unit: float) -> np.ndarray:
         f = self._frames[fid]

@@ -17,6 +17,7 @@
 #include "../../include/pfd_abi.h"
 #include "pm_kernels.h"
 #include "check_kernels.h"
+#include "refocus_kernels.h"
 
 namespace {
 
@@ -48,6 +49,13 @@ struct Frame {
     unsigned int* d_cyc_hist = nullptr;        // cycle check: masked geometric-error histogram
     float* d_cyc_maps = nullptr;               // cycle check: geo and photo error maps
     uint8_t* d_cyc_tm = nullptr;               // cycle check: texture mask
+    std::vector<float> h_centers;              // lens centres, for the refocus bucket grid
+    int* d_cells = nullptr;                    // refocus: cell_start [cells + 1] then cell_ids [V]
+    int grid_w = 0, grid_h = 0;
+    float grid_x0 = 0.f, grid_y0 = 0.f, grid_cell = 0.f;
+    float* d_slice_vd = nullptr;               // refocus: slice virtual depths [kMaxSlices]
+    float* d_stack = nullptr;                  // refocus: focal stack
+    size_t stack_bytes = 0;
 };
 
 }  // namespace
@@ -115,6 +123,18 @@ pfd_status frame_alloc(pfd_ctx* ctx, Frame& f, void** p, size_t bytes)
     f.bytes += bytes;
     if (f.registered) ctx->used += bytes;
     return PFD_OK;
+}
+
+// Frees one buffer obtained from frame_alloc.
+void frame_free_one(pfd_ctx* ctx, Frame& f, void* p, size_t bytes)
+{
+    if (!p) return;
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(p);
+    for (size_t i = 0; i < f.allocs.size(); ++i)
+        if (f.allocs[i] == p) { f.allocs.erase(f.allocs.begin() + (long)i); break; }
+    f.bytes -= bytes;
+    if (f.registered) ctx->used -= bytes;
 }
 
 void frame_release(Frame& f)
@@ -190,6 +210,9 @@ pfd_status check_device_error(pfd_ctx* ctx)
     CU(cudaStreamSynchronize(ctx->stream));
     if (h) {
         CU(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+        if (h == PFD_DEVERR_REFOCUS_LENSES)
+            return fail(ctx, PFD_EINVAL, "refocus: more than %d lenses reach one output tile (slice virtual depth "
+                        "too large for this lens density)", pfd::kMaxRefocusCand);
         return fail(ctx, PFD_ETIMEDOUT, "device wait timed out (flags 0x%x)", h);
     }
     return PFD_OK;
@@ -368,6 +391,7 @@ pfd_status pfd_frame_create(pfd_ctx* ctx, int* frame_id, int W, int H, const flo
         return fail(ctx, st, "frame_create: upload failed");
     }
     f.h_keys.assign(tilekeys, tilekeys + 2 * (size_t)n_views);
+    f.h_centers.assign(centers, centers + 2 * (size_t)n_views);
     f.h_nb_ids.assign(nb_ids, nb_ids + (size_t)n_views * max_nb);
     f.h_nb_counts.assign(nb_counts, nb_counts + n_views);
     const int id = ctx->next_id++;
@@ -819,6 +843,84 @@ pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg,
     o.masked_geo_max = geo_max;
     *stats = o;
     return PFD_OK;
+}
+
+static const int kMaxSlices = 1024;
+
+// Bucket grid of lens centres for the render (built once per frame): cells of
+// 32 px, ids ascending within a cell.
+static pfd_status build_lens_grid(pfd_ctx* ctx, Frame& f)
+{
+    if (f.d_cells) return PFD_OK;
+    float x0 = INFINITY, y0 = INFINITY, x1 = -INFINITY, y1 = -INFINITY;
+    for (int v = 0; v < f.V; ++v) {
+        x0 = std::min(x0, f.h_centers[2 * v]); x1 = std::max(x1, f.h_centers[2 * v]);
+        y0 = std::min(y0, f.h_centers[2 * v + 1]); y1 = std::max(y1, f.h_centers[2 * v + 1]);
+    }
+    const float cell = 32.0f, inv = 1.0f / cell;
+    const int gw = std::max(1, (int)std::floor((x1 - x0) * inv) + 1), gh = std::max(1, (int)std::floor((y1 - y0) * inv) + 1);
+    std::vector<int> start((size_t)gw * gh + 1, 0), ids(f.V);
+    std::vector<int> cell_of(f.V);
+    for (int v = 0; v < f.V; ++v) {
+        const int cx = std::min(gw - 1, std::max(0, (int)std::floor((f.h_centers[2 * v] - x0) * inv)));
+        const int cy = std::min(gh - 1, std::max(0, (int)std::floor((f.h_centers[2 * v + 1] - y0) * inv)));
+        cell_of[v] = cy * gw + cx;
+        start[cell_of[v] + 1]++;
+    }
+    for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int v = 0; v < f.V; ++v) ids[fill[cell_of[v]]++] = v;
+    void* p = nullptr;
+    pfd_status st = frame_alloc(ctx, f, &p, sizeof(int) * (start.size() + ids.size()) + sizeof(float) * kMaxSlices);
+    if (st != PFD_OK) return st;
+    f.d_cells = (int*)p;
+    f.d_slice_vd = (float*)(f.d_cells + start.size() + ids.size());
+    CU(cudaMemcpyAsync(f.d_cells, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(f.d_cells + start.size(), ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));      // host vectors go out of scope
+    f.grid_w = gw; f.grid_h = gh; f.grid_x0 = x0; f.grid_y0 = y0; f.grid_cell = cell;
+    return PFD_OK;
+}
+
+pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_slices, int out_w, int out_h,
+                       float* out)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!slice_vd || n_slices < 1 || n_slices > kMaxSlices)
+        return fail(ctx, PFD_EINVAL, "refocus: need 1..%d slice virtual depths", kMaxSlices);
+    if (out_w < 1 || out_h < 1 || out_w > 65536 || out_h > 65536) return fail(ctx, PFD_EINVAL, "refocus: bad output size");
+    for (int i = 0; i < n_slices; ++i)
+        if (!(slice_vd[i] > 0.0f) || !std::isfinite(slice_vd[i]))
+            return fail(ctx, PFD_EINVAL, "refocus: slice %d virtual depth must be finite and > 0", i);
+    if (!f->has_raw) return fail(ctx, PFD_ESTATE, "frame has no raw image yet");
+    DeviceGuard g(ctx->device);
+    pfd_status st = build_lens_grid(ctx, *f);
+    if (st != PFD_OK) return st;
+    const size_t need = sizeof(float) * (size_t)n_slices * out_w * out_h;
+    if (need > f->stack_bytes) {
+        frame_free_one(ctx, *f, f->d_stack, f->stack_bytes);
+        f->d_stack = nullptr;
+        f->stack_bytes = 0;
+        void* p = nullptr;
+        if ((st = frame_alloc(ctx, *f, &p, need)) != PFD_OK) return st;
+        f->d_stack = (float*)p;
+        f->stack_bytes = need;
+    }
+    pfd::RefocusFrame R;
+    R.V = f->V; R.m = f->mi_w; R.mh = f->mi_h; R.tile_stride = f->tile_stride;
+    R.gray = f->d_gray; R.centers = f->d_centers;
+    R.cell_start = f->d_cells;
+    R.cell_ids = f->d_cells + (size_t)f->grid_w * f->grid_h + 1;
+    R.grid_w = f->grid_w; R.grid_h = f->grid_h;
+    R.grid_x0 = f->grid_x0; R.grid_y0 = f->grid_y0; R.cell = f->grid_cell;
+    if (pfd::refocus_smem_bytes(R) > 227 * 1024) return fail(ctx, PFD_EINVAL, "refocus: micro-image too large");
+    CU(cudaMemcpyAsync(f->d_slice_vd, slice_vd, sizeof(float) * n_slices, cudaMemcpyHostToDevice, ctx->stream));
+    CU(pfd::launch_refocus(R, f->d_slice_vd, n_slices, f->W, f->H, out_w, out_h, f->d_stack, ctx->d_err, ctx->stream));
+    if (out) CU(cudaMemcpyAsync(out, f->d_stack, need, cudaMemcpyDeviceToHost, ctx->stream));
+    return out ? check_device_error(ctx) : PFD_OK;
 }
 
 pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane, float* cost, float* disp, uint32_t* sel)
