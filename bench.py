@@ -3,8 +3,10 @@
 
 One step = one 4080x3068 8-bit raw frame (pitch 23.2 px, three lens types with
 blur sigma 0.6/1.0/1.4, 12 slanted planes, ~26.6 k micro-images) through the
-engine: micro-image slicing, random initialisation and 8 red-black PatchMatch
-iterations with 12 neighbours and a 15x15 bilateral NCC, FP32.
+whole path: micro-image slicing, random initialisation and 8 red-black
+PatchMatch iterations with 12 neighbours and a 15x15 bilateral NCC (FP32),
+the cycle check, the disparity filter and its reprojection-error map, and a
+64-slice focal stack rendered to 2040x1534.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -30,8 +32,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "plenoptic-for-depth_b200")
 
 WORKLOAD = dict(width=4080, height=3068, pitch=23.2, n_planes=12, max_nb=12, patch_size=15, iterations=8,
-                sigma_spatial=3.0, sigma_color=12.0, n_lens_types=3, blur_sigma=(0.6, 1.0, 1.4), seed=2026)
-METRIC = "4080x3068 depth frames/s"
+                sigma_spatial=3.0, sigma_color=12.0, n_lens_types=3, blur_sigma=(0.6, 1.0, 1.4), seed=2026,
+                slices=64, vd_range=(2.0, 12.0))
+
+
+def metric() -> str:
+    return "%dx%d depth frames/s" % (WORKLOAD["width"], WORKLOAD["height"])
 FLOPS_PER_TAP = 24      # per in-bounds NCC tap: disparity 4, source coords 4, fractions 2, bilinear 6, moments 8
 
 
@@ -58,6 +64,15 @@ def make_workload(pfd, rank: int):
     w = WORKLOAD
     return pfd.make_workload(w["width"], w["height"], w["pitch"], w["n_planes"], seed=w["seed"] + rank,
                              max_nb=w["max_nb"], n_lens_types=w["n_lens_types"], blur_sigma=w["blur_sigma"])
+
+
+def stack_size():
+    return WORKLOAD["width"] // 2, WORKLOAD["height"] // 2
+
+
+def slice_vds():
+    lo, hi = WORKLOAD["vd_range"]
+    return np.linspace(lo, hi, WORKLOAD["slices"]).astype(np.float32)
 
 
 def pm_params(pfd):
@@ -123,21 +138,30 @@ class ClockSampler:
 # CPU baseline: the oracle restatement of the reference, on a bounded sample
 # --------------------------------------------------------------------------
 class CpuSample:
-    """The oracle's RandomInitializationForFrame + one CheckerboardUpdateFrame
-    half-sweep, timed on a contiguous block of micro-images and extrapolated
-    to one frame (init of every view + 2 x iterations half-sweeps).  The
-    neighbourhood the half-sweep reads (cross-view proposals) is initialised
-    once, outside the timed region."""
+    """The oracle restatement of the whole path, timed on a bounded sample of
+    one frame and scaled to the frame:
+      * PatchMatch: RandomInitializationForFrame + one CheckerboardUpdateFrame
+        half-sweep on a contiguous block of micro-images (OpenMP), extrapolated
+        to init + 2 x iterations half-sweeps of every view;
+      * the cycle check, the disparity filter and its reprojection map on the
+        full frame (single-threaded, like the reference's CPU code), run on the
+        oracle's random-initialisation state of the frame;
+      * the focal stack: 2 of the slices (virtual depths 4.5 and 9.6, whose
+        mean squared depth is that of the 64), scaled by slices / 2 (OpenMP).
+    The initialisation of the whole frame that the block reads runs once,
+    outside the timed region."""
 
-    def __init__(self, oracle, w, params, seed, nthreads):
+    def __init__(self, pfd, oracle, w, params, seed, nthreads):
+        self.pfd, self.oracle = pfd, oracle
         self.orc = oracle.Oracle(w.gray, w.centers, w.nb_ids, w.nb_counts)
         self.params, self.seed, self.nthreads = params, seed, nthreads
         self.V = w.centers.shape[0]
         self.v0 = self.V // 2
         self.max_views = min(2048, self.V - self.v0)
-        self.state = self.orc.init(params, seed, nthreads=nthreads,
-                                   views=(max(0, self.v0 - 400), min(self.V, self.v0 + 400 + self.max_views)))
+        self.state = self.orc.init(params, seed, nthreads=nthreads)
         self.nv = 2
+        vds = slice_vds()
+        self.sample_vds = vds[[len(vds) // 4, (3 * len(vds)) // 4]]
 
     def time_block(self, nv):
         t0 = time.perf_counter()
@@ -146,6 +170,20 @@ class CpuSample:
         self.orc.sweep(self.params, self.seed, 0, 0, self.state, nthreads=self.nthreads, views=(self.v0, self.v0 + nv))
         t2 = time.perf_counter()
         return t1 - t0, t2 - t1
+
+    def time_rest(self):
+        o, pfd = self.oracle, self.pfd
+        st = {k: v.copy() for k, v in self.state.items()}
+        unit = WORKLOAD["pitch"]
+        t0 = time.perf_counter()
+        o.cycle_check(self.orc, pfd.CycleCfg(), unit, st)
+        o.filter_global(self.orc, pfd.FilterCfg(), unit, st)
+        o.reprojection_error(self.orc, pfd.FilterCfg(), unit, st)
+        t1 = time.perf_counter()
+        ow, oh = stack_size()
+        o.refocus(self.orc, WORKLOAD["width"], WORKLOAD["height"], self.sample_vds, ow, oh)
+        t2 = time.perf_counter()
+        return t1 - t0, (t2 - t1) * WORKLOAD["slices"] / len(self.sample_vds)
 
     def calibrate(self, budget_s):
         nv = 2
@@ -158,8 +196,17 @@ class CpuSample:
 
     def run(self) -> dict:
         ti, ts = self.time_block(self.nv)
-        frame_s = (ti + 2 * self.params.max_iterations * ts) * self.V / self.nv
-        return {"frame_s": frame_s, "views": self.nv, "t_init": ti, "t_sweep": ts}
+        t_checks, t_stack = self.time_rest()
+        pm_s = (ti + 2 * self.params.max_iterations * ts) * self.V / self.nv
+        return {"frame_s": pm_s + t_checks + t_stack, "views": self.nv, "t_init": ti, "t_sweep": ts,
+                "pm_s": pm_s, "t_checks": t_checks, "t_stack": t_stack}
+
+    def describe(self, s) -> str:
+        return ("oracle init + one half-sweep on %d of %d micro-images (%.1f s + %.1f s, %d threads), extrapolated "
+                "to init + %d half-sweeps (%.0f s); cycle check + filter + reprojection map on the full frame "
+                "(%.1f s, 1 thread); focal stack: 2 of %d slices (%.1f s scaled, %d threads)" %
+                (s["views"], self.V, s["t_init"], s["t_sweep"], self.nthreads, 2 * self.params.max_iterations,
+                 s["pm_s"], s["t_checks"], WORKLOAD["slices"], s["t_stack"], self.nthreads))
 
 
 def cpu_threads() -> int:
@@ -172,7 +219,11 @@ def cpu_threads() -> int:
 # --------------------------------------------------------------------------
 # engine arm
 # --------------------------------------------------------------------------
+STAGES = ("slice+init", "patchmatch sweeps", "cycle check", "filter", "reprojection map", "focal stack")
+
+
 def run_engine(args, rank, world, local_rank):
+    import ctypes
     import torch
     import torch.distributed as dist
 
@@ -181,6 +232,10 @@ def run_engine(args, rank, world, local_rank):
     w = make_workload(pfd, rank)
     params = pm_params(pfd)
     V = w.centers.shape[0]
+    unit = WORKLOAD["pitch"]
+    ow, oh = stack_size()
+    vds = slice_vds()
+    ccfg, fcfg = pfd.CycleCfg(), pfd.FilterCfg()
     ctx = pfd.Context(local_rank)
     fid = ctx.frame_create(w.frame.raw.shape[1], w.frame.raw.shape[0], w.centers, w.tilekeys, w.mi, w.mi,
                            w.nb_ids, w.nb_counts)
@@ -188,20 +243,33 @@ def run_engine(args, rank, world, local_rank):
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local_rank}")
     seed = WORKLOAD["seed"]
-    launches_per_step = 1 + 1 + 2 * params.max_iterations     # slice, init, sweeps
+
+    def mark(ev, key):
+        if ev is not None:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(stream)
+            ev.setdefault(key, []).append(e)
 
     def step(ev=None):
+        """The whole path on one frame already resident in HBM."""
+        mark(ev, "t0")
         ctx.frame_set_raw_device(fid, raw_dev.data_ptr(), raw_dev.shape[1])
         ctx.pm_init(fid, params, seed)
+        mark(ev, "t1")
         for it in range(params.max_iterations):
             for ph in range(2):
-                if ev is not None:
-                    ev[0].append(torch.cuda.Event(enable_timing=True))
-                    ev[0][-1].record(stream)
+                mark(ev, "sweep_a")
                 ctx.pm_sweep(fid, params, seed, it, ph)
-                if ev is not None:
-                    ev[1].append(torch.cuda.Event(enable_timing=True))
-                    ev[1][-1].record(stream)
+                mark(ev, "sweep_b")
+        mark(ev, "t2")
+        ctx.cycle_check(fid, ccfg, unit, maps=False)
+        mark(ev, "t3")
+        ctx.filter(fid, fcfg, unit, download=False)
+        mark(ev, "t4")
+        ctx.reprojection_error(fid, fcfg, unit, download=False)
+        mark(ev, "t5")
+        ctx.refocus(fid, vds, ow, oh, download=False)
+        mark(ev, "t6")
 
     # calibration pass: in-bounds NCC taps per sweep launch (identical trajectory: same seed)
     ctx.set_tap_counting(True)
@@ -225,38 +293,51 @@ def run_engine(args, rank, world, local_rank):
     torch.cuda.synchronize()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    ev_sweep = ([], [])
+    ev = {}
+    launches0 = ctx.launch_count()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     t_start.record(stream)
     for _ in range(args.steps):
-        step(ev_sweep)
+        step(ev)
     t_end.record(stream)
     ctx.sync()
     torch.cuda.synchronize()
+    launches = ctx.launch_count() - launches0
     clk = clocks.stop()
     ms = t_start.elapsed_time(t_end)
-    sweep_ms = [a.elapsed_time(b) for a, b in zip(*ev_sweep)]
+    sweep_ms = [a.elapsed_time(b) for a, b in zip(ev["sweep_a"], ev["sweep_b"])]
+    stage_ms = {}
+    for name, (a, b) in zip(STAGES, [("t0", "t1"), ("t1", "t2"), ("t2", "t3"), ("t3", "t4"), ("t4", "t5"),
+                                     ("t5", "t6")]):
+        stage_ms[name] = round(statistics.mean(x.elapsed_time(y) for x, y in zip(ev[a], ev[b])), 3)
     if world > 1:
         t = torch.tensor([ms], device=f"cuda:{local_rank}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
 
-    # e2e through the public API with host buffers: pinned raw in, per-pixel
-    # state (plane, cost, selected views) out, every step
+    # e2e through the public API with host buffers: pinned raw frame in; the
+    # filtered per-pixel state (plane, cost, selected views) and the focal
+    # stack out, every step
     pinned_raw = torch.from_numpy(w.frame.raw).pin_memory()
     px = V * w.mi * w.mi
     out_plane = torch.empty((px, 4), dtype=torch.float32).pin_memory()
     out_cost = torch.empty(px, dtype=torch.float32).pin_memory()
     out_sel = torch.empty(px, dtype=torch.int32).pin_memory()
-    import ctypes
+    out_stack = torch.empty((len(vds), oh, ow), dtype=torch.float32).pin_memory()
+    vd_host = np.ascontiguousarray(vds)
     L = pfd.lib()
 
     def e2e_step():
         ctx._check(L.pfd_frame_set_raw(ctx._h, fid, ctypes.c_void_p(pinned_raw.data_ptr()), pinned_raw.shape[1]),
                    "pfd_frame_set_raw")
         ctx.patchmatch(fid, params, seed)
+        ctx.cycle_check(fid, ccfg, unit, maps=False)
+        ctx.filter(fid, fcfg, unit, download=False)
+        ctx.reprojection_error(fid, fcfg, unit, download=False)
+        ctx._check(L.pfd_refocus(ctx._h, fid, ctypes.c_void_p(vd_host.ctypes.data), len(vd_host), ow, oh,
+                                 ctypes.c_void_p(out_stack.data_ptr())), "pfd_refocus")
         ctx._check(L.pfd_download(ctx._h, fid, ctypes.c_void_p(out_plane.data_ptr()), ctypes.c_void_p(out_cost.data_ptr()),
                                   None, ctypes.c_void_p(out_sel.data_ptr())), "pfd_download")
 
@@ -289,21 +370,24 @@ def run_engine(args, rank, world, local_rank):
             if tj.get("workload") == "4080x3068 pitch 23.2 K12 P15":
                 traffic = tj.get("bytes_per_launch")
         result = {
-            "metric": METRIC, "value": round(value, 4), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "metric": metric(), "value": round(value, 4), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plenoptic raw frame)",
             "config": {"workload": "%dx%d raw, pitch %.1f px, 3 lens types, %d planes, %d micro-images, "
-                                   "K=%d neighbours, %dx%d bilateral NCC, %d PatchMatch iterations, FP32" %
+                                   "K=%d neighbours, %dx%d bilateral NCC, %d PatchMatch iterations, FP32; cycle "
+                                   "check, disparity filter + reprojection map; %d-slice focal stack to %dx%d" %
                                    (WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["pitch"], WORKLOAD["n_planes"], V,
                                     WORKLOAD["max_nb"], WORKLOAD["patch_size"], WORKLOAD["patch_size"],
-                                    WORKLOAD["iterations"]),
+                                    WORKLOAD["iterations"], WORKLOAD["slices"], ow, oh),
                        "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "per-step working set %.2f GB > 126 MB L2 (state + tiles)" %
-                             (px * 40 * 2 / 1e9),
-                       "stages": "slice + init + 16 half-sweeps"},
+                       "l2": "per-step working set %.2f GB > 126 MB L2 (state, tiles, focal stack)" %
+                             (px * 40 * 2 / 1e9 + len(vds) * ow * oh * 4 / 1e9),
+                       "stages": list(STAGES)},
+            "stage_ms": stage_ms,
             "e2e": {"value": round(world * e2e_steps / e2e_s, 4), "unit": "frames/s",
                     "h2d_bytes_per_step": int(w.frame.raw.nbytes),
-                    "d2h_bytes_per_step": int(out_plane.numel() * 4 + out_cost.numel() * 4 + out_sel.numel() * 4)},
+                    "d2h_bytes_per_step": int(out_plane.numel() * 4 + out_cost.numel() * 4 + out_sel.numel() * 4 +
+                                              out_stack.numel() * 4)},
             "roofline": {"bound": "fp32", "kernel": "pm_sweep_kernel", "achieved": round(achieved, 3),
                          "peak": round(fp32_tflops, 2), "unit": "TFLOP/s", "frac": round(achieved / fp32_tflops, 4),
                          "peak_source": "measured FP32 FFMA rate on this device (pfd_fp32_fma_rate); "
@@ -312,19 +396,16 @@ def run_engine(args, rank, world, local_rank):
                                         (FLOPS_PER_TAP, taps_per_launch),
                          "avg_launch_ms": round(avg_sweep_ms, 3), "traffic": traffic},
             "clocks": clk,
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": launches,
         }
         if world == 1 and not args.no_cpu_baseline:
             oracle = load_oracle()
             nth = cpu_threads()
-            cs = CpuSample(oracle, w, params, seed, nth)
+            cs = CpuSample(pfd, oracle, w, params, seed, nth)
             cs.calibrate(15.0)
-            s = cs.run()
-            result["cpu_baseline"] = {"value": round(1.0 / s["frame_s"], 8), "unit": "frames/s", "cores": nth,
-                                      "kind": "port",
-                                      "sample": "oracle init + one half-sweep on %d of %d micro-images "
-                                                "(%.1f s + %.1f s), extrapolated to init + 16 half-sweeps" %
-                                                (s["views"], V, s["t_init"], s["t_sweep"])}
+            smp = cs.run()
+            result["cpu_baseline"] = {"value": round(1.0 / smp["frame_s"], 8), "unit": "frames/s", "cores": nth,
+                                      "kind": "port", "sample": cs.describe(smp)}
     ctx.frame_free(fid)
     ctx.close()
     return result
@@ -341,28 +422,29 @@ def run_reference(args, rank, world):
     w = make_workload(pfd, 0)
     params = pm_params(pfd)
     nth = cpu_threads()
-    cs = CpuSample(oracle, w, params, WORKLOAD["seed"], nth)
+    cs = CpuSample(pfd, oracle, w, params, WORKLOAD["seed"], nth)
     cs.calibrate(6.0)
     vals = []
     samples = []
     for i in range(args.warmup + args.steps):
-        s = cs.run()
+        smp = cs.run()
         if i >= args.warmup:
-            vals.append(1.0 / s["frame_s"])
-            samples.append(s)
+            vals.append(1.0 / smp["frame_s"])
+            samples.append(smp)
     value = statistics.median(vals)
     V = w.centers.shape[0]
-    s = samples[0]
+    ow, oh = stack_size()
     return {
-        "metric": METRIC, "value": round(value, 8), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric(), "value": round(value, 8), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "dtype": "f32",
         "data": "synthetic (seeded plenoptic raw frame)",
-        "config": {"workload": "%dx%d raw, pitch %.1f px, %d micro-images, K=%d, %dx%d NCC, %d iterations" %
+        "config": {"workload": "%dx%d raw, pitch %.1f px, %d micro-images, K=%d, %dx%d NCC, %d iterations; cycle "
+                               "check, filter + reprojection map; %d-slice focal stack to %dx%d" %
                    (WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["pitch"], V, WORKLOAD["max_nb"],
-                    WORKLOAD["patch_size"], WORKLOAD["patch_size"], WORKLOAD["iterations"])},
+                    WORKLOAD["patch_size"], WORKLOAD["patch_size"], WORKLOAD["iterations"], WORKLOAD["slices"],
+                    ow, oh)},
         "cpu_baseline": {"value": round(value, 8), "unit": "frames/s", "cores": nth, "kind": "port",
-                         "sample": "oracle init + one half-sweep on %d micro-images per step, extrapolated to a "
-                                   "frame" % s["views"]},
+                         "sample": cs.describe(samples[0])},
         "e2e": {"value": round(value, 8), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

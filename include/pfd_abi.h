@@ -266,6 +266,9 @@ pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_
 pfd_status pfd_set_tap_counting(pfd_ctx* ctx, int enable);
 /* Reads and clears the tap counter (synchronises the stream). */
 pfd_status pfd_read_tap_count(pfd_ctx* ctx, unsigned long long* taps);
+/* Number of kernels this context has launched so far (every engine kernel,
+ * the FP32 probe included). */
+pfd_status pfd_launch_count(pfd_ctx* ctx, unsigned long long* n);
 /* Measured FP32 fused multiply-add throughput of the device, TFLOP/s
  * (independent FFMA chains on every SM; best of three launches). */
 pfd_status pfd_fp32_fma_rate(pfd_ctx* ctx, double* tflops);

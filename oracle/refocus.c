@@ -14,8 +14,6 @@
 #include <math.h>
 #include <stdlib.h>
 
-typedef struct { int lo, hi; } span;
-
 /* Views whose centre lies in [cx_lo, cx_hi] x [cy_lo, cy_hi], ascending. */
 static int views_in_box(const orc_frame* f, float cx_lo, float cx_hi, float cy_lo, float cy_hi, int* ids)
 {
@@ -34,47 +32,52 @@ static long long render(const orc_frame* f, int raw_w, int raw_h, const float* s
     const float cmx = (float)(m - 1) * 0.5f + 1.0f, cmy = (float)(mh - 1) * 0.5f + 1.0f;
     const float sx = (float)raw_w / (float)out_w, sy = (float)raw_h / (float)out_h;
     const float umax = (float)(m - 1), wmax = (float)(mh - 1);
-    int* ids = (int*)malloc(sizeof(int) * (size_t)(f->n_views > 0 ? f->n_views : 1));
+    const int TB = 16;                     /* output blocks, for culling only */
+    const int nbx = (out_w + TB - 1) / TB, nby = (out_h + TB - 1) / TB;
+    const long long nblocks = (long long)n_slices * nbx * nby;
     long long samples = 0;
-    const int TB = 16;                     /* output blocks for culling only */
-    for (int s = 0; s < n_slices; ++s) {
-        const float v = slice_vd[s];
-        for (int by = 0; by < out_h; by += TB)
-            for (int bx = 0; bx < out_w; bx += TB) {
-                const int ex = bx + TB < out_w ? bx + TB : out_w, ey = by + TB < out_h ? by + TB : out_h;
-                const float X0 = ((float)bx + 0.5f) * sx - 0.5f, X1 = ((float)(ex - 1) + 0.5f) * sx - 0.5f;
-                const float Y0 = ((float)by + 0.5f) * sy - 0.5f, Y1 = ((float)(ey - 1) + 0.5f) * sy - 0.5f;
-                /* u in [0, m-1]  <=>  c in [X - (m-1-cm) v, X + cm v]; 1 px of slack */
-                const int n = views_in_box(f, X0 - (umax - cmx) * v - 1.0f, X1 + cmx * v + 1.0f,
-                                           Y0 - (wmax - cmy) * v - 1.0f, Y1 + cmy * v + 1.0f, ids);
-                for (int oy = by; oy < ey; ++oy)
-                    for (int ox = bx; ox < ex; ++ox) {
-                        const float X = ((float)ox + 0.5f) * sx - 0.5f, Y = ((float)oy + 0.5f) * sy - 0.5f;
-                        float sum = 0.0f;
-                        int cnt = 0;
-                        for (int k = 0; k < n; ++k) {
-                            const int i = ids[k];
-                            const float u = (X - f->centers[2 * i]) / v + cmx;
-                            const float w = (Y - f->centers[2 * i + 1]) / v + cmy;
-                            if (!(u >= 0.0f && u <= umax && w >= 0.0f && w <= wmax)) continue;
-                            const int x0 = (int)floorf(u), y0 = (int)floorf(w);
-                            const int x1 = x0 + 1 < m - 1 ? x0 + 1 : m - 1;
-                            const int y1 = y0 + 1 < mh - 1 ? y0 + 1 : mh - 1;
-                            const float ax = u - (float)x0, ay = w - (float)y0;
-                            const float* T = f->gray + (size_t)i * m * mh;
-                            const float t00 = T[y0 * m + x0], t01 = T[y0 * m + x1];
-                            const float t10 = T[y1 * m + x0], t11 = T[y1 * m + x1];
-                            const float top = fmaf(ax, t01 - t00, t00);
-                            const float bot = fmaf(ax, t11 - t10, t10);
-                            sum = sum + fmaf(ay, bot - top, top);
-                            ++cnt;
-                        }
-                        samples += cnt;
-                        if (out) out[((size_t)s * out_h + oy) * out_w + ox] = cnt ? sum / (float)cnt : 0.0f;
+#pragma omp parallel reduction(+ : samples)
+    {
+        int* ids = (int*)malloc(sizeof(int) * (size_t)(f->n_views > 0 ? f->n_views : 1));
+#pragma omp for schedule(dynamic, 4)
+        for (long long blk = 0; blk < nblocks; ++blk) {
+            const int s = (int)(blk / ((long long)nbx * nby));
+            const int by = (int)((blk / nbx) % nby) * TB, bx = (int)(blk % nbx) * TB;
+            const float v = slice_vd[s];
+            const int ex = bx + TB < out_w ? bx + TB : out_w, ey = by + TB < out_h ? by + TB : out_h;
+            const float X0 = ((float)bx + 0.5f) * sx - 0.5f, X1 = ((float)(ex - 1) + 0.5f) * sx - 0.5f;
+            const float Y0 = ((float)by + 0.5f) * sy - 0.5f, Y1 = ((float)(ey - 1) + 0.5f) * sy - 0.5f;
+            /* u in [0, m-1]  <=>  c in [X - (m-1-cm) v, X + cm v]; 1 px of slack */
+            const int n = views_in_box(f, X0 - (umax - cmx) * v - 1.0f, X1 + cmx * v + 1.0f,
+                                       Y0 - (wmax - cmy) * v - 1.0f, Y1 + cmy * v + 1.0f, ids);
+            for (int oy = by; oy < ey; ++oy)
+                for (int ox = bx; ox < ex; ++ox) {
+                    const float X = ((float)ox + 0.5f) * sx - 0.5f, Y = ((float)oy + 0.5f) * sy - 0.5f;
+                    float sum = 0.0f;
+                    int cnt = 0;
+                    for (int k = 0; k < n; ++k) {
+                        const int i = ids[k];
+                        const float u = (X - f->centers[2 * i]) / v + cmx;
+                        const float w = (Y - f->centers[2 * i + 1]) / v + cmy;
+                        if (!(u >= 0.0f && u <= umax && w >= 0.0f && w <= wmax)) continue;
+                        const int x0 = (int)floorf(u), y0 = (int)floorf(w);
+                        const int x1 = x0 + 1 < m - 1 ? x0 + 1 : m - 1;
+                        const int y1 = y0 + 1 < mh - 1 ? y0 + 1 : mh - 1;
+                        const float ax = u - (float)x0, ay = w - (float)y0;
+                        const float* T = f->gray + (size_t)i * m * mh;
+                        const float t00 = T[y0 * m + x0], t01 = T[y0 * m + x1];
+                        const float t10 = T[y1 * m + x0], t11 = T[y1 * m + x1];
+                        const float top = fmaf(ax, t01 - t00, t00);
+                        const float bot = fmaf(ax, t11 - t10, t10);
+                        sum = sum + fmaf(ay, bot - top, top);
+                        ++cnt;
                     }
-            }
+                    samples += cnt;
+                    if (out) out[((size_t)s * out_h + oy) * out_w + ox] = cnt ? sum / (float)cnt : 0.0f;
+                }
+        }
+        free(ids);
     }
-    free(ids);
     return samples;
 }
 

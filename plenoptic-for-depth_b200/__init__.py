@@ -186,6 +186,7 @@ def lib() -> ctypes.CDLL:
             "pfd_filter": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P, _P],
             "pfd_reprojection_error": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P],
             "pfd_refocus": [_P, _I, _P, _I, _I, _I, _P],
+            "pfd_launch_count": [_P, ctypes.POINTER(ctypes.c_ulonglong)],
             "pfd_cycle_check": [_P, _I, ctypes.POINTER(CycleCfgC), _F, ctypes.POINTER(CycleStatsC), _P, _P, _P],
         }
         for name, args in sig.items():
@@ -338,13 +339,18 @@ class Context:
         self._check(self._L.pfd_fp32_fma_rate(self._h, ctypes.byref(v)), "pfd_fp32_fma_rate")
         return v.value
 
-    def filter(self, fid: int, cfg: FilterCfg, baseline_unit: float):
+    def filter(self, fid: int, cfg: FilterCfg, baseline_unit: float, download: bool = True):
         """MIDisparityFilterCPU::FilterGlobal on the frame's state, in place.
-        Returns (reason map [V*mi*mi] uint8, stats dict)."""
+        Returns (reason map [V*mi*mi] uint8, stats dict); with download=False
+        nothing is copied back (no stream synchronisation) and None is returned."""
+        c = cfg.c()
+        if not download:
+            self._check(self._L.pfd_filter(self._h, fid, ctypes.byref(c), float(baseline_unit), None, None),
+                        "pfd_filter")
+            return None
         f = self._frames[fid]
         reason = np.empty(f["V"] * f["mi_w"] * f["mi_h"], np.uint8)
         stats = np.zeros(8, np.int64)
-        c = cfg.c()
         self._check(self._L.pfd_filter(self._h, fid, ctypes.byref(c), float(baseline_unit), _ptr(reason), _ptr(stats)),
                     "pfd_filter")
         return reason, dict(zip(FILTER_STATS, (int(x) for x in stats)))
@@ -365,6 +371,11 @@ class Context:
                                             _ptr(tm) if maps else None), "pfd_cycle_check")
         return {k: getattr(out, k) for k in CYCLE_STATS}, geo, pho, tm
 
+    def launch_count(self) -> int:
+        n = ctypes.c_ulonglong()
+        self._check(self._L.pfd_launch_count(self._h, ctypes.byref(n)), "pfd_launch_count")
+        return int(n.value)
+
     def refocus(self, fid: int, slice_vd, out_w: int, out_h: int, download: bool = True):
         """Focal stack [n_slices][out_h][out_w] of the frame (pfd_refocus); with
         download=False the stack stays on the device and None is returned."""
@@ -374,10 +385,14 @@ class Context:
                                         _ptr(out) if download else None), "pfd_refocus")
         return out
 
-    def reprojection_error(self, fid: int, cfg: FilterCfg, baseline_unit: float) -> np.ndarray:
+    def reprojection_error(self, fid: int, cfg: FilterCfg, baseline_unit: float, download: bool = True):
+        c = cfg.c()
+        if not download:
+            self._check(self._L.pfd_reprojection_error(self._h, fid, ctypes.byref(c), float(baseline_unit), None),
+                        "pfd_reprojection_error")
+            return None
         f = self._frames[fid]
         err = np.empty(f["V"] * f["mi_w"] * f["mi_h"], np.float32)
-        c = cfg.c()
         self._check(self._L.pfd_reprojection_error(self._h, fid, ctypes.byref(c), float(baseline_unit), _ptr(err)),
                     "pfd_reprojection_error")
         return err

@@ -69,6 +69,7 @@ struct pfd_ctx {
     int* d_err = nullptr;
     unsigned long long* d_taps = nullptr;   // tap counter of calibration runs
     bool counting = false;
+    unsigned long long launches = 0;        // kernels this context has launched
     float* d_scratch = nullptr;             // sweep candidate costs, per resident CTA
     size_t scratch_bytes = 0;
     std::string last_error;
@@ -291,6 +292,7 @@ pfd_status pfd_fp32_fma_rate(pfd_ctx* ctx, double* tflops)
     float ms = 0.0f;
     double flops = 0.0;
     CU(pfd::measure_fma_rate(ctx->stream, &ms, &flops));
+    ctx->launches += 4;                      // warm-up + three timed launches
     *tflops = flops / (ms * 1e-3) / 1e12;
     return PFD_OK;
 }
@@ -412,6 +414,7 @@ static pfd_status set_raw(pfd_ctx* ctx, int frame_id, const uint8_t* raw, int ra
     CU(cudaMemcpy2DAsync(f->d_raw, f->W, raw, raw_pitch, f->W, f->H,
                          device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     CU(pfd::launch_slice(f->d_raw, f->W, f->d_origin, f->V, f->mi_w, f->mi_h, f->tile_stride, f->d_gray, ctx->stream));
+    ctx->launches += 1;
     f->has_raw = true;
     f->has_state = false;
     return PFD_OK;
@@ -469,6 +472,7 @@ pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, 
     if (ctx->counting) P.tap_counter = ctx->d_taps;
     f->cur = 0;
     CU(pfd::launch_init(frame_dev(*f), P, f->s[0], ctx->d_err, ctx->stream));
+    ctx->launches += 1;
     f->has_state = true;
     return PFD_OK;
 }
@@ -509,6 +513,7 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
     P.cost_scratch = ctx->d_scratch;
     CU(pfd::launch_sweep(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                          ctx->stream));
+    ctx->launches += 1;
     f->cur ^= 1;
     return PFD_OK;
 }
@@ -582,6 +587,8 @@ pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params
         pfd::launch_ncc(frame_dev(*f), P, nseg, npb, d_segv, d_segs, d_segl, d_pxy, d_plane, d_out, d_cost,
                         ctx->d_err, s) != cudaSuccess)
         rc = PFD_ECUDA;
+    else if (rc == PFD_OK)
+        ctx->launches += 1;
     if (rc == PFD_OK &&
         cudaMemcpyAsync(costs, d_cost, sizeof(float) * (size_t)n * f->K, cudaMemcpyDeviceToHost, s) != cudaSuccess)
         rc = PFD_ECUDA;
@@ -689,6 +696,7 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
         const int a = f->step_start[s], b = f->step_start[s + 1];
         cudaError_t e = pfd::launch_filter_step(F, fc, S, f->d_steps + a, b - a, f->d_reason, d_stats, ctx->stream);
         if (e != cudaSuccess) { cudaFreeAsync(d_stats, ctx->stream); return fail(ctx, PFD_ECUDA, "filter step: %s", cudaGetErrorString(e)); }
+        ctx->launches += 1;
     }
     unsigned long long h[8] = {};
     if (stats) CU(cudaMemcpyAsync(h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
@@ -719,6 +727,7 @@ pfd_status pfd_reprojection_error(pfd_ctx* ctx, int frame_id, const pfd_filter_c
     pfd::FilterCfg fc;
     std::memcpy(&fc, cfg, sizeof(fc));
     CU(pfd::launch_reproj(check_frame(*f, baseline_unit), fc, f->s[f->cur], f->d_err, ctx->stream));
+    ctx->launches += 1;
     if (err) {
         CU(cudaMemcpyAsync(err, f->d_err, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
@@ -761,6 +770,7 @@ pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg,
     CU(cudaMemsetAsync(f->d_cyc_hist, 0, sizeof(unsigned int) * pfd::kCycleHistBins, ctx->stream));
     CU(pfd::launch_cycle(F, cc, f->s[f->cur], maps ? f->d_cyc_maps : nullptr, maps ? f->d_cyc_maps + px : nullptr,
                          maps ? f->d_cyc_tm : nullptr, f->d_cyc_recs, f->d_cyc_hist, ctx->stream));
+    ctx->launches += 1;
     std::vector<pfd::CycleTileRec> rec(f->V);
     unsigned int hist[pfd::kCycleHistBins];
     CU(cudaMemcpyAsync(rec.data(), f->d_cyc_recs, sizeof(pfd::CycleTileRec) * rec.size(), cudaMemcpyDeviceToHost,
@@ -883,6 +893,13 @@ static pfd_status build_lens_grid(pfd_ctx* ctx, Frame& f)
     return PFD_OK;
 }
 
+pfd_status pfd_launch_count(pfd_ctx* ctx, unsigned long long* n)
+{
+    if (!ctx || !n) return PFD_EINVAL;
+    *n = ctx->launches;
+    return PFD_OK;
+}
+
 pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_slices, int out_w, int out_h,
                        float* out)
 {
@@ -919,6 +936,7 @@ pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_
     if (pfd::refocus_smem_bytes(R) > 227 * 1024) return fail(ctx, PFD_EINVAL, "refocus: micro-image too large");
     CU(cudaMemcpyAsync(f->d_slice_vd, slice_vd, sizeof(float) * n_slices, cudaMemcpyHostToDevice, ctx->stream));
     CU(pfd::launch_refocus(R, f->d_slice_vd, n_slices, f->W, f->H, out_w, out_h, f->d_stack, ctx->d_err, ctx->stream));
+    ctx->launches += 1;
     if (out) CU(cudaMemcpyAsync(out, f->d_stack, need, cudaMemcpyDeviceToHost, ctx->stream));
     return out ? check_device_error(ctx) : PFD_OK;
 }
@@ -1024,6 +1042,7 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     P.cost_scratch = scratch;
     CU(pfd::launch_sweep(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                          ctx->stream));
+    ctx->launches += 1;
     f->cur ^= 1;
     return PFD_OK;
 }
