@@ -128,12 +128,13 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
  * For callers that cannot allocate device memory once frames are streaming: an
  * application whose memory pool claimed all free HBM at start-up, or a
  * real-time loop that forbids cudaMalloc/cudaFree because they can synchronise
- * the whole device.  The candidate-cost scratch is a fixed 16 MiB array in the
+ * the whole device.  The cost-vector scratch is a fixed 8 MiB array in the
  * library's device image (held by every GPU that loads the library, until
  * exit) instead of a cudaMalloc'd buffer; inputs and outputs are the frame's
  * state exactly as for pfd_pm_sweep, and the results are the same bit for bit.
- * Limit: the array must hold one CTA's scratch (9 x max_nb x 128 floats) for
- * every SM, so max_nb <= 24 on a 148-SM B200; larger frames get PFD_EINVAL.
+ * Limit: the array must hold one CTA's scratch (eight warps, each the cost
+ * vectors of one pixel) for every SM, so max_nb <= 28 on a 148-SM B200;
+ * larger frames get PFD_EINVAL.
  * The first call on a device looks up the array's device address, so make
  * that call before any stream capture.  All calls on a device share the one
  * array (nothing in it has to start at zero): calls whose kernels overlap on

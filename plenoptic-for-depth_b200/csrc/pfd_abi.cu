@@ -490,11 +490,11 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
     DeviceGuard g(ctx->device);
     pfd::PmParams P = make_params(*f, params, seed);
     if (ctx->counting) P.tap_counter = ctx->d_taps;
-    if (pfd::sweep_smem_bytes(P, 128, f->has_blur) > 227 * 1024)
+    if (pfd::sweep_warp_smem_bytes(P, f->has_blur) > 227 * 1024)
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
     int n_ctas = 0;
-    CU(pfd::sweep_grid(P, f->has_blur, &n_ctas));
-    const size_t need = pfd::sweep_scratch_bytes(P, n_ctas, 1);
+    CU(pfd::sweep_warp_grid(P, f->has_blur, &n_ctas));
+    const size_t need = pfd::sweep_warp_scratch_bytes(P, n_ctas);
     if (need > ctx->scratch_bytes) {
         if (ctx->budget && ctx->used - ctx->scratch_bytes + need > ctx->budget)
             return fail(ctx, PFD_ENOMEM, "HBM budget exceeded by %zu bytes of sweep scratch", need);
@@ -511,8 +511,8 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
         ctx->used += need;
     }
     P.cost_scratch = ctx->d_scratch;
-    CU(pfd::launch_sweep(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
-                         ctx->stream));
+    CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
+                              ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
     return PFD_OK;
@@ -970,11 +970,13 @@ pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane, float* cost, f
 // pfd_pm_sweep_noalloc runs the same kernel on a fixed array that is part of
 // the library's device image instead.
 
-// 16 MiB, held by every GPU that loads the library until the process exits.
-// One CTA uses 9 x max_nb x 128 floats; the array must hold at least one CTA
-// per SM, so max_nb <= 24 on a 148-SM B200.  Nothing in it needs to start at
-// zero: a sweep writes every entry it reads, earlier in the same work item.
-static __device__ __align__(256) float g_noalloc_scratch[(size_t(16) << 20) / sizeof(float)];
+// 8 MiB, held by every GPU that loads the library until the process exits.
+// Each warp of the sweep keeps the cost vectors of its current pixel here,
+// (2 (max_nb + 1) max_nb + 3 (max_nb + 1)) words rounded up to 32, eight warps
+// per CTA; the array must hold at least one CTA per SM, so max_nb <= 28 on a
+// 148-SM B200.  Nothing in it needs to start at zero: a sweep writes every
+// entry it reads, earlier for the same pixel.
+static __device__ __align__(256) float g_noalloc_scratch[(size_t(8) << 20) / sizeof(float)];
 
 namespace {
 
@@ -1021,27 +1023,33 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     DeviceGuard g(ctx->device);
     pfd::PmParams P = make_params(*f, params, seed);
     if (ctx->counting) P.tap_counter = ctx->d_taps;
-    if (pfd::sweep_smem_bytes(P, 128, f->has_blur) > 227 * 1024)
+    if (pfd::sweep_warp_smem_bytes(P, f->has_blur) > 227 * 1024)
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
     int sms = 0;
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    const size_t per_cta = pfd::sweep_scratch_bytes(P, 1, 1);
+    const size_t per_cta = pfd::sweep_warp_scratch_bytes(P, 1);
     const size_t fit = kNoAllocScratchBytes / per_cta;
-    if (fit < (size_t)sms)
+    if (fit < (size_t)sms) {
+        int kmax = 0;                            // largest max_nb whose CTAs still cover every SM
+        for (int k = 1; k <= pfd::kMaxNb; ++k) {
+            pfd::PmParams Q = P;
+            Q.K = k;
+            if (kNoAllocScratchBytes / pfd::sweep_warp_scratch_bytes(Q, 1) >= (size_t)sms) kmax = k;
+        }
         return fail(ctx, PFD_EINVAL,
                     "pfd_pm_sweep_noalloc: %d neighbours need %zu bytes of scratch per CTA; the fixed %zu-byte "
-                    "scratch holds %zu CTAs, fewer than the %d SMs (at most %zu neighbours on this device)",
-                    f->K, per_cta, kNoAllocScratchBytes, fit, sms,
-                    kNoAllocScratchBytes / ((size_t)sms * (per_cta / (size_t)f->K)));
+                    "scratch holds %zu CTAs, fewer than the %d SMs (at most %d neighbours on this device)",
+                    f->K, per_cta, kNoAllocScratchBytes, fit, sms, kmax);
+    }
     int n_ctas = 0;
-    CU(pfd::sweep_grid(P, f->has_blur, &n_ctas));
+    CU(pfd::sweep_warp_grid(P, f->has_blur, &n_ctas));
     n_ctas = (int)std::min<size_t>((size_t)n_ctas, fit);
     float* scratch = nullptr;
     st = noalloc_scratch(ctx, ctx->device, &scratch);
     if (st != PFD_OK) return st;
     P.cost_scratch = scratch;
-    CU(pfd::launch_sweep(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
-                         ctx->stream));
+    CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
+                              ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
     return PFD_OK;

@@ -23,6 +23,13 @@ cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, 
                        const int* seg_start, const int* seg_len, const int* hyp_pxy, const float4* hyp_plane,
                        const int* hyp_out, float* costs, int* err, cudaStream_t st);
 int sweep_smem_bytes(const PmParams& P, int npb, bool blur);
+// The warp-per-pixel sweep (pm_sweep.cu): grid, shared memory, and the global
+// scratch it needs (P.cost_scratch: per warp, the cost vectors of one pixel).
+cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas);
+int sweep_warp_smem_bytes(const PmParams& P, bool blur);
+size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas);
+cudaError_t launch_sweep_warp(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
+                              int iter, int phase, int n_ctas, int* err, cudaStream_t st);
 // FP32 FFMA throughput probe (diag.cu): best of three timed launches.
 cudaError_t measure_fma_rate(cudaStream_t st, float* ms, double* flops);
 

@@ -1,0 +1,836 @@
+// pm_sweep.cu -- CheckerboardUpdateFrame (MIStereo/AdaptMIPMFrame.cu:520-947)
+// with one warp per updated pixel.
+//
+// A CTA stages one micro-image and its neighbours at a time; its warps take the
+// updated pixels of that micro-image one by one.  For a pixel, every cost
+// evaluation the reference makes (the 8 propagation candidates and the
+// current plane, the cross-view proposals, the 5 refinement candidates) is a
+// set of (hypothesis, neighbour) NCCs; the warp lays them across its lanes,
+// one NCC per lane, and walks the pixel's patch window (patch intersected
+// with the micro-image, the same for every lane) tap by tap.  The
+// reference-side values of a tap (bilateral weight w, w * r, r and the blur
+// term) are computed once per pixel into a per-warp table and read as a
+// broadcast.  Each lane accumulates its NCC's six moments in the reference's
+// tap order (x offset outer, y offset inner); a tap whose source sample
+// leaves the neighbour window adds exact zeros.
+//
+// Cross-view proposals depend on the best plane so far (AdaptMIPMFrame.cu:
+// 907-936): they are built speculatively from the best plane after
+// propagation and evaluated together, then walked in order; a proposal whose
+// neighbour-window sample position changed because an earlier one won is
+// rebuilt and evaluated again, so the result is the sequential one.
+//
+// Neighbour micro-images are held as 32-bit quads: entry (iy, ix) packs the
+// four texels of a bilinear footprint, T(iy,ix), T(iy,ix+1), T(iy+1,ix),
+// T(iy+1,ix+1), indices clamped to the window.  A fetch is one 4-byte load.
+#include <algorithm>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "pm_device.cuh"
+#include "pm_kernels.h"
+
+namespace pfd {
+
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = 32 * kWarps;
+
+struct Quad {
+    const float* R;          // [H][W] reference texels
+    const float* RB;         // [H][W] reference blur or nullptr
+    uint32_t q_addr;         // shared address of neighbour quads [K][H+1][W+1]
+    uint32_t qb_addr;        // same for blur
+    int qs;                  // W + 1
+    int q_bytes;             // (H + 1) * (W + 1) * 4
+    const NbGeo* geo;        // [K]
+    const int* nb_ok;        // [K]
+    const float* a_s;        // [ntap * ntap]
+    const float* a_c;        // [256]
+};
+
+// Per-warp scratch.  The tap table and the hypotheses, read on every tap, are
+// in shared memory; the cost vectors and their bookkeeping, written once per
+// NCC, are in the warp's slice of global scratch (P.cost_scratch), where they
+// stay in L1/L2 and leave shared memory to more resident warps.
+struct WarpBlock {
+    float4* tab;             // [tab_n] (w, w * r, r, r_blur / 255) of the current pixel's window (shared)
+    float4* plane;           // [maxh] hypotheses (shared)
+    float4* dp;              // [maxh] disparity plane (x, y, z) and disparity at the pixel (w) (shared)
+    float* cost;             // [maxh][K] (global)
+    int* pair;               // [maxh * K] compacted (hypothesis, neighbour) indices (global)
+    float* wres;             // [maxh] weighted cost (global)
+    int* wmin;               // [maxh] index of the lowest cost (global)
+    int* aux;                // [maxh] proposal sample position, or -1 (global)
+};
+
+// Hypotheses one evaluation can hold: 9 propagation slots, or every selected
+// view's proposal plus one rebuilt proposal.
+__host__ __device__ inline int sweep_maxh(int K) { return K + 1 > 9 ? K + 1 : 9; }
+// 4-byte words of global scratch per warp.
+__host__ __device__ inline int sweep_warp_words(int K)
+{
+    const int mh = sweep_maxh(K);
+    return ((2 * mh * K + 3 * mh) + 31) & ~31;
+}
+
+struct Plan {
+    int off_Q, off_QB, off_R, off_RB, off_geo, off_ok, off_as, off_ac, off_pc, off_ps, off_stage, off_bar, off_ctl;
+    int off_warp, warp_bytes, tab_n, maxh;
+    int total;
+
+    __host__ __device__ static int a16(int v) { return (v + 15) & ~15; }
+    __host__ __device__ static Plan make(int W, int H, int K, int ntap, bool blur, int tile_stride)
+    {
+        Plan p;
+        int o = 0;
+        const int qb = (H + 1) * (W + 1) * 4;
+        p.off_Q = o;     o += a16(K * qb);
+        p.off_QB = o;    o += blur ? a16(K * qb) : 0;
+        p.off_R = o;     o += a16(W * H * 4);
+        p.off_RB = o;    o += blur ? a16(W * H * 4) : 0;
+        p.off_geo = o;   o += a16(K * (int)sizeof(NbGeo));
+        p.off_ok = o;    o += a16(K * 4);
+        p.off_as = o;    o += a16(ntap * ntap * 4);
+        p.off_ac = o;    o += 256 * 4;
+        p.off_pc = o;    o += a16(W * H * 4);
+        p.off_ps = o;    o += a16(W * H * 4);
+        p.off_bar = o;   o += 16;
+        p.off_ctl = o;   o += 16;
+        p.off_stage = o; o += a16((1 + K) * tile_stride * (blur ? 2 : 1));
+        p.tab_n = (ntap < W ? ntap : W) * (ntap < H ? ntap : H);
+        p.maxh = sweep_maxh(K);
+        p.warp_bytes = a16(p.tab_n * 16) + a16(2 * p.maxh * 16);
+        p.off_warp = o;  o += kWarps * p.warp_bytes;
+        p.total = o;
+        return p;
+    }
+    __device__ WarpBlock warp_block(unsigned char* smem, float* gscratch, int w, int K) const
+    {
+        unsigned char* b = smem + off_warp + w * warp_bytes;
+        WarpBlock S;
+        S.tab = (float4*)b;                  b += a16(tab_n * 16);
+        S.plane = (float4*)b;
+        S.dp = S.plane + maxh;
+        float* g = gscratch + ((size_t)blockIdx.x * kWarps + w) * sweep_warp_words(K);
+        S.cost = g;
+        S.pair = (int*)(g + maxh * K);
+        S.wres = g + 2 * maxh * K;
+        S.wmin = (int*)(S.wres + maxh);
+        S.aux = S.wmin + maxh;
+        return S;
+    }
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint32_t lds_u32(uint32_t addr)
+{
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr));
+    return v;
+}
+
+// Linear-filter fetch of the measured texture unit (see Tiles in pm_device.cuh)
+// from a quad entry: 256 s = 256 T00 + a (T10 - T00) + b (T01 - T00) + w11 (T11 - T01 - T10 + T00).
+__device__ __forceinline__ float quad_blend(int tbx, int tby, uint32_t q)
+{
+    const int a = tbx & 0xFF, b = tby & 0xFF;
+    const int w11 = (a * b + 128) >> 8;
+    const int t00 = (int)(q & 0xFFu), t10 = (int)((q >> 8) & 0xFFu);
+    const int t01 = (int)((q >> 16) & 0xFFu), t11 = (int)(q >> 24);
+    const int d1 = t10 - t00;
+    const int s256 = (t00 << 8) + a * d1 + b * (t01 - t00) + w11 * (t11 - t01 - d1);
+    return __fsub_rn(__int_as_float(s256 | 0x47000000), 32768.0f);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return done != 0;
+}
+// Bounded wait (about 2^22 polls): records PFD_DEVERR_TMA_TIMEOUT and gives up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err)
+{
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (it > 64) __nanosleep(128);
+    }
+    if (err) atomicOr(err, PFD_DEVERR_TMA_TIMEOUT);
+    return false;
+}
+
+// Stages micro-image vid and its neighbours: bulk copies of the 8-bit tiles,
+// then the reference as floats and the neighbours as quads.  The mbarrier is
+// reused with alternating parity, one phase per staged view.
+template <bool BLUR>
+__device__ bool stage_view(unsigned char* smem, const Plan& L, const FrameDev& F, const PmParams& P, int vid, int nc,
+                           uint32_t parity, int* err, Quad& T)
+{
+    const int W = P.W, H = P.H, K = P.K, ts = P.tile_stride;
+    uint8_t* stage = (uint8_t*)(smem + L.off_stage);
+    uint64_t* bar = (uint64_t*)(smem + L.off_bar);
+    const int nt = 1 + nc;
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(nt * ts * (BLUR ? 2 : 1)));
+        for (int i = 0; i < nt; ++i) {
+            const int v = (i == 0) ? vid : F.nb_ids[vid * K + i - 1];
+            const int vv = v < 0 ? vid : v;
+            bulk_copy_g2s(stage + i * ts, F.gray + (size_t)vv * ts, (uint32_t)ts, bar);
+            if (BLUR) bulk_copy_g2s(stage + (nt + i) * ts, F.blur + (size_t)vv * ts, (uint32_t)ts, bar);
+        }
+    }
+    NbGeo* geo = (NbGeo*)(smem + L.off_geo);
+    int* okk = (int*)(smem + L.off_ok);
+    const float2 c0 = F.centers[vid];
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int v = (k < nc) ? F.nb_ids[vid * K + k] : -1;
+        okk[k] = (v >= 0);
+        geo[k] = make_geo(c0, F.centers[v >= 0 ? v : vid], P);
+    }
+    const bool ok = mbar_wait_bounded(bar, parity, err);
+    if (__syncthreads_or(!ok)) return false;
+    float* R = (float*)(smem + L.off_R);
+    for (int e = threadIdx.x; e < W * H; e += blockDim.x) R[e] = (float)stage[e];
+    if (BLUR) {
+        float* RB = (float*)(smem + L.off_RB);
+        for (int e = threadIdx.x; e < W * H; e += blockDim.x) RB[e] = (float)stage[nt * ts + e];
+    }
+    const int qs = W + 1, qn = (H + 1) * qs;
+    uint32_t* Q = (uint32_t*)(smem + L.off_Q);
+    uint32_t* QB = (uint32_t*)(smem + L.off_QB);
+    for (int e = threadIdx.x; e < nc * qn; e += blockDim.x) {
+        const int k = e / qn, r = e % qn;
+        const int iy = r / qs, ix = r % qs;
+        const int y0 = min(iy, H - 1), y1 = min(iy + 1, H - 1);
+        const int x0 = min(ix, W - 1), x1 = min(ix + 1, W - 1);
+        const uint8_t* s = stage + (1 + k) * ts;
+        Q[e] = (uint32_t)s[y0 * W + x0] | ((uint32_t)s[y0 * W + x1] << 8) | ((uint32_t)s[y1 * W + x0] << 16) |
+               ((uint32_t)s[y1 * W + x1] << 24);
+        if (BLUR) {
+            const uint8_t* sb = stage + (nt + 1 + k) * ts;
+            QB[e] = (uint32_t)sb[y0 * W + x0] | ((uint32_t)sb[y0 * W + x1] << 8) |
+                    ((uint32_t)sb[y1 * W + x0] << 16) | ((uint32_t)sb[y1 * W + x1] << 24);
+        }
+    }
+    T.R = R;
+    T.RB = BLUR ? (const float*)(smem + L.off_RB) : nullptr;
+    T.q_addr = smem_u32(Q);
+    T.qb_addr = BLUR ? smem_u32(QB) : 0u;
+    T.qs = qs;
+    T.q_bytes = qn * 4;
+    T.geo = geo;
+    T.nb_ok = okk;
+    T.a_s = (const float*)(smem + L.off_as);
+    T.a_c = (const float*)(smem + L.off_ac);
+    return true;
+}
+
+// The pixel's patch window: the patch's taps (x offset i, y offset j, step inc)
+// that fall inside the micro-image, as a rectangle of nX x nY taps.
+struct PixWin {
+    int x0, y0, nX, nY;      // first tap position and tap counts
+    int ii0, jj0;            // offset index of the first tap ((x0 - px + r) / inc)
+};
+
+__device__ __forceinline__ PixWin pixel_window(const PmParams& P, int px, int py)
+{
+    PixWin w;
+    const int r = P.radius, inc = P.inc;
+    const int sx = max(0, (r - px + inc - 1) / inc), sy = max(0, (r - py + inc - 1) / inc);
+    w.ii0 = sx;
+    w.jj0 = sy;
+    w.x0 = px - r + sx * inc;
+    w.y0 = py - r + sy * inc;
+    const int ex = min(P.ntap - 1, (P.W - 1 - px + r) / inc), ey = min(P.ntap - 1, (P.H - 1 - py + r) / inc);
+    w.nX = max(0, ex - sx + 1);
+    w.nY = max(0, ey - sy + 1);
+    return w;
+}
+
+// Reference-side table of the pixel: (w, w r, r, r_blur / 255) per tap, x outer.
+template <bool BLUR>
+__device__ __forceinline__ void build_table(const Quad& T, const PmParams& P, const PixWin& pw, int px, int py,
+                                            float4* tab, int lane)
+{
+    const int W = P.W, inc = P.inc;
+    const float rc = T.R[py * W + px];
+    const int n = pw.nX * pw.nY;
+    for (int t = lane; t < n; t += 32) {
+        const int ix = t / pw.nY, iy = t - ix * pw.nY;
+        const int X = pw.x0 + ix * inc, Y = pw.y0 + iy * inc;
+        const float rv = T.R[Y * W + X];
+        const float cd = fabsf(__fsub_rn(rv, rc));
+        const int cdi = __float_as_int(__fadd_rn(cd, 8388608.0f)) & 0xFF;
+        const int ti = (pw.ii0 + ix) * P.ntap + (pw.jj0 + iy);
+        const float w = pfd_expf_nonpos(__fsub_rn(T.a_s[ti], T.a_c[cdi]));
+        const float rb = BLUR ? __fdiv_rn(T.RB[Y * W + X], 255.0f) : 0.0f;
+        tab[t] = make_float4(w, __fmul_rn(w, rv), rv, rb);
+    }
+}
+
+// One lane's NCC (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:73-179) of the
+// pixel under plane dp against neighbour k.  Every lane of the warp walks the
+// same taps; inactive lanes add zeros.
+template <bool BLUR, bool COUNT>
+__device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, const float4* tab, const PixWin& pw,
+                                          float3 dp, int k, bool active, unsigned& ntaps)
+{
+    const NbGeo& g = T.geo[k];
+    const float stx = g.stx, sty = g.sty;
+    const uint32_t fold = 0x4B0000u * (uint32_t)(T.qs + 1) * 4u;
+    const uint32_t base = T.q_addr + (uint32_t)(k * T.q_bytes) - fold;
+    const uint32_t bbase = BLUR ? T.qb_addr + (uint32_t)(k * T.q_bytes) - fold : 0u;
+    const uint32_t qs = (uint32_t)T.qs;
+    float sr = 0.f, srr = 0.f, ss = 0.f, sss = 0.f, srs = 0.f, sw = 0.f, bsx = 0.f, bsy = 0.f;
+    const float finc = (float)P.inc;
+    float fxr = (float)pw.x0;
+    int t = 0;
+    for (int ix = 0; ix < pw.nX; ++ix, fxr = __fadd_rn(fxr, finc)) {
+        const float axr = __fmul_rn(dp.x, fxr);
+        float fyr = (float)pw.y0;
+        for (int iy = 0; iy < pw.nY; ++iy, ++t, fyr = __fadd_rn(fyr, finc)) {
+            const float4 e = tab[t];
+            const float d = __fadd_rn(__fmaf_rn(dp.y, fyr, axr), dp.z);
+            const float sx = __fmaf_rn(stx, d, fxr);
+            const float sy = __fmaf_rn(sty, d, fyr);
+            const bool v = active && (__float_as_uint(sx) < P.W_bits) && (__float_as_uint(sy) < P.H_bits);
+            if (COUNT) ntaps += v ? 1u : 0u;
+            const int tbx = tex_coord_bits(sx), tby = tex_coord_bits(sy);
+            const uint32_t rel = (((uint32_t)(tby >> 8) * qs + (uint32_t)(tbx >> 8)) << 2);
+            const uint32_t q = lds_u32(v ? base + rel : T.q_addr);
+            const float s = quad_blend(tbx, tby, q);
+            const float wv = v ? e.x : 0.0f;
+            const float wrv = v ? e.y : 0.0f;
+            const float rv = e.z;
+            const float ws = __fmul_rn(wv, s);
+            sr = __fmaf_rn(wv, rv, sr);
+            srr = __fmaf_rn(wrv, rv, srr);
+            ss = __fmaf_rn(wv, s, ss);
+            sss = __fmaf_rn(ws, s, sss);
+            srs = __fmaf_rn(wrv, s, srs);
+            sw = __fadd_rn(sw, wv);
+            if (BLUR) {
+                const uint32_t qb = lds_u32(v ? bbase + rel : T.qb_addr);
+                const float sb = quad_blend(tbx, tby, qb);
+                bsx = __fadd_rn(bsx, v ? e.w : 0.0f);
+                bsy = __fadd_rn(bsy, v ? __fdiv_rn(sb, 255.0f) : 0.0f);
+            }
+        }
+    }
+    float c = kCostMax;
+    if (sw > 1e-6f) {
+        const float inv = __fdiv_rn(1.0f, sw);
+        const float m_r = __fmul_rn(sr, inv), m_rr = __fmul_rn(srr, inv);
+        const float m_s = __fmul_rn(ss, inv), m_ss = __fmul_rn(sss, inv);
+        const float m_rs = __fmul_rn(srs, inv);
+        const float var_r = __fmaf_rn(-m_r, m_r, m_rr);
+        const float var_s = __fmaf_rn(-m_s, m_s, m_ss);
+        if (!(var_r < 1e-5f || var_s < 1e-5f)) {
+            const float cov = __fmaf_rn(-m_r, m_s, m_rs);
+            const float vv = __fsqrt_rn(__fmul_rn(var_r, var_s));
+            c = clamp_cost(__fsub_rn(1.0f, __fdiv_rn(cov, vv)));
+        }
+    }
+    if (BLUR) {
+        const float tb = __fsub_rn(bsx, bsy);
+        const float bw = pfd_expf(__fmul_rn(__fmul_rn(-0.007368f, tb), tb));
+        c = clamp_cost(__fmaf_rn(2.0f, __fsub_rn(1.0f, bw), c));
+    }
+    return c;
+}
+
+// Cost vectors (ComputeMultiViewCostVector_Frame, AdaptMIPMFrame.cu:181-225) of
+// hypotheses S.plane[0..nh) at (px, py): S.cost[h * K + k] for k < nc.  A
+// neighbour whose anchor leaves the window gets 2 without evaluation.
+template <bool BLUR, bool COUNT>
+__device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const WarpBlock& S, const PixWin& pw,
+                                       int px, int py, int nh, int nc, int lane)
+{
+    const int K = P.K;
+    for (int h = lane; h < nh; h += 32) {
+        const float3 dp = disparity_plane(px, py, S.plane[h]);
+        S.dp[h] = make_float4(dp.x, dp.y, dp.z, to_disparity(px, py, dp));
+    }
+    __syncwarp();
+    const int total = nh * nc;
+    int np = 0;
+    for (int n0 = 0; n0 < total; n0 += 32) {
+        const int n = n0 + lane;
+        bool need = false;
+        if (n < total) {
+            const int h = n / nc, k = n - h * nc;
+            if (T.nb_ok[k]) {
+                const float2 a = geo_anchor(T.geo[k], px, py, S.dp[h].w);
+                need = (__float_as_uint(a.x) < P.W_bits) && (__float_as_uint(a.y) < P.H_bits);
+            }
+            if (!need) S.cost[h * K + k] = kCostMax;
+        }
+        const unsigned m = __ballot_sync(kFullMask, need);
+        if (need) S.pair[np + __popc(m & ((1u << lane) - 1u))] = n;
+        np += __popc(m);
+    }
+    __syncwarp();
+    unsigned ntaps = 0;
+    for (int p0 = 0; p0 < np; p0 += 32) {
+        const bool act = p0 + lane < np;
+        const int n = act ? S.pair[p0 + lane] : 0;
+        const int h = n / nc, k = n - h * nc;
+        const float4 d = S.dp[h];
+        const float c = ncc_lane<BLUR, COUNT>(T, P, S.tab, pw, make_float3(d.x, d.y, d.z), k, act, ntaps);
+        if (act) S.cost[h * K + k] = c;
+    }
+    if (COUNT) {
+        const unsigned tot = __reduce_add_sync(kFullMask, ntaps);
+        if (lane == 0 && tot) atomicAdd(P.tap_counter, (unsigned long long)tot);
+    }
+    __syncwarp();
+}
+
+// ComputeWeightedCost_Frame (AdaptMIPMFrame.cu:284-317) of hypotheses [0, nh),
+// one lane per hypothesis; view weights packed 4 bits per view.
+__device__ __forceinline__ void weigh_hyps(const WarpBlock& S, int K, int nh, int nc, uint64_t vw_lo, uint64_t vw_hi,
+                                           int lane)
+{
+    for (int h = lane; h < nh; h += 32) {
+        WeightedCost wc;
+        for (int k = 0; k < nc; ++k) {
+            const float w = (float)((k < 16 ? vw_lo >> (k * 4) : vw_hi >> ((k - 16) * 4)) & 15ull);
+            wc.add(k, S.cost[h * K + k], w);
+        }
+        S.wres[h] = wc.result();
+        S.wmin[h] = wc.min_idx;
+    }
+    __syncwarp();
+}
+
+// The g-th pixel (row-major) whose colour (x + y) & 1 equals `colour`.
+__device__ __forceinline__ bool nth_pixel(int g, int colour, int W, int H, int& x, int& y)
+{
+    for (int yy = 0; yy < H; ++yy) {
+        const int x0 = (colour ^ yy) & 1;
+        const int cnt = (W - x0 + 1) >> 1;
+        if (g < cnt) { x = x0 + 2 * g; y = yy; return true; }
+        g -= cnt;
+    }
+    return false;
+}
+
+__device__ __forceinline__ int nth_set_bit(uint32_t m, int n)
+{
+    for (int i = 0; i < n && m; ++i) m &= m - 1;
+    return m ? __ffs(m) - 1 : -1;
+}
+
+struct Cands {
+    int flag[8];
+    int pos[8];
+    int src[8];
+};
+
+// Candidate positions of AdaptMIPMFrame.cu:589-795: per direction the lowest
+// prev-cost sample among the scan pattern.
+__device__ __forceinline__ void find_candidates(const float* pc, int x, int y, int W, int H, Cands& C)
+{
+    const int center = y * W + x;
+    for (int a = 0; a < 8; ++a) { C.flag[a] = 0; C.pos[a] = center; C.src[a] = -1; }
+    auto scan = [&](int start, const int* pts, const bool* ok, int n) {
+        float cm = pc[start];
+        int cp = start;
+        for (int i = 0; i < n; ++i)
+            if (ok[i] && pc[pts[i]] < cm) { cm = pc[pts[i]]; cp = pts[i]; }
+        return cp;
+    };
+    if (y > 2) {
+        const int s = center - 3 * W; const int pts[1] = { s - W }; const bool ok[1] = { y > 3 };
+        C.flag[1] = 1; C.pos[1] = scan(s, pts, ok, 1);
+    }
+    if (y < H - 3) {
+        const int s = center + 3 * W; const int pts[1] = { s + W }; const bool ok[1] = { y < H - 4 };
+        C.flag[3] = 1; C.pos[3] = scan(s, pts, ok, 1);
+    }
+    if (x > 2) {
+        const int s = center - 3; const int pts[1] = { s - 1 }; const bool ok[1] = { x > 3 };
+        C.flag[5] = 1; C.pos[5] = scan(s, pts, ok, 1);
+    }
+    if (x < W - 3) {
+        const int s = center + 3; const int pts[1] = { s + 1 }; const bool ok[1] = { x < W - 4 };
+        C.flag[7] = 1; C.pos[7] = scan(s, pts, ok, 1);
+    }
+    if (y > 0) {
+        const int s = center - W;
+        const int pts[4] = { s - W, s - W, s - 2 * W - 1, s - 2 * W + 1 };
+        const bool ok[4] = { y > 1 && x > 0, y > 1 && x < W - 1, y > 2 && x > 1, y > 2 && x < W - 2 };
+        C.flag[0] = 1; C.pos[0] = scan(s, pts, ok, 4);
+    }
+    if (y <= 2 && y > 0) { C.flag[1] = 1; C.pos[1] = C.pos[0]; C.src[1] = 0; }
+    if (y < H - 1) {
+        const int s = center + W;
+        const int pts[4] = { s + W, s + W, s + 2 * W - 1, s + 2 * W + 1 };
+        const bool ok[4] = { y < H - 2 && x > 0, y < H - 2 && x < W - 1, y < H - 3 && x > 1, y < H - 3 && x < W - 2 };
+        C.flag[2] = 1; C.pos[2] = scan(s, pts, ok, 4);
+    }
+    if (y >= H - 3 && y < H - 1) { C.flag[3] = 1; C.pos[3] = C.pos[2]; C.src[3] = 2; }
+    if (x > 0) {
+        const int s = center - 1;
+        const int pts[4] = { s - 1, s - 1, s - 2 - W, s - 2 + W };
+        const bool ok[4] = { x > 1 && y > 0, x > 1 && y < H - 1, x > 2 && y > 1, x > 2 && y < H - 2 };
+        C.flag[4] = 1; C.pos[4] = scan(s, pts, ok, 4);
+    }
+    if (x <= 2 && x > 0) { C.flag[5] = 1; C.pos[5] = C.pos[4]; C.src[5] = 4; }
+    if (x < W - 1) {
+        const int s = center + 1;
+        const int pts[4] = { s + 1, s + 1, s + 2 - W, s + 2 + W };
+        const bool ok[4] = { x < W - 2 && y > 0, x < W - 2 && y < H - 1, x < W - 3 && y > 1, x < W - 3 && y < H - 2 };
+        C.flag[6] = 1; C.pos[6] = scan(s, pts, ok, 4);
+    }
+    if (x >= W - 3 && x < W - 1) { C.flag[7] = 1; C.pos[7] = C.pos[6]; C.src[7] = 6; }
+}
+
+// BuildCrossViewPlaneProposal (AdaptMIPMFrame.cu:350-398): the sample position
+// q (local index) of pixel (x, y) under `cur` in neighbour k, or -1.
+__device__ __forceinline__ int proposal_pos(const NbGeo& gk, int x, int y, int W, int H, float4 cur)
+{
+    const float dcur = to_disparity(x, y, disparity_plane(x, y, cur));
+    const float2 qf = geo_anchor(gk, x, y, dcur);
+    const float fqx = floorf(__fadd_rn(qf.x, 0.5f)), fqy = floorf(__fadd_rn(qf.y, 0.5f));
+    if (!(fqx >= 0.0f && fqx < (float)W && fqy >= 0.0f && fqy < (float)H)) return -1;
+    return (int)fqy * W + (int)fqx;
+}
+
+__device__ __forceinline__ float4 proposal_plane(const NbGeo& gk, const float4* nb_plane, int q, int x, int y, int W)
+{
+    const int qx = q % W, qy = q / W;
+    const float4 hn = nb_plane[q];
+    const float3 dpn = disparity_plane(qx, qy, hn);
+    float denom = __fmaf_rn(dpn.y, gk.by, __fmaf_rn(dpn.x, gk.bx, 1.0f));
+    denom = safe_denom(denom);
+    return encode_plane(x, y, __fdiv_rn(dpn.x, denom), __fdiv_rn(dpn.y, denom), __fdiv_rn(dpn.z, denom));
+}
+
+}  // namespace
+
+template <bool BLUR, bool COUNT>
+__global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, PmParams P, StateDev prev,
+                                                                     StateDev next, int iter, int phase, int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int W = P.W, H = P.H, K = P.K;
+    const Plan L = Plan::make(W, H, K, P.ntap, BLUR, P.tile_stride);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const WarpBlock S = L.warp_block(smem, P.cost_scratch, warp, K);
+    float* pc = (float*)(smem + L.off_pc);
+    uint32_t* ps = (uint32_t*)(smem + L.off_ps);
+    int* ctl = (int*)(smem + L.off_ctl);
+    const int n_upd = (P.ppv + (phase == 0 ? 1 : 0)) / 2;      // pixels with (x + y) & 1 == phase
+    const uint32_t sweep_id = (uint32_t)(1 + 2 * iter + phase);
+
+    // per-launch tables and the staging barrier
+    {
+        float* a_s = (float*)(smem + L.off_as);
+        float* a_c = (float*)(smem + L.off_ac);
+        for (int t = threadIdx.x; t < P.ntap * P.ntap; t += blockDim.x) {
+            const float fi = (float)(-P.radius + (t / P.ntap) * P.inc);
+            const float fj = (float)(-P.radius + (t % P.ntap) * P.inc);
+            const float sd = __fsqrt_rn(__fmaf_rn(fj, fj, __fmul_rn(fi, fi)));
+            a_s[t] = __fdiv_rn(-sd, P.ss2);
+        }
+        for (int c = threadIdx.x; c < 256; c += blockDim.x) a_c[c] = __fdiv_rn((float)c, P.cc2);
+        if (threadIdx.x == 0) mbar_init((uint64_t*)(smem + L.off_bar), 1);
+        __syncthreads();
+    }
+
+    uint32_t parity = 0;
+    for (int vid = blockIdx.x; vid < F.V; vid += gridDim.x) {
+        const int nc = min(F.nb_counts[vid], K);
+        const size_t vbase = (size_t)vid * P.ppv;
+        // the other colour keeps its state; so does every pixel of a view without neighbours
+        for (int e = threadIdx.x; e < P.ppv; e += blockDim.x) {
+            const int ex = e % W, ey = e / W;
+            pc[e] = prev.cost[vbase + e];
+            ps[e] = prev.sel[vbase + e];
+            if (nc > 0 && ((ex + ey) & 1) == phase) continue;
+            next.plane[vbase + e] = prev.plane[vbase + e];
+            next.cost[vbase + e] = prev.cost[vbase + e];
+            next.disp[vbase + e] = prev.disp[vbase + e];
+            next.sel[vbase + e] = prev.sel[vbase + e];
+        }
+        if (nc <= 0) { __syncthreads(); continue; }
+        Quad T;
+        if (!stage_view<BLUR>(smem, L, F, P, vid, nc, parity, err, T)) return;
+        parity ^= 1u;
+        if (threadIdx.x == 0) ctl[0] = 0;
+        __syncthreads();
+
+        for (;;) {
+            int g = 0;
+            if (lane == 0) g = atomicAdd(&ctl[0], 1);
+            g = __shfl_sync(kFullMask, g, 0);
+            if (g >= n_upd) break;
+            int x = 0, y = 0;
+            nth_pixel(g, phase, W, H, x, y);
+            const int center = y * W + x;
+            const size_t idx = vbase + center;
+            const PixWin pw = pixel_window(P, x, y);
+            build_table<BLUR>(T, P, pw, x, y, S.tab, lane);
+
+            // ---- propagation candidates and the current plane --------------
+            Cands C;
+            find_candidates(pc, x, y, W, H, C);
+            int slot_h[9];
+            int nh = 0;
+            for (int s = 0; s < 8; ++s)
+                if (C.flag[s] && C.src[s] < 0) {
+                    slot_h[s] = nh;
+                    if (lane == 0) S.plane[nh] = prev.plane[vbase + C.pos[s]];
+                    ++nh;
+                }
+            slot_h[8] = nh;
+            if (lane == 0) S.plane[nh] = prev.plane[idx];
+            ++nh;
+            for (int s = 0; s < 8; ++s)
+                if (C.flag[s] && C.src[s] >= 0) slot_h[s] = slot_h[C.src[s]];
+            __syncwarp();
+            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nh, nc, lane);
+#define COSTA(s, k) S.cost[slot_h[s] * K + (k)]
+
+            // ---- view-selection priors and sampling (AdaptMIPMFrame.cu:797-875)
+            DrawStream g2;
+            g2.init(P.seed, sweep_id, (uint32_t)idx);
+            uint32_t tsel = 0;
+            uint64_t vw_lo = 0, vw_hi = 0;
+            {
+                const int dpos[4] = { (y > 0) ? center - W : -1, (y < H - 1) ? center + W : -1,
+                                      (x > 0) ? center - 1 : -1, (x < W - 1) ? center + 1 : -1 };
+                const float thr = __fmul_rn(0.8f, pfd_expf(__fdiv_rn((float)(iter * iter), -90.0f)));
+                const float p_default = pfd_expf(__fdiv_rn(__fmul_rn(thr, thr), -0.32f));
+                float cdf[kMaxNb];
+                float psum = 0.0f;
+                for (int i = 0; i < nc; ++i) {
+                    float prior = 0.0f;
+                    for (int ii = 0; ii < 4; ++ii) {
+                        if (dpos[ii] < 0 || !C.flag[2 * ii]) continue;
+                        prior = __fadd_rn(prior, ((ps[dpos[ii]] >> i) & 1u) ? 0.9f : 0.1f);
+                    }
+                    float count = 0.0f, tmpw = 0.0f;
+                    int count_false = 0;
+                    for (int j = 0; j < 8; ++j) {
+                        if (!C.flag[j]) continue;
+                        const float c = COSTA(j, i);
+                        if (c < thr) {
+                            tmpw = __fadd_rn(tmpw, pfd_expf(__fdiv_rn(__fmul_rn(c, c), -0.18f)));
+                            count = __fadd_rn(count, 1.0f);
+                        }
+                        if (c > 1.2f) count_false++;
+                    }
+                    float pr = 0.0f;
+                    if (count > 2.0f && count_false < 3) pr = __fdiv_rn(tmpw, count);
+                    else if (count_false < 3) pr = p_default;
+                    pr = __fmul_rn(pr, prior);
+                    cdf[i] = pr;
+                    psum = __fadd_rn(psum, pr);
+                }
+                {   // TransformPDFToCDF (CudaUtil.cu:491-507)
+                    const float inv = __fdiv_rn(1.0f, psum);
+                    float cum = 0.0f;
+                    for (int i = 0; i < nc; ++i) { cum = __fmaf_rn(cdf[i], inv, cum); cdf[i] = cum; }
+                }
+                for (int sample = 0; sample < 15; ++sample) {
+                    const float rp = __fsub_rn(g2.uniform(), 1.1920928955078125e-07f);
+                    for (int id = 0; id < nc; ++id)
+                        if (cdf[id] > rp) {
+                            if (id < 16) vw_lo += 1ull << (id * 4); else vw_hi += 1ull << ((id - 16) * 4);
+                            break;
+                        }
+                }
+                for (int i = 0; i < nc; ++i)
+                    if (((i < 16 ? vw_lo >> (i * 4) : vw_hi >> ((i - 16) * 4)) & 15ull) != 0) tsel |= 1u << i;
+                if (tsel == 0)
+                    for (int i = 0; i < nc; ++i) {
+                        if (i < 16) vw_lo |= 1ull << (i * 4); else vw_hi |= 1ull << ((i - 16) * 4);
+                        tsel |= 1u << i;
+                    }
+            }
+#undef COSTA
+            // weighted costs: current plane, then the candidates in slot order
+            weigh_hyps(S, K, nh, nc, vw_lo, vw_hi, lane);
+            float best_cost = S.wres[slot_h[8]];
+            int best_min = S.wmin[slot_h[8]];
+            float4 best_plane = prev.plane[idx];
+            for (int s = 0; s < 8; ++s) {
+                if (!C.flag[s]) continue;
+                const float c = S.wres[slot_h[s]];
+                if (c < best_cost) { best_cost = c; best_plane = prev.plane[vbase + C.pos[s]]; best_min = S.wmin[slot_h[s]]; }
+            }
+            __syncwarp();
+
+            // ---- cross-view proposals (AdaptMIPMFrame.cu:907-936), speculative
+            const int nsel = __popc(tsel);
+            if (nsel > 0) {
+                // proposal n (n-th selected view) from the current best plane; compact the valid ones
+                int qn = -1, kn = -1;
+                if (lane < nsel) {
+                    kn = nth_set_bit(tsel, lane);
+                    const int nvid = F.nb_ids[vid * K + kn];
+                    if (nvid >= 0) qn = proposal_pos(T.geo[kn], x, y, W, H, best_plane);
+                }
+                const unsigned actm = __ballot_sync(kFullMask, qn >= 0);
+                const int slot = __popc(actm & ((1u << lane) - 1u));
+                if (qn >= 0) {
+                    const int nvid = F.nb_ids[vid * K + kn];
+                    S.plane[slot] = proposal_plane(T.geo[kn], prev.plane + (size_t)nvid * P.ppv, qn, x, y, W);
+                }
+                if (lane < nsel) S.aux[lane] = qn;
+                __syncwarp();
+                const int nact = __popc(actm);
+                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nact, nc, lane);
+                weigh_hyps(S, K, nact, nc, vw_lo, vw_hi, lane);
+                bool changed = false;
+                int hs = 0;                      // speculative hypothesis of proposal n
+                for (int n = 0; n < nsel; ++n) {
+                    const int k = nth_set_bit(tsel, n);
+                    const int nvid = F.nb_ids[vid * K + k];
+                    const int spec_q = S.aux[n];
+                    int q = spec_q;
+                    if (changed) q = (nvid >= 0) ? proposal_pos(T.geo[k], x, y, W, H, best_plane) : -1;
+                    float c = kCostMax;
+                    int cmin = -1;
+                    float4 proxy = make_float4(0.f, 0.f, 1.f, 0.f);
+                    if (q >= 0 && q == spec_q) {
+                        c = S.wres[hs];
+                        cmin = S.wmin[hs];
+                        proxy = S.plane[hs];
+                    } else if (q >= 0) {
+                        // the best plane moved the sample position: rebuild this proposal and
+                        // evaluate it in the slot after the speculative ones
+                        proxy = proposal_plane(T.geo[k], prev.plane + (size_t)nvid * P.ppv, q, x, y, W);
+                        __syncwarp();
+                        if (lane == 0) S.plane[nact] = proxy;
+                        __syncwarp();
+                        WarpBlock S1 = S;
+                        S1.plane = S.plane + nact;
+                        S1.dp = S.dp + nact;
+                        S1.cost = S.cost + nact * K;
+                        S1.wres = S.wres + nact;
+                        S1.wmin = S.wmin + nact;
+                        eval_hyps<BLUR, COUNT>(T, P, S1, pw, x, y, 1, nc, lane);
+                        weigh_hyps(S1, K, 1, nc, vw_lo, vw_hi, lane);
+                        c = S1.wres[0];
+                        cmin = S1.wmin[0];
+                    }
+                    if (spec_q >= 0) ++hs;
+                    if (q >= 0 && c < best_cost) { best_cost = c; best_plane = proxy; best_min = cmin; changed = true; }
+                }
+                __syncwarp();
+            }
+
+            // ---- refinement (PlaneHypothesisRefinement_Frame, :400-471) -----
+            {
+                const float depth_now = best_plane.w;
+                (void)g2.uniform();                      // depth_rand: drawn, never used
+                const float4 rn = random_normal(g2);
+                const float4 pn = perturbed_normal(x, y, best_plane, g2, P.pert_pi);
+                const float dmin_p = __fmul_rn(__fsub_rn(1.0f, 0.02f), depth_now);
+                const float dmax_p = __fmul_rn(__fadd_rn(1.0f, 0.02f), depth_now);
+                const float depth_perturbed = __fmaf_rn(g2.uniform(), __fsub_rn(dmax_p, dmin_p), dmin_p);
+                float4 cand[5];
+                cand[0] = random_plane(g2, P.depth_min, P.depth_max);
+                cand[1] = rn;
+                cand[2] = pn;
+                cand[3] = best_plane;
+                cand[4] = best_plane;
+                cand[4].w = depth_perturbed;
+                for (int i = 1; i < 5; ++i) cand[i].w = to_disparity(x, y, disparity_plane(x, y, cand[i]));
+                if (lane == 0)
+                    for (int i = 0; i < 5; ++i) S.plane[i] = cand[i];
+                __syncwarp();
+                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, 5, nc, lane);
+                weigh_hyps(S, K, 5, nc, vw_lo, vw_hi, lane);
+                for (int i = 0; i < 5; ++i) {
+                    const float c = S.wres[i];
+                    if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = S.wmin[i]; }
+                }
+            }
+            if (lane == 0) {
+                float4 best_disp = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (best_min >= 0)
+                    best_disp = geo_disp(T.geo[best_min], x, y, to_disparity(x, y, disparity_plane(x, y, best_plane)));
+                next.plane[idx] = best_plane;
+                next.cost[idx] = best_cost;
+                next.disp[idx] = best_disp;
+                next.sel[idx] = tsel;
+            }
+            __syncwarp();
+        }
+        __syncthreads();                         // shared memory is restaged for the next view
+    }
+}
+
+int sweep_warp_smem_bytes(const PmParams& P, bool blur)
+{
+    return Plan::make(P.W, P.H, P.K, P.ntap, blur, P.tile_stride).total;
+}
+
+size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas)
+{
+    return (size_t)n_ctas * kWarps * (size_t)sweep_warp_words(P.K) * 4u;
+}
+
+template <class Kern>
+static cudaError_t launch_k(Kern k, dim3 grid, dim3 block, int smem, cudaStream_t st, void** args)
+{
+    cudaError_t e = cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernel((const void*)k, grid, block, args, (size_t)smem, st);
+}
+
+cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int smem = sweep_warp_smem_bytes(P, blur);
+    const void* k = blur ? (const void*)pm_sweep_warp_kernel<true, false> : (const void*)pm_sweep_warp_kernel<false, false>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    *n_ctas = sms * per_sm;
+    return cudaSuccess;
+}
+
+cudaError_t launch_sweep_warp(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
+                              int iter, int phase, int n_ctas, int* err, cudaStream_t st)
+{
+    const bool blur = F.blur != nullptr;
+    const int smem = sweep_warp_smem_bytes(P, blur);
+    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+    const int grid = std::max(1, std::min(n_ctas, F.V));
+    FrameDev f = F; PmParams p = P; StateDev a = prev, b = next; int it = iter, ph = phase; int* e = err;
+    void* args[] = { &f, &p, &a, &b, &it, &ph, &e };
+    if (P.tap_counter)
+        return blur ? launch_k(pm_sweep_warp_kernel<true, true>, grid, kThreads, smem, st, args)
+                    : launch_k(pm_sweep_warp_kernel<false, true>, grid, kThreads, smem, st, args);
+    return blur ? launch_k(pm_sweep_warp_kernel<true, false>, grid, kThreads, smem, st, args)
+                : launch_k(pm_sweep_warp_kernel<false, false>, grid, kThreads, smem, st, args);
+}
+
+}  // namespace pfd

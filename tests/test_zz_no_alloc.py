@@ -52,8 +52,9 @@ def test_noalloc_sweep_matches_pfd_pm_sweep(pfd, pitch, K, patch, blur):
 
 
 def test_noalloc_sweep_rejects_too_many_neighbours(pfd):
-    """32 neighbours need 147 KB of scratch per CTA: the 16 MiB array cannot
-    give every SM one CTA, so the call fails before launching anything."""
+    """32 neighbours need 70 KB of scratch per CTA (eight warps of cost
+    vectors): the 8 MiB array cannot give every SM one CTA, so the call fails
+    before launching anything."""
     w = pfd.make_workload(260, 200, 23.0, 4, seed=5, max_nb=32)
     P = pfd.PmParams(base=23.0, patch_size=11, max_iterations=1)
     with pfd.Context(0) as ctx:
