@@ -30,7 +30,7 @@ struct PmParams {
     int tile_stride;        // bytes per micro-image tile in HBM (W*H rounded up to 16)
     uint64_t seed;
     unsigned long long* tap_counter;   // calibration runs only: in-bounds NCC taps evaluated
-    float* cost_scratch;    // sweep: per resident CTA, [9][K][block] candidate costs
+    float* cost_scratch;    // sweep: per warp, the cost vectors of its current pixel
 };
 
 struct FrameDev {

@@ -3,7 +3,6 @@
 //   pm_slice_kernel   raw frame -> per-view micro-image tiles (Slice_RawMLAImage,
 //                     DepthSolver.cpp:1951-1997)
 //   pm_init_kernel    RandomInitializationForFrame (AdaptMIPMFrame.cu:474-518)
-//   pm_sweep_kernel   CheckerboardUpdateFrame (AdaptMIPMFrame.cu:520-947)
 //   pm_ncc_kernel     per-hypothesis cost vectors (ComputeMultiViewCostVector_Frame)
 //
 // One CTA owns one reference micro-image (and a batch of its pixels).  Its own
@@ -182,18 +181,6 @@ __device__ __forceinline__ bool stage_tiles(unsigned char* smem, const SmemPlan&
     return true;
 }
 
-// The g-th pixel (row-major) whose colour (x + y) & 1 equals `colour`.
-__device__ __forceinline__ bool nth_pixel(int g, int colour, int W, int H, int& x, int& y)
-{
-    for (int yy = 0; yy < H; ++yy) {
-        const int x0 = (colour ^ yy) & 1;
-        const int cnt = (W - x0 + 1) >> 1;
-        if (g < cnt) { x = x0 + 2 * g; y = yy; return true; }
-        g -= cnt;
-    }
-    return false;
-}
-
 // --------------------------------------------------------------------------
 // Slice: raw frame -> tiles.  Window origin trunc(c - (m-1)/2) is computed on
 // the host (DepthSolver.cpp:1894-1895 and the cv::Rect conversion at :1977).
@@ -274,309 +261,6 @@ __global__ void __launch_bounds__(256) pm_init_kernel(FrameDev F, PmParams P, St
 }
 
 // --------------------------------------------------------------------------
-// CheckerboardUpdateFrame
-// --------------------------------------------------------------------------
-struct Cands {
-    int flag[8];
-    int pos[8];        // local pixel index of the candidate plane
-    int src[8];        // slot whose cost vector this slot copies, or -1
-};
-
-// Candidate positions of AdaptMIPMFrame.cu:589-795: per direction the lowest
-// prev-cost sample among the scan pattern.
-__device__ __forceinline__ void find_candidates(const float* pc, int x, int y, int W, int H, Cands& C)
-{
-    const int center = y * W + x;
-    for (int a = 0; a < 8; ++a) { C.flag[a] = 0; C.pos[a] = center; C.src[a] = -1; }
-    auto scan = [&](int start, const int* pts, const bool* ok, int n) {
-        float cm = pc[start];
-        int cp = start;
-        for (int i = 0; i < n; ++i)
-            if (ok[i] && pc[pts[i]] < cm) { cm = pc[pts[i]]; cp = pts[i]; }
-        return cp;
-    };
-    if (y > 2) {
-        const int s = center - 3 * W; const int pts[1] = { s - W }; const bool ok[1] = { y > 3 };
-        C.flag[1] = 1; C.pos[1] = scan(s, pts, ok, 1);
-    }
-    if (y < H - 3) {
-        const int s = center + 3 * W; const int pts[1] = { s + W }; const bool ok[1] = { y < H - 4 };
-        C.flag[3] = 1; C.pos[3] = scan(s, pts, ok, 1);
-    }
-    if (x > 2) {
-        const int s = center - 3; const int pts[1] = { s - 1 }; const bool ok[1] = { x > 3 };
-        C.flag[5] = 1; C.pos[5] = scan(s, pts, ok, 1);
-    }
-    if (x < W - 3) {
-        const int s = center + 3; const int pts[1] = { s + 1 }; const bool ok[1] = { x < W - 4 };
-        C.flag[7] = 1; C.pos[7] = scan(s, pts, ok, 1);
-    }
-    if (y > 0) {
-        const int s = center - W;
-        const int pts[4] = { s - W, s - W, s - 2 * W - 1, s - 2 * W + 1 };
-        const bool ok[4] = { y > 1 && x > 0, y > 1 && x < W - 1, y > 2 && x > 1, y > 2 && x < W - 2 };
-        C.flag[0] = 1; C.pos[0] = scan(s, pts, ok, 4);
-    }
-    if (y <= 2 && y > 0) { C.flag[1] = 1; C.pos[1] = C.pos[0]; C.src[1] = 0; }
-    if (y < H - 1) {
-        const int s = center + W;
-        const int pts[4] = { s + W, s + W, s + 2 * W - 1, s + 2 * W + 1 };
-        const bool ok[4] = { y < H - 2 && x > 0, y < H - 2 && x < W - 1, y < H - 3 && x > 1, y < H - 3 && x < W - 2 };
-        C.flag[2] = 1; C.pos[2] = scan(s, pts, ok, 4);
-    }
-    if (y >= H - 3 && y < H - 1) { C.flag[3] = 1; C.pos[3] = C.pos[2]; C.src[3] = 2; }
-    if (x > 0) {
-        const int s = center - 1;
-        const int pts[4] = { s - 1, s - 1, s - 2 - W, s - 2 + W };
-        const bool ok[4] = { x > 1 && y > 0, x > 1 && y < H - 1, x > 2 && y > 1, x > 2 && y < H - 2 };
-        C.flag[4] = 1; C.pos[4] = scan(s, pts, ok, 4);
-    }
-    if (x <= 2 && x > 0) { C.flag[5] = 1; C.pos[5] = C.pos[4]; C.src[5] = 4; }
-    if (x < W - 1) {
-        const int s = center + 1;
-        const int pts[4] = { s + 1, s + 1, s + 2 - W, s + 2 + W };
-        const bool ok[4] = { x < W - 2 && y > 0, x < W - 2 && y < H - 1, x < W - 3 && y > 1, x < W - 3 && y < H - 2 };
-        C.flag[6] = 1; C.pos[6] = scan(s, pts, ok, 4);
-    }
-    if (x >= W - 3 && x < W - 1) { C.flag[7] = 1; C.pos[7] = C.pos[6]; C.src[7] = 6; }
-}
-
-// Position of the n-th (0-based) set bit of m, or -1.
-__device__ __forceinline__ int nth_set_bit(uint32_t m, int n)
-{
-    for (int i = 0; i < n && m; ++i) m &= m - 1;
-    return m ? __ffs(m) - 1 : -1;
-}
-
-// One red or black half-sweep as a persistent kernel: the grid holds as many
-// CTAs as fit on the device, and CTA b walks the (view, pixel batch) items
-// b, b + gridDim.x, ...  Each CTA owns a slice of cost_scratch for the nine
-// candidate cost vectors of its pixels, small enough (about 40 MB for the
-// whole grid) to stay in L2.
-//
-// Every lane of a warp reaches each cost evaluation together (lanes without
-// a pixel, or whose candidate slot is empty, ride along inactive); per-lane
-// logic between evaluations is free to diverge.  Cross-view proposals and
-// refinement candidates are walked by a warp-uniform loop in which every lane
-// takes its own next hypothesis.
-template <bool BLUR, bool COUNT>
-__global__ void __launch_bounds__(128, 4) pm_sweep_kernel(FrameDev F, PmParams P, StateDev prev, StateDev next,
-                                                          int iter, int phase, int nbatch, int* err)
-{
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int npb = blockDim.x;
-    const int t = threadIdx.x;
-    const int W = P.W, H = P.H, K = P.K;
-    const SmemPlan L = SmemPlan::make(W, H, K, npb, P.ntap, BLUR, 0, true, P.tile_stride);
-    float* cA = P.cost_scratch + (size_t)blockIdx.x * 9 * K * npb + t;     // [slot][k][npb]
-#define COSTA(slot, k) cA[((slot) * K + (k)) * npb]
-    const int n_items = F.V * nbatch;
-
-    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-        const int vid = item / nbatch, batch = item % nbatch;
-        const int nc = min(F.nb_counts[vid], K);
-        const size_t vbase = (size_t)vid * P.ppv;
-
-        int ux = 0, uy = 0, cx = 0, cy = 0;
-        const bool has_u = nth_pixel(batch * npb + t, phase, W, H, ux, uy);
-        const bool has_c = nth_pixel(batch * npb + t, phase ^ 1, W, H, cx, cy);
-
-        // pixels of the other colour keep their state (AdaptMIPMFrame.cu:552-559)
-        if (has_c) {
-            const size_t i = vbase + cy * W + cx;
-            next.plane[i] = prev.plane[i]; next.cost[i] = prev.cost[i];
-            next.disp[i] = prev.disp[i];   next.sel[i] = prev.sel[i];
-        }
-        if (nc <= 0) {                   // AdaptMIPMFrame.cu:562-570
-            if (has_u) {
-                const size_t i = vbase + uy * W + ux;
-                next.plane[i] = prev.plane[i]; next.cost[i] = prev.cost[i];
-                next.disp[i] = prev.disp[i];   next.sel[i] = prev.sel[i];
-            }
-            continue;
-        }
-
-        Tiles T;
-        if (!stage_tiles<BLUR>(smem, L, F, P, vid, nc, T, err)) return;
-        float* pc = (float*)(smem + L.off_prevc);
-        uint32_t* ps = (uint32_t*)(smem + L.off_prevs);
-        for (int e = t; e < P.ppv; e += npb) { pc[e] = prev.cost[vbase + e]; ps[e] = prev.sel[vbase + e]; }
-        __syncthreads();
-
-        const int x = ux, y = uy;
-        const int center = y * W + x;
-        const size_t idx = vbase + center;
-
-        // ---- propagation candidates and the current plane ----------------
-        Cands C;
-        if (has_u) find_candidates(pc, x, y, W, H, C);
-        else for (int a = 0; a < 8; ++a) { C.flag[a] = 0; C.pos[a] = 0; C.src[a] = -1; }
-        for (int s = 0; s < 8; ++s) {
-            const bool act = has_u && C.flag[s] && C.src[s] < 0;
-            const float4 h = act ? prev.plane[vbase + C.pos[s]] : make_float4(0.f, 0.f, 1.f, 0.f);
-            cost_vector<BLUR, COUNT>(T, P, x, y, act, h, nc, &COSTA(s, 0), npb);
-        }
-        for (int s = 0; s < 8; ++s) {
-            if (!has_u || !C.flag[s] || C.src[s] < 0) continue;
-            for (int k = 0; k < nc; ++k) COSTA(s, k) = COSTA(C.src[s], k);
-        }
-        float4 best_plane = has_u ? prev.plane[idx] : make_float4(0.f, 0.f, 1.f, 0.f);
-        cost_vector<BLUR, COUNT>(T, P, x, y, has_u, best_plane, nc, &COSTA(8, 0), npb);
-
-        // ---- view-selection priors and sampling (AdaptMIPMFrame.cu:797-875)
-        DrawStream g;
-        g.init(P.seed, (uint32_t)(1 + 2 * iter + phase), (uint32_t)idx);
-        uint32_t tsel = 0;
-        uint64_t vw_lo = 0, vw_hi = 0;       // 4-bit view weights, views 0-15 and 16-31
-        float best_cost = kCostMax;
-        int best_min = -1;
-        if (has_u) {
-            const int dpos[4] = { (y > 0) ? center - W : -1, (y < H - 1) ? center + W : -1,
-                                  (x > 0) ? center - 1 : -1, (x < W - 1) ? center + 1 : -1 };
-            const float thr = __fmul_rn(0.8f, pfd_expf(__fdiv_rn((float)(iter * iter), -90.0f)));
-            const float p_default = pfd_expf(__fdiv_rn(__fmul_rn(thr, thr), -0.32f));
-            float cdf[kMaxNb];
-            float psum = 0.0f;
-            for (int i = 0; i < nc; ++i) {
-                float prior = 0.0f;
-                for (int ii = 0; ii < 4; ++ii) {
-                    if (dpos[ii] < 0 || !C.flag[2 * ii]) continue;
-                    prior = __fadd_rn(prior, ((ps[dpos[ii]] >> i) & 1u) ? 0.9f : 0.1f);
-                }
-                float count = 0.0f, tmpw = 0.0f;
-                int count_false = 0;
-                for (int j = 0; j < 8; ++j) {
-                    if (!C.flag[j]) continue;
-                    const float c = COSTA(j, i);
-                    if (c < thr) { tmpw = __fadd_rn(tmpw, pfd_expf(__fdiv_rn(__fmul_rn(c, c), -0.18f))); count = __fadd_rn(count, 1.0f); }
-                    if (c > 1.2f) count_false++;
-                }
-                float pr = 0.0f;
-                if (count > 2.0f && count_false < 3) pr = __fdiv_rn(tmpw, count);
-                else if (count_false < 3) pr = p_default;
-                pr = __fmul_rn(pr, prior);
-                cdf[i] = pr;
-                psum = __fadd_rn(psum, pr);
-            }
-            {   // TransformPDFToCDF (CudaUtil.cu:491-507)
-                const float inv = __fdiv_rn(1.0f, psum);
-                float cum = 0.0f;
-                for (int i = 0; i < nc; ++i) { cum = __fmaf_rn(cdf[i], inv, cum); cdf[i] = cum; }
-            }
-            for (int sample = 0; sample < 15; ++sample) {
-                const float rp = __fsub_rn(g.uniform(), 1.1920928955078125e-07f);
-                for (int id = 0; id < nc; ++id)
-                    if (cdf[id] > rp) {
-                        if (id < 16) vw_lo += 1ull << (id * 4); else vw_hi += 1ull << ((id - 16) * 4);
-                        break;
-                    }
-            }
-            for (int i = 0; i < nc; ++i)
-                if (((i < 16 ? vw_lo >> (i * 4) : vw_hi >> ((i - 16) * 4)) & 15ull) != 0) tsel |= 1u << i;
-            if (tsel == 0)
-                for (int i = 0; i < nc; ++i) {
-                    if (i < 16) vw_lo |= 1ull << (i * 4); else vw_hi |= 1ull << ((i - 16) * 4);
-                    tsel |= 1u << i;
-                }
-        }
-#define VW(k) ((float)(((k) < 16 ? vw_lo >> ((k) * 4) : vw_hi >> (((k) - 16) * 4)) & 15ull))
-        if (has_u) {
-            // weighted costs: current plane, then the 8 candidates
-            {
-                WeightedCost wc;
-                for (int k = 0; k < nc; ++k) wc.add(k, COSTA(8, k), VW(k));
-                best_cost = wc.result();
-                best_min = wc.min_idx;
-            }
-            for (int s = 0; s < 8; ++s) {
-                if (!C.flag[s]) continue;
-                WeightedCost wc;
-                for (int k = 0; k < nc; ++k) wc.add(k, COSTA(s, k), VW(k));
-                const float c = wc.result();
-                if (c < best_cost) { best_cost = c; best_plane = prev.plane[vbase + C.pos[s]]; best_min = wc.min_idx; }
-            }
-        }
-        float* scratch = &COSTA(0, 0);                // candidate costs are dead from here on
-
-        // ---- cross-view proposals (AdaptMIPMFrame.cu:907-936) ------------
-        const int nsel = __popc(tsel);
-        const int nmax = __reduce_max_sync(kFullMask, nsel);
-        for (int n = 0; n < nmax; ++n) {
-            const int k = (n < nsel) ? nth_set_bit(tsel, n) : -1;
-            bool act = false;
-            float4 proxy = make_float4(0.f, 0.f, 1.f, 0.f);
-            if (k >= 0) {
-                const int nvid = F.nb_ids[vid * K + k];
-                if (nvid >= 0) {
-                    const NbGeo& gk = T.geo[k];
-                    const float dcur = to_disparity(x, y, disparity_plane(x, y, best_plane));
-                    const float2 qf = geo_anchor(gk, x, y, dcur);
-                    const float fqx = floorf(__fadd_rn(qf.x, 0.5f)), fqy = floorf(__fadd_rn(qf.y, 0.5f));
-                    if (fqx >= 0.0f && fqx < (float)W && fqy >= 0.0f && fqy < (float)H) {
-                        const int qx = (int)fqx, qy = (int)fqy;
-                        const float4 hn = prev.plane[(size_t)nvid * P.ppv + qy * W + qx];
-                        const float3 dpn = disparity_plane(qx, qy, hn);
-                        float denom = __fmaf_rn(dpn.y, gk.by, __fmaf_rn(dpn.x, gk.bx, 1.0f));
-                        denom = safe_denom(denom);
-                        proxy = encode_plane(x, y, __fdiv_rn(dpn.x, denom), __fdiv_rn(dpn.y, denom), __fdiv_rn(dpn.z, denom));
-                        act = true;
-                    }
-                }
-            }
-            cost_vector<BLUR, COUNT>(T, P, x, y, act, proxy, nc, scratch, npb);
-            if (act) {
-                WeightedCost wc;
-                for (int kk = 0; kk < nc; ++kk) wc.add(kk, scratch[kk * npb], VW(kk));
-                const float c = wc.result();
-                if (c < best_cost) { best_cost = c; best_plane = proxy; best_min = wc.min_idx; }
-            }
-        }
-
-        // ---- refinement (PlaneHypothesisRefinement_Frame, :400-471) -----
-        float4 cand[5];
-        if (has_u) {
-            const float depth_now = best_plane.w;
-            (void)g.uniform();                       // depth_rand: drawn, never used
-            const float4 rn = random_normal(g);
-            const float4 pn = perturbed_normal(x, y, best_plane, g, P.pert_pi);
-            const float dmin_p = __fmul_rn(__fsub_rn(1.0f, 0.02f), depth_now);
-            const float dmax_p = __fmul_rn(__fadd_rn(1.0f, 0.02f), depth_now);
-            const float depth_perturbed = __fmaf_rn(g.uniform(), __fsub_rn(dmax_p, dmin_p), dmin_p);
-            cand[0] = random_plane(g, P.depth_min, P.depth_max);
-            cand[1] = rn;
-            cand[2] = pn;
-            cand[3] = best_plane;
-            cand[4] = best_plane;
-            cand[4].w = depth_perturbed;
-            for (int i = 1; i < 5; ++i) cand[i].w = to_disparity(x, y, disparity_plane(x, y, cand[i]));
-        } else {
-            for (int i = 0; i < 5; ++i) cand[i] = make_float4(0.f, 0.f, 1.f, 0.f);
-        }
-        for (int i = 0; i < 5; ++i) {
-            cost_vector<BLUR, COUNT>(T, P, x, y, has_u, cand[i], nc, scratch, npb);
-            if (has_u) {
-                WeightedCost wc;
-                for (int kk = 0; kk < nc; ++kk) wc.add(kk, scratch[kk * npb], VW(kk));
-                const float c = wc.result();
-                if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = wc.min_idx; }
-            }
-        }
-#undef VW
-        if (has_u) {
-            float4 best_disp = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (best_min >= 0)
-                best_disp = geo_disp(T.geo[best_min], x, y, to_disparity(x, y, disparity_plane(x, y, best_plane)));
-            next.plane[idx] = best_plane;
-            next.cost[idx] = best_cost;
-            next.disp[idx] = best_disp;
-            next.sel[idx] = tsel;
-        }
-        __syncthreads();                             // shared memory is restaged for the next item
-    }
-#undef COSTA
-}
-
-// --------------------------------------------------------------------------
 // Per-hypothesis cost vectors.  Segments group hypotheses of one view.
 // --------------------------------------------------------------------------
 template <bool BLUR, bool COUNT>
@@ -604,13 +288,6 @@ __global__ void __launch_bounds__(256) pm_ncc_kernel(FrameDev F, PmParams P, con
 // --------------------------------------------------------------------------
 // Host launchers
 // --------------------------------------------------------------------------
-int sweep_smem_bytes(const PmParams& P, int npb, bool blur)
-{
-    return SmemPlan::make(P.W, P.H, P.K, npb, P.ntap, blur, 0, true, P.tile_stride).total;
-}
-
-constexpr int kSweepThreads = 128;
-
 template <class Kern>
 static cudaError_t launch(Kern k, dim3 grid, dim3 block, int smem, cudaStream_t st, void** args)
 {
@@ -640,46 +317,6 @@ cudaError_t launch_init(const FrameDev& F, const PmParams& P, const StateDev& ou
                     : launch(pm_init_kernel<false, true>, grid, npb, smem, st, args);
     return blur ? launch(pm_init_kernel<true, false>, grid, npb, smem, st, args)
                 : launch(pm_init_kernel<false, false>, grid, npb, smem, st, args);
-}
-
-size_t sweep_scratch_bytes(const PmParams& P, int n_sms, int ctas_per_sm)
-{
-    return (size_t)n_sms * (size_t)ctas_per_sm * 9u * (size_t)P.K * kSweepThreads * sizeof(float);
-}
-
-cudaError_t sweep_grid(const PmParams& P, bool blur, int* n_ctas)
-{
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int smem = sweep_smem_bytes(P, kSweepThreads, blur);
-    const void* k = blur ? (const void*)pm_sweep_kernel<true, false> : (const void*)pm_sweep_kernel<false, false>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kSweepThreads, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    *n_ctas = sms * per_sm;
-    return cudaSuccess;
-}
-
-cudaError_t launch_sweep(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
-                         int iter, int phase, int n_ctas, int* err, cudaStream_t st)
-{
-    const bool blur = F.blur != nullptr;
-    const int updated = (P.ppv + 1) / 2;
-    const int npb = kSweepThreads;
-    const int nbatch = (updated + npb - 1) / npb;
-    const int smem = sweep_smem_bytes(P, npb, blur);
-    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
-    const int grid = std::min(n_ctas, F.V * nbatch);
-    FrameDev f = F; PmParams p = P; StateDev a = prev, b = next; int it = iter, ph = phase, nb = nbatch; int* e = err;
-    void* args[] = { &f, &p, &a, &b, &it, &ph, &nb, &e };
-    if (P.tap_counter)
-        return blur ? launch(pm_sweep_kernel<true, true>, grid, npb, smem, st, args)
-                    : launch(pm_sweep_kernel<false, true>, grid, npb, smem, st, args);
-    return blur ? launch(pm_sweep_kernel<true, false>, grid, npb, smem, st, args)
-                : launch(pm_sweep_kernel<false, false>, grid, npb, smem, st, args);
 }
 
 cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, const int* seg_vid, const int* seg_start,

@@ -12,17 +12,9 @@ namespace pfd {
 cudaError_t launch_slice(const uint8_t* raw, int raw_pitch, const int2* origin, int V, int W, int H,
                          int tile_stride, uint8_t* tiles, cudaStream_t st);
 cudaError_t launch_init(const FrameDev& F, const PmParams& P, const StateDev& out, int* err, cudaStream_t st);
-// The sweep is a persistent kernel: sweep_grid gives the number of CTAs that
-// fit on the device, sweep_scratch_bytes the candidate-cost scratch they need
-// (P.cost_scratch).
-cudaError_t sweep_grid(const PmParams& P, bool blur, int* n_ctas);
-size_t sweep_scratch_bytes(const PmParams& P, int n_sms, int ctas_per_sm);
-cudaError_t launch_sweep(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
-                         int iter, int phase, int n_ctas, int* err, cudaStream_t st);
 cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, const int* seg_vid,
                        const int* seg_start, const int* seg_len, const int* hyp_pxy, const float4* hyp_plane,
                        const int* hyp_out, float* costs, int* err, cudaStream_t st);
-int sweep_smem_bytes(const PmParams& P, int npb, bool blur);
 // The warp-per-pixel sweep (pm_sweep.cu): grid, shared memory, and the global
 // scratch it needs (P.cost_scratch: per warp, the cost vectors of one pixel).
 cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas);

@@ -12,7 +12,7 @@
 // term) are computed once per pixel into a per-warp table and read as a
 // broadcast.  Each lane accumulates its NCC's six moments in the reference's
 // tap order (x offset outer, y offset inner); a tap whose source sample
-// leaves the neighbour window adds exact zeros.
+// leaves the neighbour window is skipped, as in the reference.
 //
 // Cross-view proposals depend on the best plane so far (AdaptMIPMFrame.cu:
 // 907-936): they are built speculatively from the best plane after
@@ -288,7 +288,7 @@ __device__ __forceinline__ void build_table(const Quad& T, const PmParams& P, co
 
 // One lane's NCC (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:73-179) of the
 // pixel under plane dp against neighbour k.  Every lane of the warp walks the
-// same taps; inactive lanes add zeros.
+// same taps; a lane skips the taps it does not keep.
 template <bool BLUR, bool COUNT>
 __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, const float4* tab, const PixWin& pw,
                                           float3 dp, int k, bool active, unsigned& ntaps)
@@ -313,25 +313,23 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
             const float sy = __fmaf_rn(sty, d, fyr);
             const bool v = active && (__float_as_uint(sx) < P.W_bits) && (__float_as_uint(sy) < P.H_bits);
             if (COUNT) ntaps += v ? 1u : 0u;
-            const int tbx = tex_coord_bits(sx), tby = tex_coord_bits(sy);
-            const uint32_t rel = (((uint32_t)(tby >> 8) * qs + (uint32_t)(tbx >> 8)) << 2);
-            const uint32_t q = lds_u32(v ? base + rel : T.q_addr);
-            const float s = quad_blend(tbx, tby, q);
-            const float wv = v ? e.x : 0.0f;
-            const float wrv = v ? e.y : 0.0f;
-            const float rv = e.z;
-            const float ws = __fmul_rn(wv, s);
-            sr = __fmaf_rn(wv, rv, sr);
-            srr = __fmaf_rn(wrv, rv, srr);
-            ss = __fmaf_rn(wv, s, ss);
-            sss = __fmaf_rn(ws, s, sss);
-            srs = __fmaf_rn(wrv, s, srs);
-            sw = __fadd_rn(sw, wv);
-            if (BLUR) {
-                const uint32_t qb = lds_u32(v ? bbase + rel : T.qb_addr);
-                const float sb = quad_blend(tbx, tby, qb);
-                bsx = __fadd_rn(bsx, v ? e.w : 0.0f);
-                bsy = __fadd_rn(bsy, v ? __fdiv_rn(sb, 255.0f) : 0.0f);
+            if (v) {                         // a skipped tap leaves the sums as they are
+                const int tbx = tex_coord_bits(sx), tby = tex_coord_bits(sy);
+                const uint32_t rel = (((uint32_t)(tby >> 8) * qs + (uint32_t)(tbx >> 8)) << 2);
+                const float s = quad_blend(tbx, tby, lds_u32(base + rel));
+                const float wv = e.x, wrv = e.y, rv = e.z;
+                const float ws = __fmul_rn(wv, s);
+                sr = __fmaf_rn(wv, rv, sr);
+                srr = __fmaf_rn(wrv, rv, srr);
+                ss = __fmaf_rn(wv, s, ss);
+                sss = __fmaf_rn(ws, s, sss);
+                srs = __fmaf_rn(wrv, s, srs);
+                sw = __fadd_rn(sw, wv);
+                if (BLUR) {
+                    const float sb = quad_blend(tbx, tby, lds_u32(bbase + rel));
+                    bsx = __fadd_rn(bsx, e.w);
+                    bsy = __fadd_rn(bsy, __fdiv_rn(sb, 255.0f));
+                }
             }
         }
     }
@@ -621,44 +619,53 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                                       (x > 0) ? center - 1 : -1, (x < W - 1) ? center + 1 : -1 };
                 const float thr = __fmul_rn(0.8f, pfd_expf(__fdiv_rn((float)(iter * iter), -90.0f)));
                 const float p_default = pfd_expf(__fdiv_rn(__fmul_rn(thr, thr), -0.32f));
-                float cdf[kMaxNb];
-                float psum = 0.0f;
-                for (int i = 0; i < nc; ++i) {
+                // lane i works out view i's probability; the sums over views then run in
+                // view order on every lane, as the reference's loop does
+                float pr = 0.0f;
+                if (lane < nc) {
+                    const int i = lane;
                     float prior = 0.0f;
                     for (int ii = 0; ii < 4; ++ii) {
                         if (dpos[ii] < 0 || !C.flag[2 * ii]) continue;
                         prior = __fadd_rn(prior, ((ps[dpos[ii]] >> i) & 1u) ? 0.9f : 0.1f);
                     }
+                    float cj[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) cj[j] = C.flag[j] ? COSTA(j, i) : 0.0f;
                     float count = 0.0f, tmpw = 0.0f;
                     int count_false = 0;
+#pragma unroll
                     for (int j = 0; j < 8; ++j) {
                         if (!C.flag[j]) continue;
-                        const float c = COSTA(j, i);
+                        const float c = cj[j];
                         if (c < thr) {
                             tmpw = __fadd_rn(tmpw, pfd_expf(__fdiv_rn(__fmul_rn(c, c), -0.18f)));
                             count = __fadd_rn(count, 1.0f);
                         }
                         if (c > 1.2f) count_false++;
                     }
-                    float pr = 0.0f;
                     if (count > 2.0f && count_false < 3) pr = __fdiv_rn(tmpw, count);
                     else if (count_false < 3) pr = p_default;
                     pr = __fmul_rn(pr, prior);
-                    cdf[i] = pr;
-                    psum = __fadd_rn(psum, pr);
                 }
+                float psum = 0.0f;
+                for (int i = 0; i < nc; ++i) psum = __fadd_rn(psum, __shfl_sync(kFullMask, pr, i));
+                float cdf_l = 0.0f;
                 {   // TransformPDFToCDF (CudaUtil.cu:491-507)
                     const float inv = __fdiv_rn(1.0f, psum);
                     float cum = 0.0f;
-                    for (int i = 0; i < nc; ++i) { cum = __fmaf_rn(cdf[i], inv, cum); cdf[i] = cum; }
+                    for (int i = 0; i < nc; ++i) {
+                        cum = __fmaf_rn(__shfl_sync(kFullMask, pr, i), inv, cum);
+                        if (lane == i) cdf_l = cum;
+                    }
                 }
                 for (int sample = 0; sample < 15; ++sample) {
                     const float rp = __fsub_rn(g2.uniform(), 1.1920928955078125e-07f);
-                    for (int id = 0; id < nc; ++id)
-                        if (cdf[id] > rp) {
-                            if (id < 16) vw_lo += 1ull << (id * 4); else vw_hi += 1ull << ((id - 16) * 4);
-                            break;
-                        }
+                    const unsigned hit = __ballot_sync(kFullMask, lane < nc && cdf_l > rp);
+                    if (hit) {
+                        const int id = __ffs(hit) - 1;        // the first view whose CDF exceeds rp
+                        if (id < 16) vw_lo += 1ull << (id * 4); else vw_hi += 1ull << ((id - 16) * 4);
+                    }
                 }
                 for (int i = 0; i < nc; ++i)
                     if (((i < 16 ? vw_lo >> (i * 4) : vw_hi >> ((i - 16) * 4)) & 15ull) != 0) tsel |= 1u << i;
