@@ -133,7 +133,7 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
  * exit) instead of a cudaMalloc'd buffer; inputs and outputs are the frame's
  * state exactly as for pfd_pm_sweep, and the results are the same bit for bit.
  * Limit: the array must hold one CTA's scratch (eight warps, each the cost
- * vectors of one pixel) for every SM, so max_nb <= 28 on a 148-SM B200;
+ * vectors of one pixel) for every SM, so max_nb <= 30 on a 148-SM B200;
  * larger frames get PFD_EINVAL.
  * The first call on a device looks up the array's device address, so make
  * that call before any stream capture.  All calls on a device share the one

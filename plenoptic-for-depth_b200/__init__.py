@@ -310,7 +310,7 @@ class Context:
 
     def pm_sweep_noalloc(self, fid: int, params: PmParams, seed: int, it: int, phase: int) -> None:
         """pfd_pm_sweep on the library's fixed scratch array: for callers that may
-        not allocate device memory while frames stream (max_nb <= 28 on B200)."""
+        not allocate device memory while frames stream (max_nb <= 30 on B200)."""
         p = params.c()
         self._check(self._L.pfd_pm_sweep_noalloc(self._h, fid, ctypes.byref(p), seed, it, phase),
                     "pfd_pm_sweep_noalloc")

@@ -145,16 +145,17 @@ __device__ __forceinline__ float4 random_plane(DrawStream& g, float dmin, float 
     return h;
 }
 
-// GeneratePerturbedNormalLF (CudaUtil.cu:105-142).  The perturbed normal keeps
-// n.w (the reference leaves .w uninitialised there).
-__device__ __forceinline__ float4 perturbed_normal(int px, int py, float4 n, DrawStream& g, float pert)
+// GeneratePerturbedNormalLF (CudaUtil.cu:105-142) from the three uniforms it
+// draws (u1, u2, u3 in draw order).  The perturbed normal keeps n.w (the
+// reference leaves .w uninitialised there).
+__device__ __forceinline__ float4 perturbed_normal_u(int px, int py, float4 n, float u1, float u2, float u3, float pert)
 {
     const float X0 = (float)px, X1 = (float)py, X2 = 1.0f;
     const float norm = __fsqrt_rn(__fmaf_rn(X2, X2, __fmaf_rn(X1, X1, __fmul_rn(X0, X0))));
     const float vx = __fdiv_rn(X0, norm), vy = __fdiv_rn(X1, norm), vz = __fdiv_rn(X2, norm);
-    const float a1 = __fmul_rn(__fsub_rn(g.uniform(), 0.5f), pert);
-    const float a2 = __fmul_rn(__fsub_rn(g.uniform(), 0.5f), pert);
-    const float a3 = __fmul_rn(__fsub_rn(g.uniform(), 0.5f), pert);
+    const float a1 = __fmul_rn(__fsub_rn(u1, 0.5f), pert);
+    const float a2 = __fmul_rn(__fsub_rn(u2, 0.5f), pert);
+    const float a3 = __fmul_rn(__fsub_rn(u3, 0.5f), pert);
     const float s1 = pfd_sin_small(a1), s2 = pfd_sin_small(a2), s3 = pfd_sin_small(a3);
     const float c1 = pfd_cos_small(a1), c2 = pfd_cos_small(a2), c3 = pfd_cos_small(a3);
     const float R0 = __fmul_rn(c2, c3);
@@ -174,6 +175,15 @@ __device__ __forceinline__ float4 perturbed_normal(int px, int py, float4 n, Dra
     const float dot = __fmaf_rn(q.z, vz, __fmaf_rn(q.y, vy, __fmul_rn(q.x, vx)));
     if (dot >= 0.0f) q = n;
     return normalize3(q);
+}
+
+// GeneratePerturbedNormalLF drawing its uniforms from g.
+__device__ __forceinline__ float4 perturbed_normal(int px, int py, float4 n, DrawStream& g, float pert)
+{
+    const float u1 = g.uniform();
+    const float u2 = g.uniform();
+    const float u3 = g.uniform();
+    return perturbed_normal_u(px, py, n, u1, u2, u3, pert);
 }
 
 // EncodePlaneHypothesisFromDispPlaneDevice (AdaptMIPMFrame.cu:36-53)

@@ -15,10 +15,13 @@
 // leaves the neighbour window is skipped, as in the reference.
 //
 // Cross-view proposals depend on the best plane so far (AdaptMIPMFrame.cu:
-// 907-936): they are built speculatively from the best plane after
+// 907-936), and the refinement candidates on the best plane after them
+// (:400-471).  Both are built speculatively from the best plane after
 // propagation and evaluated together, then walked in order; a proposal whose
 // neighbour-window sample position changed because an earlier one won is
-// rebuilt and evaluated again, so the result is the sequential one.
+// rebuilt and evaluated again, and so are the refinement candidates that
+// follow the best plane, so the result is the sequential one.  A refinement
+// candidate bit-identical to the best plane has its cost and is not evaluated.
 //
 // Neighbour micro-images are held as 32-bit quads: entry (iy, ix) packs the
 // four texels of a bilinear footprint, T(iy,ix), T(iy,ix+1), T(iy+1,ix),
@@ -58,20 +61,20 @@ struct WarpBlock {
     float4* plane;           // [maxh] hypotheses (shared)
     float4* dp;              // [maxh] disparity plane (x, y, z) and disparity at the pixel (w) (shared)
     float* cost;             // [maxh][K] (global)
-    int* pair;               // [maxh * K] compacted (hypothesis, neighbour) indices (global)
+    uint16_t* pair;          // [maxh * K] compacted (hypothesis, neighbour) indices (global)
     float* wres;             // [maxh] weighted cost (global)
     int* wmin;               // [maxh] index of the lowest cost (global)
     int* aux;                // [maxh] proposal sample position, or -1 (global)
 };
 
 // Hypotheses one evaluation can hold: 9 propagation slots, or every selected
-// view's proposal plus one rebuilt proposal.
-__host__ __device__ inline int sweep_maxh(int K) { return K + 1 > 9 ? K + 1 : 9; }
-// 4-byte words of global scratch per warp.
+// view's proposal, the 5 refinement candidates and one rebuilt proposal.
+__host__ __device__ inline int sweep_maxh(int K) { return K + 6 > 9 ? K + 6 : 9; }
+// 4-byte words of global scratch per warp: costs, 16-bit pair indices, wres/wmin/aux.
 __host__ __device__ inline int sweep_warp_words(int K)
 {
     const int mh = sweep_maxh(K);
-    return ((2 * mh * K + 3 * mh) + 31) & ~31;
+    return ((mh * K + (mh * K + 1) / 2 + 3 * mh) + 31) & ~31;
 }
 
 struct Plan {
@@ -114,8 +117,8 @@ struct Plan {
         S.dp = S.plane + maxh;
         float* g = gscratch + ((size_t)blockIdx.x * kWarps + w) * sweep_warp_words(K);
         S.cost = g;
-        S.pair = (int*)(g + maxh * K);
-        S.wres = g + 2 * maxh * K;
+        S.pair = (uint16_t*)(g + maxh * K);
+        S.wres = g + maxh * K + (maxh * K + 1) / 2;
         S.wmin = (int*)(S.wres + maxh);
         S.aux = S.wmin + maxh;
         return S;
@@ -356,11 +359,12 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
 }
 
 // Cost vectors (ComputeMultiViewCostVector_Frame, AdaptMIPMFrame.cu:181-225) of
-// hypotheses S.plane[0..nh) at (px, py): S.cost[h * K + k] for k < nc.  A
-// neighbour whose anchor leaves the window gets 2 without evaluation.
+// hypotheses S.plane[0..nh) at (px, py), except those whose bit is set in
+// skip: S.cost[h * K + k] for k < nc.  A neighbour whose anchor leaves the
+// window gets 2 without evaluation.
 template <bool BLUR, bool COUNT>
 __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const WarpBlock& S, const PixWin& pw,
-                                       int px, int py, int nh, int nc, int lane)
+                                       int px, int py, int nh, int nc, int lane, uint64_t skip)
 {
     const int K = P.K;
     for (int h = lane; h < nh; h += 32) {
@@ -373,8 +377,9 @@ __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const W
     for (int n0 = 0; n0 < total; n0 += 32) {
         const int n = n0 + lane;
         bool need = false;
-        if (n < total) {
-            const int h = n / nc, k = n - h * nc;
+        const int hn = n / nc;
+        if (n < total && !((skip >> hn) & 1ull)) {
+            const int h = hn, k = n - h * nc;
             if (T.nb_ok[k]) {
                 const float2 a = geo_anchor(T.geo[k], px, py, S.dp[h].w);
                 need = (__float_as_uint(a.x) < P.W_bits) && (__float_as_uint(a.y) < P.H_bits);
@@ -382,7 +387,7 @@ __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const W
             if (!need) S.cost[h * K + k] = kCostMax;
         }
         const unsigned m = __ballot_sync(kFullMask, need);
-        if (need) S.pair[np + __popc(m & ((1u << lane) - 1u))] = n;
+        if (need) S.pair[np + __popc(m & ((1u << lane) - 1u))] = (uint16_t)n;
         np += __popc(m);
     }
     __syncwarp();
@@ -523,6 +528,27 @@ __device__ __forceinline__ float4 proposal_plane(const NbGeo& gk, const float4* 
     return encode_plane(x, y, __fdiv_rn(dpn.x, denom), __fdiv_rn(dpn.y, denom), __fdiv_rn(dpn.z, denom));
 }
 
+// The five candidates of PlaneHypothesisRefinement_Frame (AdaptMIPMFrame.cu:
+// 400-471) for the best plane `best`, from the draws already taken (c0: the
+// random plane, rn: the random normal, u1-u3: the perturbation, u4: the depth
+// perturbation).
+__device__ __forceinline__ void refine_candidates(int x, int y, float4 best, float4 c0, float4 rn, float u1, float u2,
+                                                  float u3, float u4, float pert, float4 (&cand)[5])
+{
+    const float depth_now = best.w;
+    const float4 pn = perturbed_normal_u(x, y, best, u1, u2, u3, pert);
+    const float dmin_p = __fmul_rn(__fsub_rn(1.0f, 0.02f), depth_now);
+    const float dmax_p = __fmul_rn(__fadd_rn(1.0f, 0.02f), depth_now);
+    const float depth_perturbed = __fmaf_rn(u4, __fsub_rn(dmax_p, dmin_p), dmin_p);
+    cand[0] = c0;
+    cand[1] = rn;
+    cand[2] = pn;
+    cand[3] = best;
+    cand[4] = best;
+    cand[4].w = depth_perturbed;
+    for (int i = 1; i < 5; ++i) cand[i].w = to_disparity(x, y, disparity_plane(x, y, cand[i]));
+}
+
 }  // namespace
 
 template <bool BLUR, bool COUNT>
@@ -606,7 +632,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             for (int s = 0; s < 8; ++s)
                 if (C.flag[s] && C.src[s] >= 0) slot_h[s] = slot_h[C.src[s]];
             __syncwarp();
-            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nh, nc, lane);
+            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nh, nc, lane, 0ull);
 #define COSTA(s, k) S.cost[slot_h[s] * K + (k)]
 
             // ---- view-selection priors and sampling (AdaptMIPMFrame.cu:797-875)
@@ -688,92 +714,90 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             }
             __syncwarp();
 
-            // ---- cross-view proposals (AdaptMIPMFrame.cu:907-936), speculative
+            // ---- cross-view proposals (AdaptMIPMFrame.cu:907-936) and refinement
+            // (PlaneHypothesisRefinement_Frame, :400-471), evaluated together.  Proposals
+            // are built from the best plane so far and the refinement candidates from the
+            // best plane after the proposals; both are built here from the current best
+            // and rebuilt below when a proposal wins.  The refinement's random draws do
+            // not depend on the best plane, so they are taken now, in their order.
             const int nsel = __popc(tsel);
-            if (nsel > 0) {
-                // proposal n (n-th selected view) from the current best plane; compact the valid ones
-                int qn = -1, kn = -1;
-                if (lane < nsel) {
-                    kn = nth_set_bit(tsel, lane);
-                    const int nvid = F.nb_ids[vid * K + kn];
-                    if (nvid >= 0) qn = proposal_pos(T.geo[kn], x, y, W, H, best_plane);
-                }
-                const unsigned actm = __ballot_sync(kFullMask, qn >= 0);
-                const int slot = __popc(actm & ((1u << lane) - 1u));
-                if (qn >= 0) {
-                    const int nvid = F.nb_ids[vid * K + kn];
-                    S.plane[slot] = proposal_plane(T.geo[kn], prev.plane + (size_t)nvid * P.ppv, qn, x, y, W);
-                }
-                if (lane < nsel) S.aux[lane] = qn;
-                __syncwarp();
-                const int nact = __popc(actm);
-                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nact, nc, lane);
-                weigh_hyps(S, K, nact, nc, vw_lo, vw_hi, lane);
-                bool changed = false;
-                int hs = 0;                      // speculative hypothesis of proposal n
-                for (int n = 0; n < nsel; ++n) {
-                    const int k = nth_set_bit(tsel, n);
-                    const int nvid = F.nb_ids[vid * K + k];
-                    const int spec_q = S.aux[n];
-                    int q = spec_q;
-                    if (changed) q = (nvid >= 0) ? proposal_pos(T.geo[k], x, y, W, H, best_plane) : -1;
-                    float c = kCostMax;
-                    int cmin = -1;
-                    float4 proxy = make_float4(0.f, 0.f, 1.f, 0.f);
-                    if (q >= 0 && q == spec_q) {
-                        c = S.wres[hs];
-                        cmin = S.wmin[hs];
-                        proxy = S.plane[hs];
-                    } else if (q >= 0) {
-                        // the best plane moved the sample position: rebuild this proposal and
-                        // evaluate it in the slot after the speculative ones
-                        proxy = proposal_plane(T.geo[k], prev.plane + (size_t)nvid * P.ppv, q, x, y, W);
-                        __syncwarp();
-                        if (lane == 0) S.plane[nact] = proxy;
-                        __syncwarp();
-                        WarpBlock S1 = S;
-                        S1.plane = S.plane + nact;
-                        S1.dp = S.dp + nact;
-                        S1.cost = S.cost + nact * K;
-                        S1.wres = S.wres + nact;
-                        S1.wmin = S.wmin + nact;
-                        eval_hyps<BLUR, COUNT>(T, P, S1, pw, x, y, 1, nc, lane);
-                        weigh_hyps(S1, K, 1, nc, vw_lo, vw_hi, lane);
-                        c = S1.wres[0];
-                        cmin = S1.wmin[0];
-                    }
-                    if (spec_q >= 0) ++hs;
-                    if (q >= 0 && c < best_cost) { best_cost = c; best_plane = proxy; best_min = cmin; changed = true; }
-                }
-                __syncwarp();
+            int qn = -1, kn = -1;
+            if (lane < nsel) {
+                kn = nth_set_bit(tsel, lane);
+                const int nvid = F.nb_ids[vid * K + kn];
+                if (nvid >= 0) qn = proposal_pos(T.geo[kn], x, y, W, H, best_plane);
             }
+            const unsigned actm = __ballot_sync(kFullMask, qn >= 0);
+            if (qn >= 0) {
+                const int nvid = F.nb_ids[vid * K + kn];
+                S.plane[__popc(actm & ((1u << lane) - 1u))] =
+                    proposal_plane(T.geo[kn], prev.plane + (size_t)nvid * P.ppv, qn, x, y, W);
+            }
+            if (lane < nsel) S.aux[lane] = qn;
+            const int nact = __popc(actm);
+            (void)g2.uniform();                          // depth_rand: drawn, never used
+            const float4 rn = random_normal(g2);
+            const float u1 = g2.uniform(), u2 = g2.uniform(), u3 = g2.uniform();
+            const float u4 = g2.uniform();
+            const float4 c0 = random_plane(g2, P.depth_min, P.depth_max);
+            float4 cand[5];
+            refine_candidates(x, y, best_plane, c0, rn, u1, u2, u3, u4, P.pert_pi, cand);
+            // the candidate equal to the best plane has the best cost and cannot win
+            bool skip3 = __float_as_uint(cand[3].w) == __float_as_uint(best_plane.w);
+            const int r0 = nact;                         // rows of the refinement candidates
+            if (lane == 0)
+                for (int i = 0; i < 5; ++i) S.plane[r0 + i] = cand[i];
+            __syncwarp();
+            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull);
+            weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane);
 
-            // ---- refinement (PlaneHypothesisRefinement_Frame, :400-471) -----
-            {
-                const float depth_now = best_plane.w;
-                (void)g2.uniform();                      // depth_rand: drawn, never used
-                const float4 rn = random_normal(g2);
-                const float4 pn = perturbed_normal(x, y, best_plane, g2, P.pert_pi);
-                const float dmin_p = __fmul_rn(__fsub_rn(1.0f, 0.02f), depth_now);
-                const float dmax_p = __fmul_rn(__fadd_rn(1.0f, 0.02f), depth_now);
-                const float depth_perturbed = __fmaf_rn(g2.uniform(), __fsub_rn(dmax_p, dmin_p), dmin_p);
-                float4 cand[5];
-                cand[0] = random_plane(g2, P.depth_min, P.depth_max);
-                cand[1] = rn;
-                cand[2] = pn;
-                cand[3] = best_plane;
-                cand[4] = best_plane;
-                cand[4].w = depth_perturbed;
-                for (int i = 1; i < 5; ++i) cand[i].w = to_disparity(x, y, disparity_plane(x, y, cand[i]));
-                if (lane == 0)
-                    for (int i = 0; i < 5; ++i) S.plane[i] = cand[i];
-                __syncwarp();
-                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, 5, nc, lane);
-                weigh_hyps(S, K, 5, nc, vw_lo, vw_hi, lane);
-                for (int i = 0; i < 5; ++i) {
-                    const float c = S.wres[i];
-                    if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = S.wmin[i]; }
+            bool changed = false;
+            int hs = 0;                                  // speculative row of proposal n
+            for (int n = 0; n < nsel; ++n) {
+                const int k = nth_set_bit(tsel, n);
+                const int nvid = F.nb_ids[vid * K + k];
+                const int spec_q = S.aux[n];
+                int q = spec_q;
+                if (changed) q = (nvid >= 0) ? proposal_pos(T.geo[k], x, y, W, H, best_plane) : -1;
+                float c = kCostMax;
+                int cmin = -1;
+                float4 proxy = make_float4(0.f, 0.f, 1.f, 0.f);
+                if (q >= 0 && q == spec_q) {
+                    c = S.wres[hs];
+                    cmin = S.wmin[hs];
+                    proxy = S.plane[hs];
+                } else if (q >= 0) {
+                    // the best plane moved the sample position: rebuild this proposal in its
+                    // own row (or the spare row after the refinement candidates) and evaluate it
+                    const int row = (spec_q >= 0) ? hs : r0 + 5;
+                    proxy = proposal_plane(T.geo[k], prev.plane + (size_t)nvid * P.ppv, q, x, y, W);
+                    __syncwarp();
+                    if (lane == 0) S.plane[row] = proxy;
+                    __syncwarp();
+                    eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull);
+                    weigh_hyps(S, K, row + 1, nc, vw_lo, vw_hi, lane);
+                    c = S.wres[row];
+                    cmin = S.wmin[row];
                 }
+                if (spec_q >= 0) ++hs;
+                if (q >= 0 && c < best_cost) { best_cost = c; best_plane = proxy; best_min = cmin; changed = true; }
+            }
+            if (changed) {
+                // candidates 2-4 follow the best plane: rebuild and evaluate them again
+                refine_candidates(x, y, best_plane, c0, rn, u1, u2, u3, u4, P.pert_pi, cand);
+                skip3 = __float_as_uint(cand[3].w) == __float_as_uint(best_plane.w);
+                __syncwarp();
+                if (lane == 0)
+                    for (int i = 2; i < 5; ++i) S.plane[r0 + i] = cand[i];
+                __syncwarp();
+                const uint64_t redo = (7ull << (r0 + 2)) & ~(skip3 ? (1ull << (r0 + 3)) : 0ull);
+                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo);
+                weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane);
+            }
+            for (int i = 0; i < 5; ++i) {
+                if (i == 3 && skip3) continue;
+                const float c = S.wres[r0 + i];
+                if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = S.wmin[r0 + i]; }
             }
             if (lane == 0) {
                 float4 best_disp = make_float4(0.f, 0.f, 0.f, 0.f);

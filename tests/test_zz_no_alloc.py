@@ -52,7 +52,7 @@ def test_noalloc_sweep_matches_pfd_pm_sweep(pfd, pitch, K, patch, blur):
 
 
 def test_noalloc_sweep_rejects_too_many_neighbours(pfd):
-    """32 neighbours need 70 KB of scratch per CTA (eight warps of cost
+    """32 neighbours need 62 KB of scratch per CTA (eight warps of cost
     vectors): the 8 MiB array cannot give every SM one CTA, so the call fails
     before launching anything."""
     w = pfd.make_workload(260, 200, 23.0, 4, seed=5, max_nb=32)
