@@ -388,7 +388,7 @@ def run_engine(args, rank, world, local_rank):
                     "h2d_bytes_per_step": int(w.frame.raw.nbytes),
                     "d2h_bytes_per_step": int(out_plane.numel() * 4 + out_cost.numel() * 4 + out_sel.numel() * 4 +
                                               out_stack.numel() * 4)},
-            "roofline": {"bound": "fp32", "kernel": "pm_sweep_kernel", "achieved": round(achieved, 3),
+            "roofline": {"bound": "fp32", "kernel": "pm_sweep_warp_kernel", "achieved": round(achieved, 3),
                          "peak": round(fp32_tflops, 2), "unit": "TFLOP/s", "frac": round(achieved / fp32_tflops, 4),
                          "peak_source": "measured FP32 FFMA rate on this device (pfd_fp32_fma_rate); "
                                         "MEASURED_PEAKS.json has no FP32 figure",
