@@ -258,6 +258,35 @@ pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg,
 pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_slices, int out_w, int out_h,
                        float* out);
 
+/* ---- virtual depth to real depth (FP64) -----------------------------------
+ * The behavioural model z = (v c1 + c2) / (1 - v c0) of FocalStack/
+ * VirtualToRealDepthFunc.cpp and LFRefocus.cpp, in double precision on the
+ * device.  vd and the outputs are host arrays of n values. */
+/* VirtualToRealDepthFunc::convertVirtualToRealDepth (VirtualToRealDepthFunc.cpp:
+ * 3421-3450): double results; NaN, infinite and negative values become 0. */
+pfd_status pfd_vd_to_rd_map(pfd_ctx* ctx, const float* vd, size_t n, const double c[3], double* rd);
+/* The same on device arrays (enqueued on the context's stream, no synchronisation). */
+pfd_status pfd_vd_to_rd_map_device(pfd_ctx* ctx, const float* vd_dev, size_t n, const double c[3], double* rd_dev);
+/* LFRefocus::ConvertVdToRd (LFRefocus.cpp:2515-2534) per value: |1 - v c0| < 1e-12,
+ * non-finite or negative results give 0; float results. */
+pfd_status pfd_vd_to_rd_points(pfd_ctx* ctx, const float* vd, size_t n, const double c[3], float* rd);
+/* One depth interval of the segmented model (behaviorModelParamsSegment.xml). */
+typedef struct pfd_vd_segment {
+    double depth_min, depth_max, c0, c1, c2;
+} pfd_vd_segment;
+/* LFRefocus::ConvertVdToRdSegment (LFRefocus.cpp:2536-2593): the first segment
+ * with depth_min <= v < depth_max applies, 0 when none does; at most 64
+ * segments.  The reference re-reads the XML file for every pixel; here the
+ * caller passes the segments once. */
+pfd_status pfd_vd_to_rd_segments(pfd_ctx* ctx, const float* vd, size_t n, const pfd_vd_segment* segs, int nseg,
+                                 float* rd);
+/* VirtualToRealDepthFunc::BehavioralModel (VirtualToRealDepthFunc.cpp:3390-3418):
+ * least-squares c of [a_L v, v, 1] c = a_L over n >= 3 pairs (a_L = real_depth).
+ * The normal-equation sums are formed in FP64 on the device and the 3x3 system
+ * is solved on the host (the reference uses cv::solve with SVD; results agree
+ * to the system's conditioning). */
+pfd_status pfd_fit_behavioral_model(pfd_ctx* ctx, const float* real_depth, const float* vd, size_t n, double c[3]);
+
 /* ---- measurement --------------------------------------------------------
  * No counterpart in the reference (it has no timers or counters on this path,
  * see its Util/Logger only).  Tap counting switches the PatchMatch kernels to

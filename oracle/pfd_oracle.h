@@ -194,6 +194,13 @@ int orc_refocus(const orc_frame* f, int raw_w, int raw_h, const float* slice_vd,
 long long orc_refocus_samples(const orc_frame* f, int raw_w, int raw_h, const float* slice_vd, int n_slices,
                               int out_w, int out_h);
 
+/* Virtual-to-real depth (FocalStack/LFRefocus.cpp:2515-2593,
+ * FocalStack/VirtualToRealDepthFunc.cpp:3390-3450), FP64. */
+float orc_vd_to_rd(float v_depth, const double c[3]);
+float orc_vd_to_rd_segment(float v_depth, const double* segs /* [nseg][5]: min, max, c0, c1, c2 */, int nseg);
+void  orc_vd_to_rd_map(const float* vd, long n, const double c[3], double* rd);
+int   orc_behavioral_fit(const float* real_depth, const float* vd, long n, double c[3]);
+
 /* Scalar hooks for unit tests of the canonical arithmetic. */
 float orc_expf(float x);
 float orc_uniform(uint64_t seed, uint32_t sweep, uint32_t pixel, uint32_t n);

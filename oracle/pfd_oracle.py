@@ -106,6 +106,12 @@ def lib() -> ctypes.CDLL:
         L.orc_cycle_check.argtypes = [FP, YP, _F, SP, ctypes.POINTER(OrcCycleStats), _P, _P, _P]
         L.orc_mean_std_3x3.argtypes = [_P, _I, _I, _I, _P, _P]
         L.orc_refocus.argtypes = [FP, _I, _I, _P, _I, _I, _I, _P]
+        L.orc_vd_to_rd.argtypes = [_F, _P]
+        L.orc_vd_to_rd.restype = _F
+        L.orc_vd_to_rd_segment.argtypes = [_F, _P, _I]
+        L.orc_vd_to_rd_segment.restype = _F
+        L.orc_vd_to_rd_map.argtypes = [_P, ctypes.c_long, _P, _P]
+        L.orc_behavioral_fit.argtypes = [_P, _P, ctypes.c_long, _P]
         L.orc_refocus_samples.argtypes = [FP, _I, _I, _P, _I, _I, _I]
         L.orc_refocus_samples.restype = ctypes.c_longlong
         _lib = L
@@ -273,6 +279,37 @@ def refocus(orc: "Oracle", raw_w: int, raw_h: int, slice_vd, out_w: int, out_h: 
 def refocus_samples(orc: "Oracle", raw_w: int, raw_h: int, slice_vd, out_w: int, out_h: int) -> int:
     vd = np.ascontiguousarray(slice_vd, np.float32)
     return int(lib().orc_refocus_samples(ctypes.byref(orc.f), raw_w, raw_h, _p(vd), vd.shape[0], out_w, out_h))
+
+
+def vd_to_rd_points(vd, c):
+    """LFRefocus::ConvertVdToRd per value (float results)."""
+    cc = np.ascontiguousarray(c, np.float64)
+    return np.array([lib().orc_vd_to_rd(float(v), _p(cc)) for v in np.asarray(vd, np.float32)], np.float32)
+
+
+def vd_to_rd_segments(vd, segs):
+    """LFRefocus::ConvertVdToRdSegment per value; segs [n][5] (min, max, c0, c1, c2)."""
+    sg = np.ascontiguousarray(segs, np.float64).reshape(-1, 5)
+    return np.array([lib().orc_vd_to_rd_segment(float(v), _p(sg), sg.shape[0]) for v in np.asarray(vd, np.float32)],
+                    np.float32)
+
+
+def vd_to_rd_map(vd, c) -> np.ndarray:
+    """VirtualToRealDepthFunc::convertVirtualToRealDepth (double results)."""
+    v = np.ascontiguousarray(vd, np.float32).ravel()
+    out = np.zeros(v.shape[0], np.float64)
+    cc = np.ascontiguousarray(c, np.float64)
+    lib().orc_vd_to_rd_map(_p(v), v.shape[0], _p(cc), _p(out))
+    return out
+
+
+def behavioral_fit(real_depth, vd):
+    """VirtualToRealDepthFunc::BehavioralModel (normal equations, long double)."""
+    r = np.ascontiguousarray(real_depth, np.float32)
+    v = np.ascontiguousarray(vd, np.float32)
+    c = np.zeros(3, np.float64)
+    assert lib().orc_behavioral_fit(_p(r), _p(v), r.shape[0], _p(c)) == 0
+    return c
 
 
 def mean_std_3x3(img, x0: int, y0: int):

@@ -187,6 +187,11 @@ def lib() -> ctypes.CDLL:
             "pfd_reprojection_error": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P],
             "pfd_refocus": [_P, _I, _P, _I, _I, _I, _P],
             "pfd_launch_count": [_P, ctypes.POINTER(ctypes.c_ulonglong)],
+            "pfd_vd_to_rd_map": [_P, _P, ctypes.c_size_t, _P, _P],
+            "pfd_vd_to_rd_map_device": [_P, _P, ctypes.c_size_t, _P, _P],
+            "pfd_vd_to_rd_points": [_P, _P, ctypes.c_size_t, _P, _P],
+            "pfd_vd_to_rd_segments": [_P, _P, ctypes.c_size_t, _P, _I, _P],
+            "pfd_fit_behavioral_model": [_P, _P, _P, ctypes.c_size_t, _P],
             "pfd_cycle_check": [_P, _I, ctypes.POINTER(CycleCfgC), _F, ctypes.POINTER(CycleStatsC), _P, _P, _P],
         }
         for name, args in sig.items():
@@ -370,6 +375,45 @@ class Context:
                                             _ptr(geo) if maps else None, _ptr(pho) if maps else None,
                                             _ptr(tm) if maps else None), "pfd_cycle_check")
         return {k: getattr(out, k) for k in CYCLE_STATS}, geo, pho, tm
+
+    def vd_to_rd_map(self, vd, c) -> np.ndarray:
+        """VirtualToRealDepthFunc::convertVirtualToRealDepth on the device (FP64)."""
+        v = np.ascontiguousarray(vd, dtype=np.float32)
+        out = np.empty(v.shape, np.float64)
+        cc = np.ascontiguousarray(c, dtype=np.float64)
+        self._check(self._L.pfd_vd_to_rd_map(self._h, _ptr(v), v.size, _ptr(cc), _ptr(out)), "pfd_vd_to_rd_map")
+        return out
+
+    def vd_to_rd_map_device(self, vd_ptr: int, n: int, c, rd_ptr: int) -> None:
+        cc = np.ascontiguousarray(c, dtype=np.float64)
+        self._check(self._L.pfd_vd_to_rd_map_device(self._h, _P(vd_ptr), n, _ptr(cc), _P(rd_ptr)),
+                    "pfd_vd_to_rd_map_device")
+
+    def vd_to_rd_points(self, vd, c) -> np.ndarray:
+        """LFRefocus::ConvertVdToRd per value on the device."""
+        v = np.ascontiguousarray(vd, dtype=np.float32)
+        out = np.empty(v.shape, np.float32)
+        cc = np.ascontiguousarray(c, dtype=np.float64)
+        self._check(self._L.pfd_vd_to_rd_points(self._h, _ptr(v), v.size, _ptr(cc), _ptr(out)), "pfd_vd_to_rd_points")
+        return out
+
+    def vd_to_rd_segments(self, vd, segs) -> np.ndarray:
+        """LFRefocus::ConvertVdToRdSegment; segs [n][5] (depth_min, depth_max, c0, c1, c2)."""
+        v = np.ascontiguousarray(vd, dtype=np.float32)
+        sg = np.ascontiguousarray(segs, dtype=np.float64).reshape(-1, 5)
+        out = np.empty(v.shape, np.float32)
+        self._check(self._L.pfd_vd_to_rd_segments(self._h, _ptr(v), v.size, _ptr(sg), sg.shape[0], _ptr(out)),
+                    "pfd_vd_to_rd_segments")
+        return out
+
+    def fit_behavioral_model(self, real_depth, vd) -> np.ndarray:
+        """VirtualToRealDepthFunc::BehavioralModel: (c0, c1, c2)."""
+        r = np.ascontiguousarray(real_depth, dtype=np.float32)
+        v = np.ascontiguousarray(vd, dtype=np.float32)
+        c = np.zeros(3, np.float64)
+        self._check(self._L.pfd_fit_behavioral_model(self._h, _ptr(r), _ptr(v), r.size, _ptr(c)),
+                    "pfd_fit_behavioral_model")
+        return c
 
     def launch_count(self) -> int:
         n = ctypes.c_ulonglong()

@@ -18,6 +18,7 @@
 #include "pm_kernels.h"
 #include "check_kernels.h"
 #include "refocus_kernels.h"
+#include "vdrd_kernels.h"
 
 namespace {
 
@@ -890,6 +891,129 @@ static pfd_status build_lens_grid(pfd_ctx* ctx, Frame& f)
                        ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));      // host vectors go out of scope
     f.grid_w = gw; f.grid_h = gh; f.grid_x0 = x0; f.grid_y0 = y0; f.grid_cell = cell;
+    return PFD_OK;
+}
+
+// Stream-ordered scratch for the host-array entry points below.
+struct AsyncBuf {
+    cudaStream_t st;
+    void* p = nullptr;
+    AsyncBuf(cudaStream_t s, size_t bytes, cudaError_t& e) : st(s) { e = cudaMallocAsync(&p, bytes, s); }
+    ~AsyncBuf() { if (p) cudaFreeAsync(p, st); }
+};
+
+static pfd_status vd_args(pfd_ctx* ctx, const void* vd, size_t n, const void* out)
+{
+    if (!ctx) return PFD_EINVAL;
+    if (n > 0 && (!vd || !out)) return fail(ctx, PFD_EINVAL, "vd / output array is NULL");
+    if (n > ((size_t)1 << 33)) return fail(ctx, PFD_EINVAL, "too many values (%zu)", n);
+    return PFD_OK;
+}
+
+pfd_status pfd_vd_to_rd_map_device(pfd_ctx* ctx, const float* vd_dev, size_t n, const double c[3], double* rd_dev)
+{
+    pfd_status st = vd_args(ctx, vd_dev, n, rd_dev);
+    if (st != PFD_OK) return st;
+    if (!c) return fail(ctx, PFD_EINVAL, "model coefficients are NULL");
+    if (n == 0) return PFD_OK;
+    DeviceGuard g(ctx->device);
+    CU(pfd::launch_vd_to_rd(vd_dev, n, c[0], c[1], c[2], 0, rd_dev, ctx->stream));
+    ctx->launches += 1;
+    return PFD_OK;
+}
+
+static pfd_status vd_host(pfd_ctx* ctx, const float* vd, size_t n, const double c[3], int mode, void* out)
+{
+    pfd_status st = vd_args(ctx, vd, n, out);
+    if (st != PFD_OK) return st;
+    if (!c) return fail(ctx, PFD_EINVAL, "model coefficients are NULL");
+    if (n == 0) return PFD_OK;
+    DeviceGuard g(ctx->device);
+    const size_t osz = mode == 0 ? 8 : 4;
+    cudaError_t e;
+    AsyncBuf buf(ctx->stream, n * 4 + n * osz + 16, e);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, PFD_ENOMEM, "vd_to_rd: device buffer of %zu bytes", n * (4 + osz)); }
+    float* d_vd = (float*)buf.p;
+    void* d_out = (void*)(((uintptr_t)(d_vd + n) + 15) & ~(uintptr_t)15);
+    CU(cudaMemcpyAsync(d_vd, vd, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CU(pfd::launch_vd_to_rd(d_vd, n, c[0], c[1], c[2], mode, d_out, ctx->stream));
+    ctx->launches += 1;
+    CU(cudaMemcpyAsync(out, d_out, n * osz, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return PFD_OK;
+}
+
+pfd_status pfd_vd_to_rd_map(pfd_ctx* ctx, const float* vd, size_t n, const double c[3], double* rd)
+{
+    return vd_host(ctx, vd, n, c, 0, rd);
+}
+
+pfd_status pfd_vd_to_rd_points(pfd_ctx* ctx, const float* vd, size_t n, const double c[3], float* rd)
+{
+    return vd_host(ctx, vd, n, c, 1, rd);
+}
+
+pfd_status pfd_vd_to_rd_segments(pfd_ctx* ctx, const float* vd, size_t n, const pfd_vd_segment* segs, int nseg,
+                                 float* rd)
+{
+    pfd_status st = vd_args(ctx, vd, n, rd);
+    if (st != PFD_OK) return st;
+    if (nseg < 0 || nseg > pfd::kMaxVdSegments || (nseg > 0 && !segs))
+        return fail(ctx, PFD_EINVAL, "need 0..%d segments", pfd::kMaxVdSegments);
+    if (n == 0) return PFD_OK;
+    DeviceGuard g(ctx->device);
+    cudaError_t e;
+    AsyncBuf buf(ctx->stream, n * 8 + (size_t)nseg * 40 + 32, e);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, PFD_ENOMEM, "vd_to_rd_segments: device buffer"); }
+    double* d_seg = (double*)buf.p;
+    float* d_vd = (float*)(d_seg + 5 * (size_t)nseg);
+    float* d_out = d_vd + n;
+    static_assert(sizeof(pfd_vd_segment) == 5 * sizeof(double), "segment layout");
+    if (nseg) CU(cudaMemcpyAsync(d_seg, segs, (size_t)nseg * 40, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(d_vd, vd, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CU(pfd::launch_vd_to_rd_segments(d_vd, n, d_seg, nseg, d_out, ctx->stream));
+    ctx->launches += 1;
+    CU(cudaMemcpyAsync(rd, d_out, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return PFD_OK;
+}
+
+pfd_status pfd_fit_behavioral_model(pfd_ctx* ctx, const float* real_depth, const float* vd, size_t n, double c[3])
+{
+    pfd_status st = vd_args(ctx, vd, n, c);
+    if (st != PFD_OK) return st;
+    if (!real_depth) return fail(ctx, PFD_EINVAL, "real_depth is NULL");
+    if (n < 3) return fail(ctx, PFD_EINVAL, "the behavioural model needs at least 3 pairs, got %zu", n);
+    DeviceGuard g(ctx->device);
+    const int nb = pfd::fit_blocks(n);
+    cudaError_t e;
+    AsyncBuf buf(ctx->stream, n * 8 + (size_t)nb * 72 + 72 + 32, e);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, PFD_ENOMEM, "behavioural fit: device buffer"); }
+    double* d_partial = (double*)buf.p;
+    double* d_sums = d_partial + (size_t)nb * 9;
+    float* d_real = (float*)(d_sums + 9);
+    float* d_vd = d_real + n;
+    CU(cudaMemcpyAsync(d_real, real_depth, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(d_vd, vd, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CU(pfd::launch_fit_sums(d_real, d_vd, n, d_partial, d_sums, ctx->stream));
+    ctx->launches += 2;
+    double h[9];
+    CU(cudaMemcpyAsync(h, d_sums, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    // normal equations, Gaussian elimination with partial pivoting
+    double M[3][4] = { { h[0], h[1], h[2], h[6] }, { h[1], h[3], h[4], h[7] }, { h[2], h[4], h[5], h[8] } };
+    for (int col = 0; col < 3; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 3; ++r) if (std::fabs(M[r][col]) > std::fabs(M[piv][col])) piv = r;
+        if (!(std::fabs(M[piv][col]) > 1e-300)) return fail(ctx, PFD_EINVAL, "behavioural fit: singular system");
+        if (piv != col) for (int q = 0; q < 4; ++q) std::swap(M[col][q], M[piv][q]);
+        for (int r = 0; r < 3; ++r) {
+            if (r == col) continue;
+            const double f = M[r][col] / M[col][col];
+            for (int q = col; q < 4; ++q) M[r][q] -= f * M[col][q];
+        }
+    }
+    for (int r = 0; r < 3; ++r) c[r] = M[r][3] / M[r][r];
     return PFD_OK;
 }
 
