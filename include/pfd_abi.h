@@ -47,6 +47,9 @@ typedef int pfd_status;
 #define PFD_ENODEV      -6   /* no such CUDA device */
 #define PFD_ESTATE      -7   /* call out of order (e.g. a sweep before initialisation) */
 
+/* Longest neighbour list of a view: selected-view masks are 32 bits. */
+#define PFD_MAX_NEIGHBORS 32
+
 /* Matching parameters: the fields of PatchMatchParamsLF (MVStereo/LFDepthInfo.h:19-46)
  * that the frame path reads, as AdaptMIPMFrame::InitGPUParamsFromCPUParams sets
  * them (AdaptMIPMFrame.cpp:126-143). */
@@ -64,7 +67,8 @@ typedef struct {
 
 /* ---- context ------------------------------------------------------------ */
 
-/* Opens a context on CUDA device `device` with its own stream.  hbm_budget_bytes
+/* Opens a context on CUDA device `device` (-1: the calling thread's current
+ * device, the one cudaSetDevice chose) with its own stream.  hbm_budget_bytes
  * caps the device memory the context's frames may hold (0 = no cap). */
 pfd_status pfd_create(pfd_ctx** out, int device, size_t hbm_budget_bytes);
 /* Frees every frame and the context.  Safe on NULL. */
@@ -105,6 +109,13 @@ pfd_status pfd_frame_create(pfd_ctx* ctx, int* frame_id, int W, int H,
 pfd_status pfd_frame_set_raw(pfd_ctx* ctx, int frame_id, const uint8_t* raw, int raw_pitch);
 /* Same, from a raw frame already in this device's memory. */
 pfd_status pfd_frame_set_raw_device(pfd_ctx* ctx, int frame_id, const uint8_t* raw_dev, int raw_pitch);
+/* Fills the micro-images directly, for callers that hold them already sliced:
+ * MLA_Problem::m_Image_gray of every view, the images
+ * AdaptMIPMFrame::BuildViewIndexMap (AdaptMIPMFrame.cpp:126-215) collects and
+ * CreateGrayImageObject (:217-245) binds to textures.  images [n_views][mi_h][mi_w],
+ * views in frame order.  The frame then has no raw image (pfd_refocus needs one).
+ * Returns when the host buffer may be reused. */
+pfd_status pfd_frame_set_micro_images(pfd_ctx* ctx, int frame_id, const uint8_t* images);
 /* pfd_frame_create + pfd_frame_set_raw. */
 pfd_status pfd_frame_upload(pfd_ctx* ctx, int* frame_id, const uint8_t* raw, int W, int H, int raw_pitch,
                             const float* centers, const int* tilekeys, int n_views,
@@ -156,6 +167,14 @@ pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params
  * c_cuda, disp_v_cuda, selected_views}. */
 pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane /*[.][4]*/, float* cost,
                         float* disp /*[.][4]*/, uint32_t* sel);
+/* The inverse of pfd_download: makes host arrays in the same layout the frame's
+ * current state, for a consistency pass over results that live on the host
+ * (the DisparityAndNormal arrays MIDisparityFilterCPU::FilterGlobal and
+ * MICycleCheckerCPU::CheckGlobal read, MIDisparityFilter.cpp:962-986,
+ * MICycleCheck.cpp:780-893).  All four are required.  Returns when the host
+ * buffers may be reused. */
+pfd_status pfd_state_upload(pfd_ctx* ctx, int frame_id, const float* plane /*[.][4]*/, const float* cost,
+                            const float* disp /*[.][4]*/, const uint32_t* sel);
 
 /* ---- consistency pass -------------------------------------------------------
  * MIDisparityFilterConfig (CheckModule/MIDisparityFilter.h:24-57).  The values

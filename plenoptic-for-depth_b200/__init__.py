@@ -171,6 +171,8 @@ def lib() -> ctypes.CDLL:
             "pfd_frame_create": [_P, ctypes.POINTER(_I), _I, _I, _P, _P, _I, _I, _I, _P, _P, _I, _P],
             "pfd_frame_set_raw": [_P, _I, _P, _I],
             "pfd_frame_set_raw_device": [_P, _I, _P, _I],
+            "pfd_frame_set_micro_images": [_P, _I, _P],
+            "pfd_state_upload": [_P, _I, _P, _P, _P, _P],
             "pfd_frame_upload": [_P, ctypes.POINTER(_I), _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _I, _P],
             "pfd_frame_free": [_P, _I],
             "pfd_patchmatch": [_P, _I, ctypes.POINTER(PmParamsC), ctypes.c_uint64],
@@ -287,6 +289,20 @@ class Context:
 
     def frame_set_raw_device(self, fid: int, dev_ptr: int, pitch: int) -> None:
         self._check(self._L.pfd_frame_set_raw_device(self._h, fid, _P(dev_ptr), pitch), "pfd_frame_set_raw_device")
+
+    def frame_set_micro_images(self, fid: int, images: np.ndarray) -> None:
+        f = self._frames[fid]
+        im = np.ascontiguousarray(images, dtype=np.uint8)
+        if im.shape != (f["V"], f["mi_h"], f["mi_w"]):
+            raise ValueError(f"micro-images must be {(f['V'], f['mi_h'], f['mi_w'])}, got {im.shape}")
+        self._check(self._L.pfd_frame_set_micro_images(self._h, fid, _ptr(im)), "pfd_frame_set_micro_images")
+
+    def state_upload(self, fid: int, plane, cost, disp, sel) -> None:
+        f = self._frames[fid]
+        n = f["V"] * f["mi_w"] * f["mi_h"]
+        arrs = [np.ascontiguousarray(plane, np.float32).reshape(n, 4), np.ascontiguousarray(cost, np.float32).reshape(n),
+                np.ascontiguousarray(disp, np.float32).reshape(n, 4), np.ascontiguousarray(sel, np.uint32).reshape(n)]
+        self._check(self._L.pfd_state_upload(self._h, fid, *[_ptr(a) for a in arrs]), "pfd_state_upload")
 
     def frame_upload(self, raw, centers, tilekeys, mi_w, mi_h, nb_ids, nb_counts, blur=None) -> int:
         fid = self.frame_create(raw.shape[1], raw.shape[0], centers, tilekeys, mi_w, mi_h, nb_ids, nb_counts, blur)

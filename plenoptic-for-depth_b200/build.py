@@ -26,6 +26,11 @@ NVCC_FLAGS = [
 CU_SOURCES = ["pm_kernels.cu", "pm_sweep.cu", "check_kernels.cu", "refocus_kernels.cu", "vdrd_kernels.cu", "pfd_abi.cu", "diag.cu"]
 CPP_SOURCES = ["neighbors.cpp"]
 SYNTH_LIB = os.path.join(OUT, "libpfd_synth.so")
+HOST_DIR = os.path.join(PKG_DIR, "host")
+HOST_LIB = os.path.join(OUT, "libpfd_host.so")
+HOST_SOURCES = ["lf_types.cpp", "frame_views.cpp", "AdaptMIPMFrame.cpp", "MIDisparityFilter.cpp", "MICycleCheck.cpp"]
+GXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-parameter",
+             "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include"]
 
 
 def _run(cmd: list[str]) -> None:
@@ -72,9 +77,24 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
               "-I", "/usr/local/cuda/include", "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
     tmp = LIB + ".tmp"
-    _run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-ccbin", "/usr/bin/g++"])
+    _run([NVCC, *ARCH, "-shared", "-Xlinker", "-soname=libpfd.so", "-o", tmp, *objs, "-ccbin", "/usr/bin/g++"])
     os.replace(tmp, LIB)
     return LIB
+
+
+def build_host(force: bool = False) -> str:
+    """Compile libpfd_host.so: the C++ classes with the reference's interface
+    (include/pfd/) over libpfd.so.  Plain g++; no device code."""
+    lib = build_lib()
+    srcs = [os.path.join(HOST_DIR, s) for s in HOST_SOURCES]
+    deps = srcs + [os.path.join(HOST_DIR, "frame_views.h"), lib, __file__] + _deps()
+    if not force and not _stale(HOST_LIB, deps):
+        return HOST_LIB
+    tmp = HOST_LIB + ".tmp"
+    _run(["/usr/bin/g++", *GXX_FLAGS, "-shared", "-Wl,-soname,libpfd_host.so", "-o", tmp, *srcs,
+          "-L", OUT, "-l:libpfd.so", "-Wl,-rpath,$ORIGIN"])
+    os.replace(tmp, HOST_LIB)
+    return HOST_LIB
 
 
 def build_synth(force: bool = False) -> str:
@@ -90,6 +110,7 @@ def build_synth(force: bool = False) -> str:
 
 TEST_OUT = os.path.join(ROOT, "tests", "_build")
 TEX_PROBE = os.path.join(TEST_OUT, "libtexprobe.so")
+SHIM_PROBE = os.path.join(TEST_OUT, "libshimprobe.so")
 
 
 def build_test_helpers(force: bool = False) -> str:
@@ -100,11 +121,19 @@ def build_test_helpers(force: bool = False) -> str:
         tmp = TEX_PROBE + ".tmp"
         _run([NVCC, *ARCH, "-O2", "-shared", "-Xcompiler", "-fPIC", "-ccbin", "/usr/bin/g++", src, "-o", tmp])
         os.replace(tmp, TEX_PROBE)
+    host = build_host()
+    src = os.path.join(ROOT, "tests", "csrc", "shim_probe.cpp")
+    if force or _stale(SHIM_PROBE, [src, host, __file__] + _deps()):
+        tmp = SHIM_PROBE + ".tmp"
+        rel = os.path.relpath(OUT, TEST_OUT)
+        _run(["/usr/bin/g++", *GXX_FLAGS, "-shared", "-o", tmp, src, "-L", OUT, "-l:libpfd_host.so", "-l:libpfd.so",
+              "-Wl,-rpath,$ORIGIN/" + rel])
+        os.replace(tmp, SHIM_PROBE)
     return TEX_PROBE
 
 
 def build_all(force: bool = False, verbose: bool = False) -> list[str]:
-    return [build_lib(force, verbose), build_synth(force), build_test_helpers(force)]
+    return [build_lib(force, verbose), build_host(force), build_synth(force), build_test_helpers(force)]
 
 
 if __name__ == "__main__":

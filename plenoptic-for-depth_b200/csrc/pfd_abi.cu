@@ -26,6 +26,7 @@ struct Frame {
     int W = 0, H = 0;                 // raw frame
     int V = 0, mi_w = 0, mi_h = 0, K = 0, tile_stride = 0;
     bool has_raw = false, has_blur = false;
+    bool has_mi = false;              // micro-image tiles filled (from a raw frame or uploaded)
     uint8_t* d_raw = nullptr;
     uint8_t* d_gray = nullptr;
     uint8_t* d_blur = nullptr;
@@ -163,7 +164,7 @@ pfd_status check_params(pfd_ctx* ctx, const Frame& f, const pfd_pm_params* p)
     if (!(p->base > 0.0f)) return fail(ctx, PFD_EINVAL, "base (lens pitch) must be > 0");
     if (p->top_k < 1) return fail(ctx, PFD_EINVAL, "top_k must be >= 1");
     if (p->max_iterations < 0) return fail(ctx, PFD_EINVAL, "max_iterations must be >= 0");
-    if (!f.has_raw) return fail(ctx, PFD_ESTATE, "frame has no raw image yet");
+    if (!f.has_mi) return fail(ctx, PFD_ESTATE, "frame has no micro-images yet");
     return PFD_OK;
 }
 
@@ -230,6 +231,7 @@ pfd_status pfd_create(pfd_ctx** out, int device, size_t hbm_budget_bytes)
     if (!out) return PFD_EINVAL;
     *out = nullptr;
     int n = 0;
+    if (device == -1 && cudaGetDevice(&device) != cudaSuccess) device = -2;   // the caller's current device
     if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
         cudaGetLastError();
         return PFD_ENODEV;
@@ -417,6 +419,7 @@ static pfd_status set_raw(pfd_ctx* ctx, int frame_id, const uint8_t* raw, int ra
     CU(pfd::launch_slice(f->d_raw, f->W, f->d_origin, f->V, f->mi_w, f->mi_h, f->tile_stride, f->d_gray, ctx->stream));
     ctx->launches += 1;
     f->has_raw = true;
+    f->has_mi = true;
     f->has_state = false;
     return PFD_OK;
 }
@@ -429,6 +432,42 @@ pfd_status pfd_frame_set_raw(pfd_ctx* ctx, int frame_id, const uint8_t* raw, int
 pfd_status pfd_frame_set_raw_device(pfd_ctx* ctx, int frame_id, const uint8_t* raw_dev, int raw_pitch)
 {
     return set_raw(ctx, frame_id, raw_dev, raw_pitch, true);
+}
+
+pfd_status pfd_frame_set_micro_images(pfd_ctx* ctx, int frame_id, const uint8_t* images)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!images) return fail(ctx, PFD_EINVAL, "micro-images are NULL");
+    DeviceGuard g(ctx->device);
+    const size_t ppv = (size_t)f->mi_w * f->mi_h;
+    std::vector<uint8_t> tiles((size_t)f->V * f->tile_stride, 0);
+    for (int v = 0; v < f->V; ++v) std::memcpy(&tiles[(size_t)v * f->tile_stride], images + (size_t)v * ppv, ppv);
+    CU(cudaMemcpyAsync(f->d_gray, tiles.data(), tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));       // the staging vector dies on return
+    f->has_mi = true;
+    f->has_state = false;
+    return PFD_OK;
+}
+
+pfd_status pfd_state_upload(pfd_ctx* ctx, int frame_id, const float* plane, const float* cost, const float* disp,
+                            const uint32_t* sel)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!plane || !cost || !disp || !sel) return fail(ctx, PFD_EINVAL, "state_upload: NULL array");
+    DeviceGuard g(ctx->device);
+    const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
+    const pfd::StateDev& s = f->s[f->cur];
+    CU(cudaMemcpyAsync(s.plane, plane, sizeof(float4) * px, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(s.cost, cost, sizeof(float) * px, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(s.disp, disp, sizeof(float4) * px, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(s.sel, sel, sizeof(uint32_t) * px, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));       // host buffers may be reused on return
+    f->has_state = true;
+    return PFD_OK;
 }
 
 pfd_status pfd_frame_upload(pfd_ctx* ctx, int* frame_id, const uint8_t* raw, int W, int H, int raw_pitch,

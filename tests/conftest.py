@@ -49,7 +49,7 @@ def pfd():
     build = importlib.util.spec_from_file_location("pfd_build", os.path.join(PKG_DIR, "build.py"))
     b = importlib.util.module_from_spec(build)
     build.loader.exec_module(b)
-    if not os.path.exists(mod.LIB_PATH) or not os.path.exists(mod.SYNTH_PATH):
+    if not all(os.path.exists(p) for p in (mod.LIB_PATH, mod.SYNTH_PATH, b.HOST_LIB, b.SHIM_PROBE, b.TEX_PROBE)):
         b.build_all()
     return mod
 
