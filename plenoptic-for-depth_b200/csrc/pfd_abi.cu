@@ -37,6 +37,13 @@ struct Frame {
     int* d_nb_counts = nullptr;
     pfd::StateDev s[2] = {};
     int cur = 0;                      // s[cur] is the latest state
+    // Cost vector of every pixel's current plane ([V*ppv][K]), written by the
+    // initialisation and by each sweep for the pixels it updates; bit c of
+    // cvec_valid says the vectors of colour c match the latest state under the
+    // parameters cvec_key (patch, tap stride, sigmas, base).
+    float* d_cvec = nullptr;
+    unsigned cvec_valid = 0;
+    pfd_pm_params cvec_key = {};
     bool has_state = false;
     size_t bytes = 0;
     bool registered = false;          // bytes already counted in the context's total
@@ -191,7 +198,30 @@ pfd::PmParams make_params(const Frame& f, const pfd_pm_params* p, uint64_t seed)
     P.seed = seed;
     P.tap_counter = nullptr;
     P.cost_scratch = nullptr;
+    P.cvec = f.d_cvec;
+    P.cvec_ok = 0;
     return P;
+}
+
+// The stored cost vectors depend on the parameters that shape an NCC.
+bool same_cost_params(const pfd_pm_params& a, const pfd_pm_params& b)
+{
+    return a.patch_size == b.patch_size && a.radius_increment == b.radius_increment &&
+           std::memcmp(&a.sigma_spatial, &b.sigma_spatial, 4) == 0 &&
+           std::memcmp(&a.sigma_color, &b.sigma_color, 4) == 0 && std::memcmp(&a.base, &b.base, 4) == 0;
+}
+
+// Before a sweep of `phase`: may it use the stored vectors?  After it: the
+// updated colour's vectors are valid under `p`.
+bool cvec_usable(const Frame& f, const pfd_pm_params& p, int phase)
+{
+    return ((f.cvec_valid >> phase) & 1u) && same_cost_params(f.cvec_key, p);
+}
+void cvec_swept(Frame& f, const pfd_pm_params& p, int phase)
+{
+    if (!same_cost_params(f.cvec_key, p)) f.cvec_valid = 0;
+    f.cvec_key = p;
+    f.cvec_valid |= 1u << phase;
 }
 
 pfd::FrameDev frame_dev(const Frame& f)
@@ -364,6 +394,7 @@ pfd_status pfd_frame_create(pfd_ctx* ctx, int* frame_id, int W, int H, const flo
     A((void**)&f.d_origin, sizeof(int2) * n_views);
     A((void**)&f.d_nb_ids, sizeof(int) * (size_t)n_views * max_nb);
     A((void**)&f.d_nb_counts, sizeof(int) * n_views);
+    A((void**)&f.d_cvec, sizeof(float) * px * max_nb);
     for (int b = 0; b < 2; ++b) {
         A((void**)&f.s[b].plane, sizeof(float4) * px);
         A((void**)&f.s[b].cost, sizeof(float) * px);
@@ -421,6 +452,7 @@ static pfd_status set_raw(pfd_ctx* ctx, int frame_id, const uint8_t* raw, int ra
     f->has_raw = true;
     f->has_mi = true;
     f->has_state = false;
+    f->cvec_valid = 0;
     return PFD_OK;
 }
 
@@ -448,6 +480,7 @@ pfd_status pfd_frame_set_micro_images(pfd_ctx* ctx, int frame_id, const uint8_t*
     CU(cudaStreamSynchronize(ctx->stream));       // the staging vector dies on return
     f->has_mi = true;
     f->has_state = false;
+    f->cvec_valid = 0;
     return PFD_OK;
 }
 
@@ -467,6 +500,7 @@ pfd_status pfd_state_upload(pfd_ctx* ctx, int frame_id, const float* plane, cons
     CU(cudaMemcpyAsync(s.sel, sel, sizeof(uint32_t) * px, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));       // host buffers may be reused on return
     f->has_state = true;
+    f->cvec_valid = 0;
     return PFD_OK;
 }
 
@@ -511,9 +545,12 @@ pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, 
     pfd::PmParams P = make_params(*f, params, seed);
     if (ctx->counting) P.tap_counter = ctx->d_taps;
     f->cur = 0;
+    f->cvec_valid = 0;
     CU(pfd::launch_init(frame_dev(*f), P, f->s[0], ctx->d_err, ctx->stream));
     ctx->launches += 1;
     f->has_state = true;
+    f->cvec_valid = 3u;
+    f->cvec_key = *params;
     return PFD_OK;
 }
 
@@ -551,10 +588,12 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
         ctx->used += need;
     }
     P.cost_scratch = ctx->d_scratch;
+    P.cvec_ok = cvec_usable(*f, *params, phase);
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
+    cvec_swept(*f, *params, phase);
     return PFD_OK;
 }
 
@@ -732,6 +771,7 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
     CU(cudaMallocAsync((void**)&d_stats, 8 * sizeof(unsigned long long), ctx->stream));
     CU(cudaMemsetAsync(d_stats, 0, 8 * sizeof(unsigned long long), ctx->stream));
     const pfd::StateDev& S = f->s[f->cur];
+    f->cvec_valid = 0;                             // rejected pixels get new planes
     for (size_t s = 0; s + 1 < f->step_start.size(); ++s) {
         const int a = f->step_start[s], b = f->step_start[s + 1];
         cudaError_t e = pfd::launch_filter_step(F, fc, S, f->d_steps + a, b - a, f->d_reason, d_stats, ctx->stream);
@@ -1211,9 +1251,11 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     st = noalloc_scratch(ctx, ctx->device, &scratch);
     if (st != PFD_OK) return st;
     P.cost_scratch = scratch;
+    P.cvec_ok = cvec_usable(*f, *params, phase);
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
+    cvec_swept(*f, *params, phase);
     return PFD_OK;
 }

@@ -31,6 +31,8 @@ struct PmParams {
     uint64_t seed;
     unsigned long long* tap_counter;   // calibration runs only: in-bounds NCC taps evaluated
     float* cost_scratch;    // sweep: per warp, the cost vectors of its current pixel
+    float* cvec;            // [V * ppv][K]: cost vector of each pixel's current plane (init and sweeps write it)
+    int cvec_ok;            // sweep: cvec holds the vectors of the updated colour's current planes
 };
 
 struct FrameDev {

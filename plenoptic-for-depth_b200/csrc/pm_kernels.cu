@@ -258,6 +258,8 @@ __global__ void __launch_bounds__(256) pm_init_kernel(FrameDev F, PmParams P, St
     out.cost[idx] = mean;
     out.disp[idx] = disp;
     out.sel[idx] = mask;
+    if (P.cvec)
+        for (int i = 0; i < nc; ++i) P.cvec[idx * P.K + i] = cs[i * npb];
 }
 
 // --------------------------------------------------------------------------

@@ -360,11 +360,12 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
 
 // Cost vectors (ComputeMultiViewCostVector_Frame, AdaptMIPMFrame.cu:181-225) of
 // hypotheses S.plane[0..nh) at (px, py), except those whose bit is set in
-// skip: S.cost[h * K + k] for k < nc.  A neighbour whose anchor leaves the
-// window gets 2 without evaluation.
+// skip: S.cost[h * K + k] for the neighbours k < nc whose bit is set in vmask
+// (the other entries are left as they are).  A neighbour whose anchor leaves
+// the window gets 2 without evaluation.
 template <bool BLUR, bool COUNT>
 __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const WarpBlock& S, const PixWin& pw,
-                                       int px, int py, int nh, int nc, int lane, uint64_t skip)
+                                       int px, int py, int nh, int nc, int lane, uint64_t skip, uint32_t vmask)
 {
     const int K = P.K;
     for (int h = lane; h < nh; h += 32) {
@@ -378,7 +379,7 @@ __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const W
         const int n = n0 + lane;
         bool need = false;
         const int hn = n / nc;
-        if (n < total && !((skip >> hn) & 1ull)) {
+        if (n < total && !((skip >> hn) & 1ull) && ((vmask >> (n - hn * nc)) & 1u)) {
             const int h = hn, k = n - h * nc;
             if (T.nb_ok[k]) {
                 const float2 a = geo_anchor(T.geo[k], px, py, S.dp[h].w);
@@ -408,13 +409,16 @@ __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const W
 }
 
 // ComputeWeightedCost_Frame (AdaptMIPMFrame.cu:284-317) of hypotheses [0, nh),
-// one lane per hypothesis; view weights packed 4 bits per view.
+// one lane per hypothesis; view weights packed 4 bits per view.  Only the
+// views in vmask are read: the weighted cost is exact whenever vmask holds
+// every view of non-zero weight, the lowest-cost index covers vmask's views.
 __device__ __forceinline__ void weigh_hyps(const WarpBlock& S, int K, int nh, int nc, uint64_t vw_lo, uint64_t vw_hi,
-                                           int lane)
+                                           int lane, uint32_t vmask)
 {
     for (int h = lane; h < nh; h += 32) {
         WeightedCost wc;
         for (int k = 0; k < nc; ++k) {
+            if (!((vmask >> k) & 1u)) continue;
             const float w = (float)((k < 16 ? vw_lo >> (k * 4) : vw_hi >> ((k - 16) * 4)) & 15ull);
             wc.add(k, S.cost[h * K + k], w);
         }
@@ -616,24 +620,41 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             build_table<BLUR>(T, P, pw, x, y, S.tab, lane);
 
             // ---- propagation candidates and the current plane --------------
+            // Row 0 holds the current plane, then one row per distinct candidate plane:
+            // a cost vector depends only on the pixel and the plane, so candidates whose
+            // planes are bit-identical (to each other or to the current plane) share a
+            // row.  The current plane's vector is the one stored when this pixel was last
+            // updated, when that store is valid; otherwise it is evaluated.
             Cands C;
             find_candidates(pc, x, y, W, H, C);
-            int slot_h[9];
-            int nh = 0;
-            for (int s = 0; s < 8; ++s)
-                if (C.flag[s] && C.src[s] < 0) {
-                    slot_h[s] = nh;
-                    if (lane == 0) S.plane[nh] = prev.plane[vbase + C.pos[s]];
-                    ++nh;
+            const float4 cur_plane = prev.plane[idx];
+            uint64_t slots = 0;                          // row of slot s in bits [4s, 4s + 4); slot 8 = row 0
+            int nh = 1;
+            if (lane == 0) {
+                S.plane[0] = cur_plane;
+                for (int s = 0; s < 8; ++s) {
+                    if (!C.flag[s] || C.src[s] >= 0) continue;
+                    const float4 q = prev.plane[vbase + C.pos[s]];
+                    int r = 0;
+                    for (; r < nh; ++r) {
+                        const float4 o = S.plane[r];
+                        if (__float_as_uint(o.x) == __float_as_uint(q.x) && __float_as_uint(o.y) == __float_as_uint(q.y) &&
+                            __float_as_uint(o.z) == __float_as_uint(q.z) && __float_as_uint(o.w) == __float_as_uint(q.w))
+                            break;
+                    }
+                    if (r == nh) S.plane[nh++] = q;
+                    slots |= (uint64_t)r << (4 * s);
                 }
-            slot_h[8] = nh;
-            if (lane == 0) S.plane[nh] = prev.plane[idx];
-            ++nh;
-            for (int s = 0; s < 8; ++s)
-                if (C.flag[s] && C.src[s] >= 0) slot_h[s] = slot_h[C.src[s]];
+                for (int s = 0; s < 8; ++s)
+                    if (C.flag[s] && C.src[s] >= 0) slots |= ((slots >> (4 * C.src[s])) & 15ull) << (4 * s);
+            }
+            slots = __shfl_sync(kFullMask, slots, 0);
+            nh = __shfl_sync(kFullMask, nh, 0);
+            if (P.cvec_ok && lane < nc) S.cost[lane] = P.cvec[idx * K + lane];
             __syncwarp();
-            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nh, nc, lane, 0ull);
-#define COSTA(s, k) S.cost[slot_h[s] * K + (k)]
+            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nh, nc, lane, P.cvec_ok ? 1ull : 0ull, ~0u);
+#define SLOT(s) ((int)((slots >> (4 * (s))) & 15ull))
+#define COSTA(s, k) S.cost[SLOT(s) * K + (k)]
 
             // ---- view-selection priors and sampling (AdaptMIPMFrame.cu:797-875)
             DrawStream g2;
@@ -703,15 +724,19 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             }
 #undef COSTA
             // weighted costs: current plane, then the candidates in slot order
-            weigh_hyps(S, K, nh, nc, vw_lo, vw_hi, lane);
-            float best_cost = S.wres[slot_h[8]];
-            int best_min = S.wmin[slot_h[8]];
-            float4 best_plane = prev.plane[idx];
+            weigh_hyps(S, K, nh, nc, vw_lo, vw_hi, lane, ~0u);
+            float best_cost = S.wres[0];
+            int best_min = S.wmin[0];
+            float4 best_plane = cur_plane;
+            int best_row = 0;
             for (int s = 0; s < 8; ++s) {
                 if (!C.flag[s]) continue;
-                const float c = S.wres[slot_h[s]];
-                if (c < best_cost) { best_cost = c; best_plane = prev.plane[vbase + C.pos[s]]; best_min = S.wmin[slot_h[s]]; }
+                const float c = S.wres[SLOT(s)];
+                if (c < best_cost) { best_cost = c; best_plane = S.plane[SLOT(s)]; best_min = S.wmin[SLOT(s)]; best_row = SLOT(s); }
             }
+#undef SLOT
+            // this lane's entry of the best vector so far (the rows are reused below)
+            float best_vec = lane < nc ? S.cost[best_row * K + lane] : 0.0f;
             __syncwarp();
 
             // ---- cross-view proposals (AdaptMIPMFrame.cu:907-936) and refinement
@@ -748,10 +773,10 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             if (lane == 0)
                 for (int i = 0; i < 5; ++i) S.plane[r0 + i] = cand[i];
             __syncwarp();
-            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull);
-            weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane);
+            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull, tsel);
+            weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
 
-            bool changed = false;
+            bool changed = false, partial = false;
             int hs = 0;                                  // speculative row of proposal n
             for (int n = 0; n < nsel; ++n) {
                 const int k = nth_set_bit(tsel, n);
@@ -774,13 +799,13 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                     __syncwarp();
                     if (lane == 0) S.plane[row] = proxy;
                     __syncwarp();
-                    eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull);
-                    weigh_hyps(S, K, row + 1, nc, vw_lo, vw_hi, lane);
+                    eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull, tsel);
+                    weigh_hyps(S, K, row + 1, nc, vw_lo, vw_hi, lane, tsel);
                     c = S.wres[row];
                     cmin = S.wmin[row];
                 }
                 if (spec_q >= 0) ++hs;
-                if (q >= 0 && c < best_cost) { best_cost = c; best_plane = proxy; best_min = cmin; changed = true; }
+                if (q >= 0 && c < best_cost) { best_cost = c; best_plane = proxy; best_min = cmin; changed = true; partial = true; }
             }
             if (changed) {
                 // candidates 2-4 follow the best plane: rebuild and evaluate them again
@@ -791,14 +816,31 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                     for (int i = 2; i < 5; ++i) S.plane[r0 + i] = cand[i];
                 __syncwarp();
                 const uint64_t redo = (7ull << (r0 + 2)) & ~(skip3 ? (1ull << (r0 + 3)) : 0ull);
-                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo);
-                weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane);
+                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo, tsel);
+                weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
             }
             for (int i = 0; i < 5; ++i) {
                 if (i == 3 && skip3) continue;
                 const float c = S.wres[r0 + i];
-                if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = S.wmin[r0 + i]; }
+                if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = S.wmin[r0 + i]; partial = true; }
             }
+            if (partial) {
+                // proposals and refinement candidates were evaluated on the selected views
+                // only, which fixes their weighted cost; the winner's lowest-cost view runs
+                // over every view, and its vector is stored, so the whole vector is
+                // evaluated again (one NCC per lane, a single pass over the taps)
+                __syncwarp();
+                if (lane == 0) S.plane[0] = best_plane;
+                __syncwarp();
+                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
+                weigh_hyps(S, K, 1, nc, vw_lo, vw_hi, lane, ~0u);
+                best_min = S.wmin[0];
+                best_vec = lane < nc ? S.cost[lane] : 0.0f;
+                best_row = -1;
+            }
+            // the stored vector of the new current plane (unchanged when the current
+            // plane stays and its stored vector was used)
+            if (P.cvec && lane < nc && !(best_row == 0 && P.cvec_ok)) P.cvec[idx * K + lane] = best_vec;
             if (lane == 0) {
                 float4 best_disp = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (best_min >= 0)

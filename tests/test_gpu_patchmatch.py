@@ -131,6 +131,48 @@ def test_init_and_sweeps_bitexact(pfd, oracle, ctx, pitch, K, patch):
     ctx.frame_free(fid)
 
 
+def test_sweeps_after_state_changes_bitexact(pfd, oracle, ctx):
+    """The sweep reuses the stored cost vector of each pixel's current plane.
+    Every way the state can change outside the sweeps must drop that store:
+    the disparity filter (rejected pixels get new planes), an uploaded state,
+    and a sweep whose NCC parameters differ from the ones that made the store."""
+    pitch, K = 23.2, 12
+    w = _workload(pfd, 260, 200, pitch, K=K, seed=8)
+    fid = _upload(ctx, w)
+    P = pfd.PmParams(base=pitch, patch_size=15, max_iterations=2)
+    orc = oracle.Oracle(w.gray, w.centers, w.nb_ids, w.nb_counts)
+    seed = 5
+    ctx.pm_init(fid, P, seed)
+    st = orc.init(P, seed)
+    ctx.pm_sweep(fid, P, seed, 0, 0)
+    st = orc.sweep(P, seed, 0, 0, st)
+    _state_equal(ctx.download(fid), st, "sweep 0.0")
+    # the filter rewrites rejected pixels in place
+    reason, _ = ctx.filter(fid, pfd.FilterCfg(), pitch)
+    assert np.count_nonzero(reason) > 100
+    plane, cost, disp, sel = ctx.download(fid)
+    st = dict(plane=plane.copy(), cost=cost.copy(), disp=disp.copy(), sel=sel.copy())
+    for ph in (1, 0):
+        ctx.pm_sweep(fid, P, seed, 1, ph)
+        st = orc.sweep(P, seed, 1, ph, st)
+        _state_equal(ctx.download(fid), st, f"sweep 1.{ph} after the filter")
+    # an uploaded state: planes moved between pixels
+    rs = np.random.RandomState(1)
+    perm = rs.permutation(st["plane"].shape[0])
+    up = dict(plane=st["plane"][perm].copy(), cost=st["cost"].copy(), disp=st["disp"].copy(), sel=st["sel"].copy())
+    ctx.state_upload(fid, up["plane"], up["cost"], up["disp"], up["sel"])
+    ctx.pm_sweep(fid, P, seed, 2, 1)
+    st = orc.sweep(P, seed, 2, 1, up)
+    _state_equal(ctx.download(fid), st, "sweep after an uploaded state")
+    # other NCC parameters than the stored vectors were made with
+    P2 = pfd.PmParams(base=pitch, patch_size=11, max_iterations=2, sigma_color=10.0)
+    for ph in (0, 1):
+        ctx.pm_sweep(fid, P2, seed, 3, ph)
+        st = orc.sweep(P2, seed, 3, ph, st)
+        _state_equal(ctx.download(fid), st, f"sweep 3.{ph} with other parameters")
+    ctx.frame_free(fid)
+
+
 def test_patchmatch_virtual_depth_parity(pfd, oracle, ctx):
     """Full pfd_patchmatch (3 iterations): >= 99.5% of valid pixels within 0.01
     virtual depth of the oracle (virtual depth = pitch / disparity)."""
