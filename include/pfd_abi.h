@@ -277,6 +277,43 @@ pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg,
 pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_slices, int out_w, int out_h,
                        float* out);
 
+/* ---- virtual-depth fusion ------------------------------------------------
+ * LFRefocus::FuseVirtualDepth_BackProject (FocalStack/LFRefocus.cpp:1553-1794):
+ * every reference micro-image pixel with disparity >= min_ref_disp becomes a
+ * virtual point (ComputeVirtual3D, :2100-2117, at virtual depth mla_base / d,
+ * ComputeVirtualDepth :2087-2098); it is back-projected into each micro-image of
+ * its list (BackProject2MI, :2119-2125), and a list entry is consistent when
+ * that pixel, unmasked and with a disparity > 0, projects back within
+ * max_reproj_px at a virtual depth within max_rel_vd.  With min_consistent or
+ * more consistent entries the point, normal and colour are averaged, written
+ * to the raw-resolution maps at the rounded point position, and the entries'
+ * pixels are masked for everything after: micro-images in frame order, pixels
+ * row by row, exactly as the reference, whose result depends on that order.
+ * The reference's literals are min_ref_disp 1, max_reproj_px 1, max_rel_vd
+ * 0.05, min_consistent 2; mla_base = LightFieldParams::baseline * g_bl0 /
+ * (g_bl0 + g_B). */
+typedef struct {
+    float mla_base;
+    float min_ref_disp;
+    float max_reproj_px;
+    float max_rel_vd;
+    int   min_consistent;
+} pfd_fuse_params;
+/* Reads the frame's current state (normal: plane.xyz, disparity: plane.w).
+ *   lists        [n_views][max_list] each view's m_NeighsSortVecForMatch as view
+ *                ids, -1 for a key with no result (skipped); max_list <= 128
+ *   list_counts  [n_views]
+ *   is_ref       [n_views] 1 for the micro-images fused as references (not garbage)
+ *   bgr          [n_views][mi_h][mi_w][3] colour micro-images (MLA_Problem::
+ *                m_Image_rgb), or NULL to use the gray ones in all channels
+ * Outputs (host, any may be NULL), W x H of the frame's raw size:
+ *   vd_map float (m_VirtualDepthMap), conf u8 (VD_Confidence), aif u8 x 3 BGR
+ *   (m_AIF_Color); points [n][9] (point, normal, colour) in the reference's order,
+ *   sized by a first call with points NULL and n_points set. */
+pfd_status pfd_fuse_virtual_depth(pfd_ctx* ctx, int frame_id, const pfd_fuse_params* params, const int* lists,
+                                  const int* list_counts, int max_list, const uint8_t* is_ref, const uint8_t* bgr,
+                                  float* vd_map, uint8_t* conf, uint8_t* aif, float* points, long long* n_points);
+
 /* ---- virtual depth to real depth (FP64) -----------------------------------
  * The behavioural model z = (v c1 + c2) / (1 - v c0) of FocalStack/
  * VirtualToRealDepthFunc.cpp and LFRefocus.cpp, in double precision on the

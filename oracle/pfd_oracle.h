@@ -194,6 +194,29 @@ int orc_refocus(const orc_frame* f, int raw_w, int raw_h, const float* slice_vd,
 long long orc_refocus_samples(const orc_frame* f, int raw_w, int raw_h, const float* slice_vd, int n_slices,
                               int out_w, int out_h);
 
+/* Virtual-depth fusion and all-in-focus splat, LFRefocus::FuseVirtualDepth_BackProject
+ * (FocalStack/LFRefocus.cpp:1553-1794).  The thresholds are the reference's
+ * literals; mla_base = LightFieldParams::baseline * g_bl0 / (g_bl0 + g_B)
+ * (ComputeVirtualDepth, :2087-2098). */
+typedef struct {
+    float mla_base;
+    float min_ref_disp;          /* 1.0: reference pixels with a smaller disparity are skipped (:1641) */
+    float max_reproj_px;         /* 1.0 (:1734) */
+    float max_rel_vd;            /* 0.05 (:1734) */
+    int   min_consistent;        /* 2 (:1752) */
+} orc_fuse_params;
+/* plane [V*ppv][4] (normal, disparity: ph_cuda.xyz and d_cuda), bgr [V][mi_h][mi_w][3]
+ * (m_Image_rgb) or NULL for the gray images in all three channels; lists [V][max_list]
+ * the views' m_NeighsSortVecForMatch as view ids (-1: a key with no result);
+ * is_ref [V]: 1 for the micro-images fused as references (not garbage).
+ * Outputs (raw_h x raw_w, zeroed first): vd_map float, conf u8, aif u8 x 3 (BGR);
+ * points (may be NULL) [n][9] point, normal, colour in the reference's push order.
+ * Returns the number of points, or -1. */
+long long orc_fuse_virtual_depth(const orc_frame* f, const float* plane, const uint8_t* bgr, const int* lists,
+                                 const int* list_counts, int max_list, const uint8_t* is_ref,
+                                 const orc_fuse_params* p, int raw_w, int raw_h, float* vd_map, uint8_t* conf,
+                                 uint8_t* aif, float* points);
+
 /* Virtual-to-real depth (FocalStack/LFRefocus.cpp:2515-2593,
  * FocalStack/VirtualToRealDepthFunc.cpp:3390-3450), FP64. */
 float orc_vd_to_rd(float v_depth, const double c[3]);

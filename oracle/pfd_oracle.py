@@ -59,6 +59,11 @@ class OrcCycleStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_longlong if n in _INT_STATS else ctypes.c_double) for n in CYCLE_STAT_FIELDS]
 
 
+class OrcFuseParams(ctypes.Structure):
+    _fields_ = [("mla_base", _F), ("min_ref_disp", _F), ("max_reproj_px", _F), ("max_rel_vd", _F),
+                ("min_consistent", _I)]
+
+
 class OrcState(ctypes.Structure):
     _fields_ = [("plane", _P), ("cost", _P), ("disp", _P), ("sel", _P)]
 
@@ -114,6 +119,9 @@ def lib() -> ctypes.CDLL:
         L.orc_behavioral_fit.argtypes = [_P, _P, ctypes.c_long, _P]
         L.orc_refocus_samples.argtypes = [FP, _I, _I, _P, _I, _I, _I]
         L.orc_refocus_samples.restype = ctypes.c_longlong
+        L.orc_fuse_virtual_depth.argtypes = [FP, _P, _P, _P, _P, _I, _P, ctypes.POINTER(OrcFuseParams), _I, _I,
+                                             _P, _P, _P, _P]
+        L.orc_fuse_virtual_depth.restype = ctypes.c_longlong
         _lib = L
     return _lib
 
@@ -279,6 +287,25 @@ def refocus(orc: "Oracle", raw_w: int, raw_h: int, slice_vd, out_w: int, out_h: 
 def refocus_samples(orc: "Oracle", raw_w: int, raw_h: int, slice_vd, out_w: int, out_h: int) -> int:
     vd = np.ascontiguousarray(slice_vd, np.float32)
     return int(lib().orc_refocus_samples(ctypes.byref(orc.f), raw_w, raw_h, _p(vd), vd.shape[0], out_w, out_h))
+
+
+def fuse_virtual_depth(orc: "Oracle", plane, lists, list_counts, is_ref, raw_w: int, raw_h: int, mla_base: float,
+                       bgr=None, min_ref_disp=1.0, max_reproj_px=1.0, max_rel_vd=0.05, min_consistent=2):
+    """LFRefocus::FuseVirtualDepth_BackProject: (vd_map, conf, aif [h][w][3], points [n][9])."""
+    pl = np.ascontiguousarray(plane, np.float32).reshape(-1, 4)
+    ls = np.ascontiguousarray(lists, np.int32)
+    lc = np.ascontiguousarray(list_counts, np.int32)
+    ir = np.ascontiguousarray(is_ref, np.uint8)
+    b = None if bgr is None else np.ascontiguousarray(bgr, np.uint8)
+    vd = np.zeros((raw_h, raw_w), np.float32)
+    cf = np.zeros((raw_h, raw_w), np.uint8)
+    aif = np.zeros((raw_h, raw_w, 3), np.uint8)
+    pts = np.zeros((pl.shape[0], 9), np.float32)
+    prm = OrcFuseParams(mla_base, min_ref_disp, max_reproj_px, max_rel_vd, min_consistent)
+    n = lib().orc_fuse_virtual_depth(ctypes.byref(orc.f), _p(pl), _p(b), _p(ls), _p(lc), ls.shape[1], _p(ir),
+                                     ctypes.byref(prm), raw_w, raw_h, _p(vd), _p(cf), _p(aif), _p(pts))
+    assert n >= 0
+    return vd, cf, aif, pts[:n]
 
 
 def vd_to_rd_points(vd, c):

@@ -144,6 +144,11 @@ class CycleStatsC(ctypes.Structure):
     _fields_ = [(n, ctypes.c_longlong if n in _CYCLE_INT else ctypes.c_double) for n in CYCLE_STATS]
 
 
+class FuseParamsC(ctypes.Structure):
+    _fields_ = [("mla_base", ctypes.c_float), ("min_ref_disp", ctypes.c_float), ("max_reproj_px", ctypes.c_float),
+                ("max_rel_vd", ctypes.c_float), ("min_consistent", ctypes.c_int)]
+
+
 FILTER_STATS = ("total", "valid_in", "kept", "removed", "by_cost", "by_no_support", "by_cycle", "by_spike")
 
 _lib = None
@@ -195,6 +200,8 @@ def lib() -> ctypes.CDLL:
             "pfd_vd_to_rd_segments": [_P, _P, ctypes.c_size_t, _P, _I, _P],
             "pfd_fit_behavioral_model": [_P, _P, _P, ctypes.c_size_t, _P],
             "pfd_cycle_check": [_P, _I, ctypes.POINTER(CycleCfgC), _F, ctypes.POINTER(CycleStatsC), _P, _P, _P],
+            "pfd_fuse_virtual_depth": [_P, _I, ctypes.POINTER(FuseParamsC), _P, _P, _I, _P, _P, _P, _P, _P, _P,
+                                       ctypes.POINTER(ctypes.c_longlong)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -456,6 +463,34 @@ class Context:
         self._check(self._L.pfd_reprojection_error(self._h, fid, ctypes.byref(c), float(baseline_unit), _ptr(err)),
                     "pfd_reprojection_error")
         return err
+
+    def fuse_virtual_depth(self, fid: int, lists, list_counts, is_ref, mla_base: float, bgr=None,
+                           points: bool = True, download: bool = True, min_ref_disp: float = 1.0,
+                           max_reproj_px: float = 1.0, max_rel_vd: float = 0.05, min_consistent: int = 2):
+        """LFRefocus::FuseVirtualDepth_BackProject on the frame's state.  Returns
+        (vd_map, conf, aif [H][W][3], points [n][9] or None); with download=False
+        nothing is copied back and None is returned."""
+        f = self._frames[fid]
+        ls = np.ascontiguousarray(lists, np.int32)
+        lc = np.ascontiguousarray(list_counts, np.int32)
+        ir = np.ascontiguousarray(is_ref, np.uint8)
+        b = None if bgr is None else np.ascontiguousarray(bgr, np.uint8)
+        prm = FuseParamsC(mla_base, min_ref_disp, max_reproj_px, max_rel_vd, min_consistent)
+        if not download:
+            self._check(self._L.pfd_fuse_virtual_depth(self._h, fid, ctypes.byref(prm), _ptr(ls), _ptr(lc),
+                                                       ls.shape[1], _ptr(ir), _ptr(b), None, None, None, None, None),
+                        "pfd_fuse_virtual_depth")
+            return None
+        H, W = f["H"], f["W"]
+        vd = np.empty((H, W), np.float32)
+        cf = np.empty((H, W), np.uint8)
+        aif = np.empty((H, W, 3), np.uint8)
+        n = ctypes.c_longlong(0)
+        pts = np.empty((f["V"] * f["mi_w"] * f["mi_h"], 9), np.float32) if points else None
+        self._check(self._L.pfd_fuse_virtual_depth(self._h, fid, ctypes.byref(prm), _ptr(ls), _ptr(lc), ls.shape[1],
+                                                   _ptr(ir), _ptr(b), _ptr(vd), _ptr(cf), _ptr(aif), _ptr(pts),
+                                                   ctypes.byref(n)), "pfd_fuse_virtual_depth")
+        return vd, cf, aif, (pts[:n.value] if points else None)
 
     def download(self, fid: int):
         f = self._frames[fid]

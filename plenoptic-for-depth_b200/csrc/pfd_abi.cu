@@ -19,6 +19,7 @@
 #include "check_kernels.h"
 #include "refocus_kernels.h"
 #include "vdrd_kernels.h"
+#include "fuse_kernels.h"
 
 namespace {
 
@@ -1142,6 +1143,147 @@ pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_
     ctx->launches += 1;
     if (out) CU(cudaMemcpyAsync(out, f->d_stack, need, cudaMemcpyDeviceToHost, ctx->stream));
     return out ? check_device_error(ctx) : PFD_OK;
+}
+
+// Wavefront steps of the fusion: a reference micro-image runs one step after
+// the last step that touched any micro-image it touches (itself and its list
+// entries), so two micro-images that share one keep the reference's order and
+// micro-images of one step touch disjoint sets.
+static void fuse_schedule(int V, const int* lists, const int* counts, int max_list, const uint8_t* is_ref,
+                          std::vector<int>& order, std::vector<int>& step_start)
+{
+    std::vector<int> last(V, 0), step(V, 0);
+    int nsteps = 0;
+    for (int v = 0; v < V; ++v) {
+        if (!is_ref[v]) continue;
+        const int nl = std::min(counts[v], max_list);
+        int s = last[v];
+        for (int j = 0; j < nl; ++j) {
+            const int u = lists[(size_t)v * max_list + j];
+            if (u >= 0) s = std::max(s, last[u]);
+        }
+        step[v] = ++s;
+        last[v] = s;
+        for (int j = 0; j < nl; ++j) {
+            const int u = lists[(size_t)v * max_list + j];
+            if (u >= 0) last[u] = s;
+        }
+        nsteps = std::max(nsteps, s);
+    }
+    std::vector<int> cnt((size_t)nsteps + 2, 0);
+    for (int v = 0; v < V; ++v)
+        if (is_ref[v]) cnt[(size_t)step[v]]++;
+    step_start.assign((size_t)nsteps + 1, 0);
+    for (int s = 1; s <= nsteps; ++s) step_start[s] = step_start[s - 1] + cnt[(size_t)s];
+    order.assign((size_t)step_start[nsteps], 0);
+    std::vector<int> fill(step_start.begin(), step_start.end());
+    for (int v = 0; v < V; ++v)                       // ascending view order inside a step
+        if (is_ref[v]) order[(size_t)fill[(size_t)step[v] - 1]++] = v;
+}
+
+pfd_status pfd_fuse_virtual_depth(pfd_ctx* ctx, int frame_id, const pfd_fuse_params* p, const int* lists,
+                                  const int* list_counts, int max_list, const uint8_t* is_ref, const uint8_t* bgr,
+                                  float* vd_map, uint8_t* conf, uint8_t* aif, float* points, long long* n_points)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!p || !lists || !list_counts || !is_ref) return fail(ctx, PFD_EINVAL, "fuse: NULL argument");
+    if (max_list < 1 || max_list > pfd::kFuseMaxList)
+        return fail(ctx, PFD_EINVAL, "fuse: max_list %d outside [1, %d]", max_list, pfd::kFuseMaxList);
+    if (!std::isfinite(p->mla_base) || !std::isfinite(p->min_ref_disp) || !std::isfinite(p->max_reproj_px) ||
+        !std::isfinite(p->max_rel_vd))
+        return fail(ctx, PFD_EINVAL, "fuse: parameters must be finite");
+    if (f->mi_w != f->mi_h) return fail(ctx, PFD_EINVAL, "fuse: square micro-images only (%dx%d)", f->mi_w, f->mi_h);
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "fuse before PatchMatch");
+    if (!bgr && !f->has_mi) return fail(ctx, PFD_ESTATE, "frame has no micro-images yet");
+    const int V = f->V;
+    for (int v = 0; v < V; ++v) {
+        if (list_counts[v] < 0 || list_counts[v] > max_list)
+            return fail(ctx, PFD_EINVAL, "fuse: view %d list count %d outside [0, %d]", v, list_counts[v], max_list);
+        for (int j = 0; j < list_counts[v]; ++j) {
+            const int u = lists[(size_t)v * max_list + j];
+            if (u < -1 || u >= V) return fail(ctx, PFD_EINVAL, "fuse: view %d list entry %d is %d", v, j, u);
+        }
+    }
+    DeviceGuard g(ctx->device);
+    std::vector<int> order, step_start;
+    fuse_schedule(V, lists, list_counts, max_list, is_ref, order, step_start);
+    const size_t ppv = (size_t)f->mi_w * f->mi_h, px = (size_t)V * ppv, npix = (size_t)f->W * f->H;
+    const size_t nb = (px + pfd::kFuseScanBlock - 1) / pfd::kFuseScanBlock;
+    cudaStream_t s = ctx->stream;
+    // scratch of this call, from the stream-ordered pool
+    struct Scratch {
+        cudaStream_t s;
+        std::vector<void*> ptrs;
+        ~Scratch() { for (void* q : ptrs) cudaFreeAsync(q, s); }
+        cudaError_t get(void** q, size_t bytes) {
+            cudaError_t e = cudaMallocAsync(q, bytes > 0 ? bytes : 1, s);
+            if (e == cudaSuccess) ptrs.push_back(*q);
+            return e;
+        }
+    } S{ s, {} };
+    int *d_lists = nullptr, *d_counts = nullptr, *d_order = nullptr;
+    uint8_t *d_bgr = nullptr, *d_mask = nullptr, *d_conf = nullptr, *d_aif = nullptr;
+    unsigned int *d_winner = nullptr, *d_has = nullptr, *d_bcount = nullptr;
+    float *d_rec = nullptr, *d_vd = nullptr, *d_points = nullptr;
+    CU(S.get((void**)&d_lists, sizeof(int) * (size_t)V * max_list));
+    CU(S.get((void**)&d_counts, sizeof(int) * (size_t)V));
+    CU(S.get((void**)&d_order, sizeof(int) * std::max<size_t>(order.size(), 1)));
+    if (bgr) CU(S.get((void**)&d_bgr, px * 3));
+    CU(S.get((void**)&d_mask, px));
+    CU(S.get((void**)&d_winner, sizeof(unsigned int) * npix));
+    CU(S.get((void**)&d_has, sizeof(unsigned int) * px));
+    CU(S.get((void**)&d_rec, sizeof(float) * 10 * px));
+    CU(S.get((void**)&d_vd, sizeof(float) * npix));
+    CU(S.get((void**)&d_conf, npix));
+    CU(S.get((void**)&d_aif, npix * 3));
+    CU(cudaMemcpyAsync(d_lists, lists, sizeof(int) * (size_t)V * max_list, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(d_counts, list_counts, sizeof(int) * (size_t)V, cudaMemcpyHostToDevice, s));
+    if (!order.empty())
+        CU(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, s));
+    if (bgr) CU(cudaMemcpyAsync(d_bgr, bgr, px * 3, cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(d_mask, 0, px, s));
+    CU(cudaMemsetAsync(d_winner, 0, sizeof(unsigned int) * npix, s));
+    CU(cudaMemsetAsync(d_has, 0, sizeof(unsigned int) * px, s));
+    pfd::FuseFrame F;
+    F.V = V; F.m = f->mi_w; F.ppv = (int)ppv; F.tile_stride = f->tile_stride;
+    F.gray = f->d_gray; F.bgr = d_bgr; F.centers = f->d_centers; F.plane = f->s[f->cur].plane;
+    F.lists = d_lists; F.list_counts = d_counts; F.max_list = max_list;
+    F.mla_base = p->mla_base; F.min_ref_disp = p->min_ref_disp; F.max_reproj_px = p->max_reproj_px;
+    F.max_rel_vd = p->max_rel_vd; F.min_consistent = p->min_consistent;
+    F.raw_w = f->W; F.raw_h = f->H;
+    F.mask = d_mask; F.winner = d_winner; F.rec = d_rec; F.has_rec = d_has;
+    for (size_t k = 0; k + 1 < step_start.size(); ++k) {
+        const int a = step_start[k], b = step_start[k + 1];
+        CU(pfd::launch_fuse_step(F, d_order + a, b - a, s));
+        ctx->launches += 1;
+    }
+    CU(pfd::launch_fuse_maps(F, d_vd, d_conf, d_aif, s));
+    ctx->launches += 1;
+    if (vd_map) CU(cudaMemcpyAsync(vd_map, d_vd, sizeof(float) * npix, cudaMemcpyDeviceToHost, s));
+    if (conf) CU(cudaMemcpyAsync(conf, d_conf, npix, cudaMemcpyDeviceToHost, s));
+    if (aif) CU(cudaMemcpyAsync(aif, d_aif, npix * 3, cudaMemcpyDeviceToHost, s));
+    if (points || n_points) {
+        CU(S.get((void**)&d_bcount, sizeof(unsigned int) * nb));
+        CU(pfd::launch_fuse_count(F, d_bcount, s));
+        ctx->launches += 1;
+        std::vector<unsigned int> bc(nb);
+        CU(cudaMemcpyAsync(bc.data(), d_bcount, sizeof(unsigned int) * nb, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        unsigned long long total = 0;
+        for (size_t i = 0; i < nb; ++i) { const unsigned int c = bc[i]; bc[i] = (unsigned int)total; total += c; }
+        if (n_points) *n_points = (long long)total;
+        if (points && total) {
+            CU(cudaMemcpyAsync(d_bcount, bc.data(), sizeof(unsigned int) * nb, cudaMemcpyHostToDevice, s));
+            CU(S.get((void**)&d_points, sizeof(float) * 9 * total));
+            CU(pfd::launch_fuse_compact(F, d_bcount, d_points, s));
+            ctx->launches += 1;
+            CU(cudaMemcpyAsync(points, d_points, sizeof(float) * 9 * total, cudaMemcpyDeviceToHost, s));
+        }
+    }
+    if (vd_map || conf || aif || points || n_points) return check_device_error(ctx);
+    return PFD_OK;
 }
 
 pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane, float* cost, float* disp, uint32_t* sel)
