@@ -277,6 +277,39 @@ pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg,
 pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_slices, int out_w, int out_h,
                        float* out);
 
+/* ---- micro-lens centres -------------------------------------------------
+ * DepthSolver::ComputeMLACentersFromWhiteImage (DepthSolver.cpp:710-870) on the
+ * device: the reference's Otsu threshold (:486-546, which histograms the first W
+ * bytes of every row of the 3-channel image), BGR2GRAY and the binary threshold,
+ * the external contours of the 8-connected bright blobs with their polygon
+ * moments and areas (as findContours(RETR_EXTERNAL) + moments + contourArea
+ * give them), then the reference's position filter, rows by running mean y,
+ * columns by x and the small-area flag (area < 0.8 x the mean over all contours).
+ * One entry per MLA_Info map key, in key order (row, then column). */
+typedef struct {
+    int   col, row;          /* the key (QuadTreeTileKey tile x, tile y) */
+    float cx, cy;            /* MLA_Info::GetCenter */
+    float area;              /* MLA_Info::GetArea (contour area) */
+    int   abandon;           /* MLA_Info::IsAbandonByArea */
+} pfd_mla_lens;
+/* white_bgr: host 3-channel 8-bit image, W x H, rows step bytes apart (a gray
+ * image repeated in three channels for a one-channel white image).  baseline,
+ * mla_u_size, mla_v_size: LightFieldParams (lens pitch, lenses per row and per
+ * column).  n_out receives the entry count; out (room for max_out entries) the
+ * entries, or with out NULL only the count.  threshold (may be NULL) receives
+ * the Otsu threshold. */
+pfd_status pfd_mla_centers(pfd_ctx* ctx, const uint8_t* white_bgr, int W, int H, int step, float baseline,
+                           int mla_u_size, int mla_v_size, pfd_mla_lens* out, int max_out, int* n_out,
+                           int* threshold);
+
+/* Least-squares hexagonal lattice through detected centres (FP64, normal
+ * equations summed on the device): centre(col, row) = origin + (col + (row & 1)
+ * / 2) u + row (sqrt(3) / 2) u_perp, u = pitch (cos angle, sin angle).  No
+ * counterpart in the reference, which keeps the detected centres as they are;
+ * it measures them.  fit: origin x, origin y, pitch, angle (radians), RMS
+ * residual (pixels), lenses used.  skip_abandoned: leave out flagged lenses. */
+pfd_status pfd_mla_lattice_fit(pfd_ctx* ctx, const pfd_mla_lens* lenses, int n, int skip_abandoned, double fit[6]);
+
 /* ---- virtual-depth fusion ------------------------------------------------
  * LFRefocus::FuseVirtualDepth_BackProject (FocalStack/LFRefocus.cpp:1553-1794):
  * every reference micro-image pixel with disparity >= min_ref_disp becomes a

@@ -217,6 +217,19 @@ long long orc_fuse_virtual_depth(const orc_frame* f, const float* plane, const u
                                  const orc_fuse_params* p, int raw_w, int raw_h, float* vd_map, uint8_t* conf,
                                  uint8_t* aif, float* points);
 
+/* Micro-lens centres from a white image (DepthSolver::ComputeMLACentersFromWhiteImage,
+ * DepthSolver.cpp:710-870; Otsu :486-546).  bgr: 3-channel 8-bit image, row stride
+ * step bytes.  orc_mla_otsu: the reference's threshold (histogram of the first W
+ * bytes of each row).  orc_mla_contours: centroid and area of every external
+ * contour of the thresholded gray image, in OpenCV's order.  orc_mla_centers: the
+ * map entries in key order (row, column). */
+int orc_mla_otsu(const uint8_t* bgr, int W, int H, int step);
+int orc_mla_contours(const uint8_t* bgr, int W, int H, int step, int threshold, float* cx, float* cy, double* area,
+                     int max_out);
+int orc_mla_centers(const uint8_t* bgr, int W, int H, int step, float baseline, int mla_u_size, int mla_v_size,
+                    int* out_col, int* out_row, float* out_cx, float* out_cy, float* out_area, int* out_abandon,
+                    int max_out, int* threshold_out);
+
 /* Virtual-to-real depth (FocalStack/LFRefocus.cpp:2515-2593,
  * FocalStack/VirtualToRealDepthFunc.cpp:3390-3450), FP64. */
 float orc_vd_to_rd(float v_depth, const double c[3]);

@@ -122,6 +122,9 @@ def lib() -> ctypes.CDLL:
         L.orc_fuse_virtual_depth.argtypes = [FP, _P, _P, _P, _P, _I, _P, ctypes.POINTER(OrcFuseParams), _I, _I,
                                              _P, _P, _P, _P]
         L.orc_fuse_virtual_depth.restype = ctypes.c_longlong
+        L.orc_mla_otsu.argtypes = [_P, _I, _I, _I]
+        L.orc_mla_contours.argtypes = [_P, _I, _I, _I, _I, _P, _P, _P, _I]
+        L.orc_mla_centers.argtypes = [_P, _I, _I, _I, _F, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P]
         _lib = L
     return _lib
 
@@ -306,6 +309,47 @@ def fuse_virtual_depth(orc: "Oracle", plane, lists, list_counts, is_ref, raw_w: 
                                      ctypes.byref(prm), raw_w, raw_h, _p(vd), _p(cf), _p(aif), _p(pts))
     assert n >= 0
     return vd, cf, aif, pts[:n]
+
+
+def _bgr(img):
+    img = np.ascontiguousarray(img, np.uint8)
+    if img.ndim == 2:
+        img = np.ascontiguousarray(np.repeat(img[:, :, None], 3, axis=2))
+    return img
+
+
+def mla_otsu(img) -> int:
+    b = _bgr(img)
+    return int(lib().orc_mla_otsu(_p(b), b.shape[1], b.shape[0], b.strides[0]))
+
+
+def mla_contours(img, threshold: int):
+    """(cx, cy, area) of the external contours, in OpenCV's order."""
+    b = _bgr(img)
+    cap = b.shape[0] * b.shape[1] // 2 + 1
+    cx = np.zeros(cap, np.float32)
+    cy = np.zeros(cap, np.float32)
+    ar = np.zeros(cap, np.float64)
+    n = lib().orc_mla_contours(_p(b), b.shape[1], b.shape[0], b.strides[0], threshold, _p(cx), _p(cy), _p(ar), cap)
+    assert n >= 0
+    return cx[:n], cy[:n], ar[:n]
+
+
+def mla_centers(img, baseline: float, mla_u_size: int, mla_v_size: int):
+    """Map entries in key order: dict of col, row, cx, cy, area, abandon; and the threshold."""
+    b = _bgr(img)
+    cap = b.shape[0] * b.shape[1] // 2 + 1
+    col = np.zeros(cap, np.int32)
+    row = np.zeros(cap, np.int32)
+    cx = np.zeros(cap, np.float32)
+    cy = np.zeros(cap, np.float32)
+    ar = np.zeros(cap, np.float32)
+    ab = np.zeros(cap, np.int32)
+    t = ctypes.c_int(0)
+    n = lib().orc_mla_centers(_p(b), b.shape[1], b.shape[0], b.strides[0], baseline, mla_u_size, mla_v_size, _p(col),
+                              _p(row), _p(cx), _p(cy), _p(ar), _p(ab), cap, ctypes.byref(t))
+    assert n >= 0
+    return dict(col=col[:n], row=row[:n], cx=cx[:n], cy=cy[:n], area=ar[:n], abandon=ab[:n]), t.value
 
 
 def vd_to_rd_points(vd, c):

@@ -144,6 +144,11 @@ class CycleStatsC(ctypes.Structure):
     _fields_ = [(n, ctypes.c_longlong if n in _CYCLE_INT else ctypes.c_double) for n in CYCLE_STATS]
 
 
+class MlaLensC(ctypes.Structure):
+    _fields_ = [("col", ctypes.c_int), ("row", ctypes.c_int), ("cx", ctypes.c_float), ("cy", ctypes.c_float),
+                ("area", ctypes.c_float), ("abandon", ctypes.c_int)]
+
+
 class FuseParamsC(ctypes.Structure):
     _fields_ = [("mla_base", ctypes.c_float), ("min_ref_disp", ctypes.c_float), ("max_reproj_px", ctypes.c_float),
                 ("max_rel_vd", ctypes.c_float), ("min_consistent", ctypes.c_int)]
@@ -200,6 +205,8 @@ def lib() -> ctypes.CDLL:
             "pfd_vd_to_rd_segments": [_P, _P, ctypes.c_size_t, _P, _I, _P],
             "pfd_fit_behavioral_model": [_P, _P, _P, ctypes.c_size_t, _P],
             "pfd_cycle_check": [_P, _I, ctypes.POINTER(CycleCfgC), _F, ctypes.POINTER(CycleStatsC), _P, _P, _P],
+            "pfd_mla_lattice_fit": [_P, _P, _I, _I, _P],
+            "pfd_mla_centers": [_P, _P, _I, _I, _I, _F, _I, _I, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
             "pfd_fuse_virtual_depth": [_P, _I, ctypes.POINTER(FuseParamsC), _P, _P, _I, _P, _P, _P, _P, _P, _P,
                                        ctypes.POINTER(ctypes.c_longlong)],
         }
@@ -463,6 +470,37 @@ class Context:
         self._check(self._L.pfd_reprojection_error(self._h, fid, ctypes.byref(c), float(baseline_unit), _ptr(err)),
                     "pfd_reprojection_error")
         return err
+
+    def mla_centers(self, white, baseline: float, mla_u_size: int, mla_v_size: int):
+        """DepthSolver::ComputeMLACentersFromWhiteImage on a white image (H x W x 3
+        BGR, or H x W gray).  Returns (dict of col, row, cx, cy, area, abandon
+        arrays in key order, Otsu threshold)."""
+        img = np.ascontiguousarray(white, np.uint8)
+        if img.ndim == 2:
+            img = np.ascontiguousarray(np.repeat(img[:, :, None], 3, axis=2))
+        H, W = img.shape[:2]
+        n = _I(0)
+        t = _I(0)
+        self._check(self._L.pfd_mla_centers(self._h, _ptr(img), W, H, img.strides[0], float(baseline), mla_u_size,
+                                            mla_v_size, None, 0, ctypes.byref(n), ctypes.byref(t)), "pfd_mla_centers")
+        out = (MlaLensC * max(1, n.value))()
+        self._check(self._L.pfd_mla_centers(self._h, _ptr(img), W, H, img.strides[0], float(baseline), mla_u_size,
+                                            mla_v_size, ctypes.cast(out, _P), n.value, ctypes.byref(n),
+                                            ctypes.byref(t)), "pfd_mla_centers")
+        a = np.ctypeslib.as_array(out)[:n.value]
+        return {k: np.array(a[k]) for k in ("col", "row", "cx", "cy", "area", "abandon")}, t.value
+
+    def mla_lattice_fit(self, lenses: dict, skip_abandoned: bool = True) -> dict:
+        """Hexagonal lattice through the centres of mla_centers()."""
+        n = len(lenses["col"])
+        arr = (MlaLensC * n)()
+        for i in range(n):
+            arr[i] = MlaLensC(int(lenses["col"][i]), int(lenses["row"][i]), float(lenses["cx"][i]),
+                              float(lenses["cy"][i]), float(lenses["area"][i]), int(lenses["abandon"][i]))
+        fit = np.zeros(6, np.float64)
+        self._check(self._L.pfd_mla_lattice_fit(self._h, ctypes.cast(arr, _P), n, int(skip_abandoned), _ptr(fit)),
+                    "pfd_mla_lattice_fit")
+        return dict(origin=(fit[0], fit[1]), pitch=fit[2], angle=fit[3], rms=fit[4], used=int(fit[5]))
 
     def fuse_virtual_depth(self, fid: int, lists, list_counts, is_ref, mla_base: float, bgr=None,
                            points: bool = True, download: bool = True, min_ref_disp: float = 1.0,

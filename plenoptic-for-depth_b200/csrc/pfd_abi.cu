@@ -20,6 +20,7 @@
 #include "refocus_kernels.h"
 #include "vdrd_kernels.h"
 #include "fuse_kernels.h"
+#include "mla_kernels.h"
 
 namespace {
 
@@ -1283,6 +1284,225 @@ pfd_status pfd_fuse_virtual_depth(pfd_ctx* ctx, int frame_id, const pfd_fuse_par
         }
     }
     if (vd_map || conf || aif || points || n_points) return check_device_error(ctx);
+    return PFD_OK;
+}
+
+// ---- micro-lens centres ------------------------------------------------------
+
+// DepthSolver::Otsu (DepthSolver.cpp:486-546) on the histogram, float arithmetic as written.
+static int otsu_threshold(const unsigned int* count, long long pixel_sum)
+{
+    float pro[256];
+    for (int i = 0; i < 256; ++i) pro[i] = (float)count[i] / (float)pixel_sum;
+    float deltaMax = 0;
+    int threshold = 0;
+    for (int i = 0; i < 256; ++i) {
+        float w0 = 0, w1 = 0, u0tmp = 0, u1tmp = 0;
+        for (int j = 0; j < 256; ++j) {
+            if (j <= i) { w0 += pro[j]; u0tmp += j * pro[j]; }
+            else { w1 += pro[j]; u1tmp += j * pro[j]; }
+        }
+        const float u0 = u0tmp / w0, u1 = u1tmp / w1, u = u0tmp + u1tmp;
+        const float deltaTmp = w0 * (u0 - u) * (u0 - u) + w1 * (u1 - u) * (u1 - u);
+        if (deltaTmp > deltaMax) { deltaMax = deltaTmp; threshold = i; }
+    }
+    return threshold;
+}
+
+pfd_status pfd_mla_centers(pfd_ctx* ctx, const uint8_t* white_bgr, int W, int H, int step, float baseline,
+                           int mla_u_size, int mla_v_size, pfd_mla_lens* out, int max_out, int* n_out, int* threshold)
+{
+    if (!ctx) return PFD_EINVAL;
+    if (!white_bgr || !n_out || (!out && max_out > 0)) return fail(ctx, PFD_EINVAL, "mla_centers: NULL argument");
+    if (W < 1 || H < 1 || step < 3 * W || (long long)W * H > (1LL << 30))
+        return fail(ctx, PFD_EINVAL, "mla_centers: bad image size %dx%d, step %d", W, H, step);
+    if (!(baseline > 0.0f) || mla_u_size < 1 || mla_v_size < 1)
+        return fail(ctx, PFD_EINVAL, "mla_centers: baseline and lens counts must be positive");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const size_t n = (size_t)W * H;
+    const int max_roots = (int)std::min<size_t>(n / 2 + 1, (size_t)1 << 24);
+    uint8_t *d_bgr = nullptr, *d_fg = nullptr;
+    int *d_L = nullptr, *d_roots = nullptr;
+    unsigned int* d_hist = nullptr;
+    double* d_sums = nullptr;
+    struct Pool {
+        cudaStream_t s;
+        std::vector<void*> p;
+        ~Pool() { for (void* q : p) cudaFreeAsync(q, s); }
+        cudaError_t get(void** q, size_t b) { cudaError_t e = cudaMallocAsync(q, b, s); if (!e) p.push_back(*q); return e; }
+    } P{ s, {} };
+    CU(P.get((void**)&d_bgr, (size_t)step * H));
+    CU(P.get((void**)&d_fg, n));
+    CU(P.get((void**)&d_L, sizeof(int) * n));
+    CU(P.get((void**)&d_roots, sizeof(int) * (size_t)max_roots));
+    CU(P.get((void**)&d_hist, sizeof(unsigned int) * (256 + 1)));
+    CU(cudaMemcpyAsync(d_bgr, white_bgr, (size_t)step * H, cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(d_hist, 0, sizeof(unsigned int) * (256 + 1), s));
+    CU(pfd::launch_mla_hist(d_bgr, W, H, step, d_hist, s));
+    unsigned int hist[256];
+    CU(cudaMemcpyAsync(hist, d_hist, sizeof(hist), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    const int t = otsu_threshold(hist, (long long)W * H);
+    if (threshold) *threshold = t;
+    unsigned int* d_nroots = d_hist + 256;
+    CU(pfd::launch_mla_components(d_bgr, W, H, step, t, d_fg, d_L, d_roots, d_nroots, max_roots, ctx->d_err, s));
+    unsigned int nr = 0;
+    CU(cudaMemcpyAsync(&nr, d_nroots, sizeof(nr), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if ((int)nr > max_roots) return fail(ctx, PFD_EINVAL, "mla_centers: %u components exceed %d", nr, max_roots);
+    // findContours lists the external contours in reverse order of discovery
+    std::vector<int> roots(nr);
+    if (nr) CU(cudaMemcpyAsync(roots.data(), d_roots, sizeof(int) * nr, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    std::sort(roots.begin(), roots.end(), [](int a, int b) { return a > b; });
+    std::vector<double> sums(3 * (size_t)nr);
+    if (nr) {
+        CU(P.get((void**)&d_sums, sizeof(double) * 3 * nr));
+        CU(cudaMemcpyAsync(d_roots, roots.data(), sizeof(int) * nr, cudaMemcpyHostToDevice, s));
+        CU(pfd::launch_mla_trace(d_fg, W, H, d_roots, (int)nr, d_sums, ctx->d_err, s));
+        CU(cudaMemcpyAsync(sums.data(), d_sums, sizeof(double) * 3 * nr, cudaMemcpyDeviceToHost, s));
+    }
+    ctx->launches += 4 + (nr ? 1 : 0);
+    pfd_status st = check_device_error(ctx);
+    if (st != PFD_OK) return fail(ctx, PFD_EINVAL, "mla_centers: component labelling or border tracing did not finish");
+
+    // ComputeMLACentersFromWhiteImage (:752-868): moments, position filter,
+    // rows by running mean y, columns by x, small-area flag.
+    struct Info { float x, y, area; int col, row; bool abandon; };
+    std::vector<Info> infos;
+    double average_area = 0.0;
+    for (unsigned k = 0; k < nr; ++k) {
+        const double a00 = sums[3 * k], a10 = sums[3 * k + 1], a01 = sums[3 * k + 2];
+        double m00 = 0, m10 = 0, m01 = 0;
+        if (std::fabs(a00) > 1.1920928955078125e-07) {       // moments() (FLT_EPSILON)
+            const double h = a00 > 0 ? 0.5 : -0.5, s6 = a00 > 0 ? 1.0 / 6.0 : -1.0 / 6.0;
+            m00 = a00 * h; m10 = a10 * s6; m01 = a01 * s6;
+        }
+        float x = -1, y = -1;
+        if (m00 != 0) { x = (float)(m10 / m00); y = (float)(m01 / m00); }
+        if (y >= baseline * 0.5 && y <= baseline * mla_v_size && x >= baseline * 0.5 && x <= baseline * mla_u_size) {
+            const double area = std::fabs(a00 * 0.5);                 // contourArea()
+            average_area += area;
+            infos.push_back({ x, y, (float)area, 0, 0, false });      // MLA_Info::SetArea(float)
+        }
+    }
+    average_area /= (double)nr;
+    std::map<int, std::vector<int>> rows;
+    float y_ideal_next = 0.0f;
+    int y_ideal_next_count = 0;
+    for (int row = 0; row < mla_v_size; ++row) {
+        std::vector<int> members;
+        float y_ideal = 0.0f;
+        if (row == 0) {
+            y_ideal = baseline * 0.5;
+        } else {
+            y_ideal = y_ideal_next / y_ideal_next_count;
+            y_ideal += baseline;
+            y_ideal_next = 0.0f;
+            y_ideal_next_count = 0;
+        }
+        for (int i = 0; i < (int)infos.size(); ++i)
+            if (std::fabs(infos[i].y - y_ideal) < baseline * 0.5) {
+                members.push_back(i);
+                y_ideal_next += infos[i].y;
+                y_ideal_next_count++;
+            }
+        std::map<float, int> by_x;                                   // equal x: the later lens wins
+        for (int i = 0; i < (int)members.size(); ++i) by_x[infos[members[i]].x] = i;
+        std::vector<int> sorted;
+        for (auto& kv : by_x) sorted.push_back(members[kv.second]);
+        rows[row] = sorted;
+    }
+    std::map<std::pair<int, int>, int> keyed;                        // (row, col), the map's key order
+    for (auto& kv : rows)
+        for (int col = 0; col < (int)kv.second.size(); ++col) {
+            Info& I = infos[kv.second[col]];
+            I.col = col;
+            I.row = kv.first;
+            I.abandon = I.area < average_area * 0.8;
+            keyed[{ kv.first, col }] = kv.second[col];
+        }
+    *n_out = (int)keyed.size();
+    if ((int)keyed.size() > max_out) return out ? fail(ctx, PFD_EINVAL, "mla_centers: %d lenses, room for %d", *n_out, max_out)
+                                                : PFD_OK;
+    int i = 0;
+    for (auto& kv : keyed) {
+        const Info& I = infos[kv.second];
+        out[i].col = kv.first.second;
+        out[i].row = kv.first.first;
+        out[i].cx = I.x;
+        out[i].cy = I.y;
+        out[i].area = I.area;
+        out[i].abandon = I.abandon ? 1 : 0;
+        ++i;
+    }
+    return PFD_OK;
+}
+
+pfd_status pfd_mla_lattice_fit(pfd_ctx* ctx, const pfd_mla_lens* lenses, int n, int skip_abandoned, double fit[6])
+{
+    if (!ctx) return PFD_EINVAL;
+    if (!lenses || !fit || n < 1) return fail(ctx, PFD_EINVAL, "mla_lattice_fit: need lenses and an output");
+    static_assert(sizeof(pfd_mla_lens) == sizeof(pfd::pfd_mla_lens_dev), "lens layouts differ");
+    std::vector<pfd_mla_lens> use;
+    for (int i = 0; i < n; ++i)
+        if (!(skip_abandoned && lenses[i].abandon) && std::isfinite(lenses[i].cx) && std::isfinite(lenses[i].cy))
+            use.push_back(lenses[i]);
+    if (use.size() < 3) return fail(ctx, PFD_EINVAL, "mla_lattice_fit: fewer than 3 usable lenses");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const int nb = (int)std::max<size_t>(1, std::min<size_t>((use.size() + 1023) / 1024, 256));
+    void *d_l = nullptr, *d_p = nullptr;
+    CU(cudaMallocAsync(&d_l, sizeof(pfd_mla_lens) * use.size(), s));
+    if (cudaMallocAsync(&d_p, sizeof(double) * 14 * nb, s) != cudaSuccess) {
+        cudaFreeAsync(d_l, s);
+        return fail(ctx, PFD_ENOMEM, "mla_lattice_fit: scratch");
+    }
+    std::vector<double> part(14 * (size_t)nb);
+    cudaError_t e = cudaMemcpyAsync(d_l, use.data(), sizeof(pfd_mla_lens) * use.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = pfd::launch_mla_lattice((const pfd::pfd_mla_lens_dev*)d_l, (int)use.size(), (double*)d_p, nb, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(part.data(), d_p, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(d_l, s);
+    cudaFreeAsync(d_p, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(ctx, PFD_ECUDA, "mla_lattice_fit: %s", cudaGetErrorString(e));
+    ctx->launches += 1;
+    double S[14] = { 0 };
+    for (int b = 0; b < nb; ++b)
+        for (int q = 0; q < 14; ++q) S[q] += part[(size_t)b * 14 + q];
+    double M[4][5];
+    int q = 0;
+    for (int i0 = 0; i0 < 4; ++i0)
+        for (int i1 = i0; i1 < 4; ++i1, ++q) M[i0][i1] = M[i1][i0] = S[q];
+    for (int i0 = 0; i0 < 4; ++i0) M[i0][4] = S[10 + i0];
+    // Gaussian elimination with partial pivoting (4 x 4, FP64)
+    for (int c = 0; c < 4; ++c) {
+        int pr = c;
+        for (int r = c + 1; r < 4; ++r)
+            if (std::fabs(M[r][c]) > std::fabs(M[pr][c])) pr = r;
+        if (!(std::fabs(M[pr][c]) > 1e-300)) return fail(ctx, PFD_EINVAL, "mla_lattice_fit: degenerate lens layout");
+        for (int k = 0; k < 5; ++k) std::swap(M[c][k], M[pr][k]);
+        for (int r = 0; r < 4; ++r) {
+            if (r == c) continue;
+            const double f = M[r][c] / M[c][c];
+            for (int k = c; k < 5; ++k) M[r][k] -= f * M[c][k];
+        }
+    }
+    const double ox = M[0][4] / M[0][0], oy = M[1][4] / M[1][1], a = M[2][4] / M[2][2], b = M[3][4] / M[3][3];
+    double ss = 0.0;
+    const double h3 = 0.86602540378443864676;
+    for (const pfd_mla_lens& L : use) {
+        const double u = L.col + ((L.row & 1) ? 0.5 : 0.0), w = L.row * h3;
+        const double ex = ox + u * a - w * b - L.cx, ey = oy + u * b + w * a - L.cy;
+        ss += ex * ex + ey * ey;
+    }
+    fit[0] = ox;
+    fit[1] = oy;
+    fit[2] = std::sqrt(a * a + b * b);
+    fit[3] = std::atan2(b, a);
+    fit[4] = std::sqrt(ss / (double)use.size());
+    fit[5] = (double)use.size();
     return PFD_OK;
 }
 
