@@ -262,7 +262,7 @@ def run_engine(args, rank, world, local_rank):
                 ctx.pm_sweep(fid, params, seed, it, ph)
                 mark(ev, "sweep_b")
         mark(ev, "t2")
-        ctx.cycle_check(fid, ccfg, unit, maps=False)
+        ctx.cycle_check(fid, ccfg, unit, maps=False, stats=False)
         mark(ev, "t3")
         ctx.filter(fid, fcfg, unit, download=False)
         mark(ev, "t4")
@@ -270,6 +270,7 @@ def run_engine(args, rank, world, local_rank):
         mark(ev, "t5")
         ctx.refocus(fid, vds, ow, oh, download=False)
         mark(ev, "t6")
+        ctx.cycle_check_stats(fid)            # the statistics, folded once the path is enqueued
 
     # calibration pass: in-bounds NCC taps per sweep launch (identical trajectory: same seed)
     ctx.set_tap_counting(True)
@@ -333,13 +334,14 @@ def run_engine(args, rank, world, local_rank):
         ctx._check(L.pfd_frame_set_raw(ctx._h, fid, ctypes.c_void_p(pinned_raw.data_ptr()), pinned_raw.shape[1]),
                    "pfd_frame_set_raw")
         ctx.patchmatch(fid, params, seed)
-        ctx.cycle_check(fid, ccfg, unit, maps=False)
+        ctx.cycle_check(fid, ccfg, unit, maps=False, stats=False)
         ctx.filter(fid, fcfg, unit, download=False)
         ctx.reprojection_error(fid, fcfg, unit, download=False)
         ctx._check(L.pfd_refocus(ctx._h, fid, ctypes.c_void_p(vd_host.ctypes.data), len(vd_host), ow, oh,
                                  ctypes.c_void_p(out_stack.data_ptr())), "pfd_refocus")
         ctx._check(L.pfd_download(ctx._h, fid, ctypes.c_void_p(out_plane.data_ptr()), ctypes.c_void_p(out_cost.data_ptr()),
                                   None, ctypes.c_void_p(out_sel.data_ptr())), "pfd_download")
+        ctx.cycle_check_stats(fid)
 
     e2e_step()
     e2e_steps = max(1, min(args.steps, 3))

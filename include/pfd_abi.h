@@ -262,6 +262,11 @@ typedef struct pfd_cycle_stats {
  * each may be NULL. */
 pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg, float baseline_unit,
                            pfd_cycle_stats* stats, float* geo_err, float* pho_err, uint8_t* texmask);
+/* With stats and all three maps NULL, pfd_cycle_check only enqueues the check
+ * (no synchronisation), and this folds its statistics later, e.g. after the
+ * filter and the render are enqueued behind it, so the device does not wait
+ * for the host fold.  Valid until the frame's next cycle check. */
+pfd_status pfd_cycle_check_stats(pfd_ctx* ctx, int frame_id, pfd_cycle_stats* stats);
 
 /* ---- focal stack ----------------------------------------------------------
  * Renders n_slices refocused images of out_w x out_h from the frame's gray

@@ -735,6 +735,27 @@ int orc_pm_sweep_views(const orc_frame* f, const orc_params* p, uint64_t seed, i
     return 0;
 }
 
+long long orc_pm_sweep_taps(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
+                            const orc_state* prev, orc_state* next, int nthreads)
+{
+    if (!f || !p || f->max_nb > MAX_NB) return -1;
+    const long ppv = (long)f->mi_w * f->mi_h, total = ppv * f->n_views;
+    long long taps = 0;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads) reduction(+ : taps)
+#endif
+    for (long t = 0; t < total; ++t) {
+        long long mine = 0;
+        const int vid = (int)(t / ppv);
+        const int rem = (int)(t % ppv);
+        update_pixel(f, p, seed, iter, phase, vid, rem % f->mi_w, rem / f->mi_w, prev, next, &mine);
+        taps += mine;
+    }
+    (void)nthreads;
+    return taps;
+}
+
 int orc_pm_sweep(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
                  const orc_state* prev, orc_state* next, int nthreads)
 {

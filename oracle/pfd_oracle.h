@@ -84,6 +84,10 @@ int orc_pm_sweep(const orc_frame* f, const orc_params* p, uint64_t seed, int ite
                  const orc_state* prev, orc_state* next, int nthreads);
 
 /* Same, restricted to views [v0, v1): the bounded sample the CPU baseline times. */
+/* orc_pm_sweep that also returns the in-bounds NCC taps the reference's algorithm
+ * evaluates in it (the roofline's algorithmic unit), or -1. */
+long long orc_pm_sweep_taps(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
+                            const orc_state* prev, orc_state* next, int nthreads);
 int orc_pm_sweep_views(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
                        const orc_state* prev, orc_state* next, int v0, int v1, int nthreads);
 

@@ -122,6 +122,9 @@ def lib() -> ctypes.CDLL:
         L.orc_fuse_virtual_depth.argtypes = [FP, _P, _P, _P, _P, _I, _P, ctypes.POINTER(OrcFuseParams), _I, _I,
                                              _P, _P, _P, _P]
         L.orc_fuse_virtual_depth.restype = ctypes.c_longlong
+        L.orc_pm_sweep_taps.argtypes = [ctypes.POINTER(OrcFrame), ctypes.POINTER(OrcParams), ctypes.c_uint64, _I, _I,
+                                        ctypes.POINTER(OrcState), ctypes.POINTER(OrcState), _I]
+        L.orc_pm_sweep_taps.restype = ctypes.c_longlong
         L.orc_mla_otsu.argtypes = [_P, _I, _I, _I]
         L.orc_mla_contours.argtypes = [_P, _I, _I, _I, _I, _P, _P, _P, _I]
         L.orc_mla_centers.argtypes = [_P, _I, _I, _I, _F, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P]
@@ -209,6 +212,16 @@ class Oracle:
                                           ctypes.byref(st), views[0], views[1], nthreads)
         assert rc == 0
         return arr
+
+    def sweep_taps(self, params, seed, it, phase, prev, nthreads=0):
+        """(next state, in-bounds NCC taps of the reference's algorithm in this sweep)."""
+        arr, st = self.new_state()
+        ps = OrcState(_p(prev["plane"]), _p(prev["cost"]), _p(prev["disp"]), _p(prev["sel"]))
+        p = self.params(params)
+        taps = lib().orc_pm_sweep_taps(ctypes.byref(self.f), ctypes.byref(p), seed, it, phase, ctypes.byref(ps),
+                                       ctypes.byref(st), nthreads)
+        assert taps >= 0
+        return arr, int(taps)
 
     def patchmatch(self, params, seed, nthreads=0):
         arr, st = self.new_state()

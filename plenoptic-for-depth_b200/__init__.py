@@ -205,6 +205,7 @@ def lib() -> ctypes.CDLL:
             "pfd_vd_to_rd_segments": [_P, _P, ctypes.c_size_t, _P, _I, _P],
             "pfd_fit_behavioral_model": [_P, _P, _P, ctypes.c_size_t, _P],
             "pfd_cycle_check": [_P, _I, ctypes.POINTER(CycleCfgC), _F, ctypes.POINTER(CycleStatsC), _P, _P, _P],
+            "pfd_cycle_check_stats": [_P, _I, ctypes.POINTER(CycleStatsC)],
             "pfd_mla_lattice_fit": [_P, _P, _I, _I, _P],
             "pfd_mla_centers": [_P, _P, _I, _I, _I, _F, _I, _I, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
             "pfd_fuse_virtual_depth": [_P, _I, ctypes.POINTER(FuseParamsC), _P, _P, _I, _P, _P, _P, _P, _P, _P,
@@ -390,11 +391,17 @@ class Context:
                     "pfd_filter")
         return reason, dict(zip(FILTER_STATS, (int(x) for x in stats)))
 
-    def cycle_check(self, fid: int, cfg: CycleCfg, baseline_unit: float, maps: bool = True):
+    def cycle_check(self, fid: int, cfg: CycleCfg, baseline_unit: float, maps: bool = True, stats: bool = True):
         """MICycleCheckerCPU::CheckGlobal on the frame's state (read-only).
         Returns (stats dict, geo_err, pho_err, texture mask); maps are None
-        unless maps=True."""
+        unless maps=True.  With maps and stats False the check is only
+        enqueued and None is returned; cycle_check_stats() folds it later."""
         f = self._frames[fid]
+        if not maps and not stats:
+            c = cfg.c()
+            self._check(self._L.pfd_cycle_check(self._h, fid, ctypes.byref(c), float(baseline_unit), None, None, None,
+                                                None), "pfd_cycle_check")
+            return None
         n = f["V"] * f["mi_w"] * f["mi_h"]
         geo = np.empty(n, np.float32) if maps else None
         pho = np.empty(n, np.float32) if maps else None
@@ -405,6 +412,11 @@ class Context:
                                             _ptr(geo) if maps else None, _ptr(pho) if maps else None,
                                             _ptr(tm) if maps else None), "pfd_cycle_check")
         return {k: getattr(out, k) for k in CYCLE_STATS}, geo, pho, tm
+
+    def cycle_check_stats(self, fid: int) -> dict:
+        out = CycleStatsC()
+        self._check(self._L.pfd_cycle_check_stats(self._h, fid, ctypes.byref(out)), "pfd_cycle_check_stats")
+        return {k: getattr(out, k) for k in CYCLE_STATS}
 
     def vd_to_rd_map(self, vd, c) -> np.ndarray:
         """VirtualToRealDepthFunc::convertVirtualToRealDepth on the device (FP64)."""

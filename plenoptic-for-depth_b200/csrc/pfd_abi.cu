@@ -60,6 +60,7 @@ struct Frame {
     unsigned int* d_cyc_hist = nullptr;        // cycle check: masked geometric-error histogram
     float* d_cyc_maps = nullptr;               // cycle check: geo and photo error maps
     uint8_t* d_cyc_tm = nullptr;               // cycle check: texture mask
+    bool cyc_done = false;                     // d_cyc_recs / d_cyc_hist hold a cycle check
     std::vector<float> h_centers;              // lens centres, for the refocus bucket grid
     int* d_cells = nullptr;                    // refocus: cell_start [cells + 1] then cell_ids [V]
     int grid_w = 0, grid_h = 0;
@@ -590,12 +591,13 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
         ctx->used += need;
     }
     P.cost_scratch = ctx->d_scratch;
-    P.cvec_ok = cvec_usable(*f, *params, phase);
+    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase);
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
-    cvec_swept(*f, *params, phase);
+    if (ctx->counting) f->cvec_valid = 0;        // tap counting evaluates everything and stores nothing
+    else cvec_swept(*f, *params, phase);
     return PFD_OK;
 }
 
@@ -817,56 +819,9 @@ pfd_status pfd_reprojection_error(pfd_ctx* ctx, int frame_id, const pfd_filter_c
     return PFD_OK;
 }
 
-pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg, float baseline_unit,
-                           pfd_cycle_stats* stats, float* geo_err, float* pho_err, uint8_t* texmask)
+// CheckGlobal's fold of the per-tile records (MICycleCheck.cpp:541-600, 742-832).
+static void fold_cycle_stats(const std::vector<pfd::CycleTileRec>& rec, const unsigned int* hist, pfd_cycle_stats* stats)
 {
-    if (!ctx) return PFD_EINVAL;
-    Frame* f = find_frame(ctx, frame_id);
-    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
-    if (!cfg) return fail(ctx, PFD_EINVAL, "cycle config is NULL");
-    if (cfg->max_triplet < 0 || cfg->max_triplet > 32) return fail(ctx, PFD_EINVAL, "max_triplet outside [0, 32]");
-    if (!(baseline_unit > 0.0f)) return fail(ctx, PFD_EINVAL, "baseline_unit must be > 0");
-    if (!f->has_state) return fail(ctx, PFD_ESTATE, "cycle check before PatchMatch");
-    DeviceGuard g(ctx->device);
-    const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
-    pfd_status st;
-    void* p = nullptr;
-    if (!f->d_cyc_recs) {
-        const size_t rec_bytes = sizeof(pfd::CycleTileRec) * (size_t)f->V;
-        if ((st = frame_alloc(ctx, *f, &p, rec_bytes + sizeof(unsigned int) * pfd::kCycleHistBins)) != PFD_OK)
-            return st;
-        f->d_cyc_recs = (pfd::CycleTileRec*)p;
-        f->d_cyc_hist = (unsigned int*)((char*)p + rec_bytes);
-    }
-    const bool maps = geo_err || pho_err || texmask;
-    if (maps && !f->d_cyc_maps) {
-        if ((st = frame_alloc(ctx, *f, &p, 2 * sizeof(float) * px + px)) != PFD_OK) return st;
-        f->d_cyc_maps = (float*)p;
-        f->d_cyc_tm = (uint8_t*)(f->d_cyc_maps + 2 * px);
-    }
-    pfd::CycleCfg cc;
-    static_assert(sizeof(cc) == sizeof(pfd_cycle_cfg), "cycle config layouts differ");
-    std::memcpy(&cc, cfg, sizeof(cc));
-    const pfd::CheckFrame F = check_frame(*f, baseline_unit);
-    if (pfd::cycle_smem_bytes(F) > 227 * 1024) return fail(ctx, PFD_EINVAL, "cycle-check tile does not fit shared memory");
-    CU(cudaMemsetAsync(f->d_cyc_hist, 0, sizeof(unsigned int) * pfd::kCycleHistBins, ctx->stream));
-    CU(pfd::launch_cycle(F, cc, f->s[f->cur], maps ? f->d_cyc_maps : nullptr, maps ? f->d_cyc_maps + px : nullptr,
-                         maps ? f->d_cyc_tm : nullptr, f->d_cyc_recs, f->d_cyc_hist, ctx->stream));
-    ctx->launches += 1;
-    std::vector<pfd::CycleTileRec> rec(f->V);
-    unsigned int hist[pfd::kCycleHistBins];
-    CU(cudaMemcpyAsync(rec.data(), f->d_cyc_recs, sizeof(pfd::CycleTileRec) * rec.size(), cudaMemcpyDeviceToHost,
-                       ctx->stream));
-    CU(cudaMemcpyAsync(hist, f->d_cyc_hist, sizeof(hist), cudaMemcpyDeviceToHost, ctx->stream));
-    if (geo_err) CU(cudaMemcpyAsync(geo_err, f->d_cyc_maps, sizeof(float) * px, cudaMemcpyDeviceToHost, ctx->stream));
-    if (pho_err)
-        CU(cudaMemcpyAsync(pho_err, f->d_cyc_maps + px, sizeof(float) * px, cudaMemcpyDeviceToHost, ctx->stream));
-    if (texmask) CU(cudaMemcpyAsync(texmask, f->d_cyc_tm, px, cudaMemcpyDeviceToHost, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
-    if ((st = check_device_error(ctx)) != PFD_OK) return st;
-    if (!stats) return PFD_OK;
-
-    // CheckGlobal's fold over the tiles in key order (MICycleCheck.cpp:541-600, 742-832)
     pfd_cycle_stats o;
     std::memset(&o, 0, sizeof(o));
     double io_mean_geo = 0.0, io_mean_photo = 0.0, io_sq_geo = 0.0, io_sq_photo = 0.0;
@@ -874,7 +829,7 @@ pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg,
     double m_sq_geo = 0.0, m_sq_photo = 0.0, m_sum_geo = 0.0, m_sum_photo = 0.0;
     long long m_count = 0, all_count = 0, c_total = 0, c_good = 0, c_geo = 0, c_photo = 0;
     double geo_min = INFINITY, geo_max = 0.0;
-    for (int v = 0; v < f->V; ++v) {
+    for (size_t v = 0; v < rec.size(); ++v) {
         const pfd::CycleTileRec& r = rec[v];
         if (r.n > 0) {
             const double mg = r.sum_geo / (double)r.n, mp = r.sum_photo / (double)r.n;
@@ -934,8 +889,81 @@ pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg,
     o.masked_geo_min = std::isfinite(geo_min) ? geo_min : 0.0;
     o.masked_geo_max = geo_max;
     *stats = o;
+}
+
+pfd_status pfd_cycle_check(pfd_ctx* ctx, int frame_id, const pfd_cycle_cfg* cfg, float baseline_unit,
+                           pfd_cycle_stats* stats, float* geo_err, float* pho_err, uint8_t* texmask)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!cfg) return fail(ctx, PFD_EINVAL, "cycle config is NULL");
+    if (cfg->max_triplet < 0 || cfg->max_triplet > 32) return fail(ctx, PFD_EINVAL, "max_triplet outside [0, 32]");
+    if (!(baseline_unit > 0.0f)) return fail(ctx, PFD_EINVAL, "baseline_unit must be > 0");
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "cycle check before PatchMatch");
+    DeviceGuard g(ctx->device);
+    const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
+    pfd_status st;
+    void* p = nullptr;
+    if (!f->d_cyc_recs) {
+        const size_t rec_bytes = sizeof(pfd::CycleTileRec) * (size_t)f->V;
+        if ((st = frame_alloc(ctx, *f, &p, rec_bytes + sizeof(unsigned int) * pfd::kCycleHistBins)) != PFD_OK)
+            return st;
+        f->d_cyc_recs = (pfd::CycleTileRec*)p;
+        f->d_cyc_hist = (unsigned int*)((char*)p + rec_bytes);
+    }
+    const bool maps = geo_err || pho_err || texmask;
+    if (maps && !f->d_cyc_maps) {
+        if ((st = frame_alloc(ctx, *f, &p, 2 * sizeof(float) * px + px)) != PFD_OK) return st;
+        f->d_cyc_maps = (float*)p;
+        f->d_cyc_tm = (uint8_t*)(f->d_cyc_maps + 2 * px);
+    }
+    pfd::CycleCfg cc;
+    static_assert(sizeof(cc) == sizeof(pfd_cycle_cfg), "cycle config layouts differ");
+    std::memcpy(&cc, cfg, sizeof(cc));
+    const pfd::CheckFrame F = check_frame(*f, baseline_unit);
+    if (pfd::cycle_smem_bytes(F) > 227 * 1024) return fail(ctx, PFD_EINVAL, "cycle-check tile does not fit shared memory");
+    CU(cudaMemsetAsync(f->d_cyc_hist, 0, sizeof(unsigned int) * pfd::kCycleHistBins, ctx->stream));
+    CU(pfd::launch_cycle(F, cc, f->s[f->cur], maps ? f->d_cyc_maps : nullptr, maps ? f->d_cyc_maps + px : nullptr,
+                         maps ? f->d_cyc_tm : nullptr, f->d_cyc_recs, f->d_cyc_hist, ctx->stream));
+    ctx->launches += 1;
+    f->cyc_done = true;
+    if (!stats && !geo_err && !pho_err && !texmask) return PFD_OK;   // stays enqueued; pfd_cycle_check_stats folds it later
+    std::vector<pfd::CycleTileRec> rec(f->V);
+    unsigned int hist[pfd::kCycleHistBins];
+    CU(cudaMemcpyAsync(rec.data(), f->d_cyc_recs, sizeof(pfd::CycleTileRec) * rec.size(), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaMemcpyAsync(hist, f->d_cyc_hist, sizeof(hist), cudaMemcpyDeviceToHost, ctx->stream));
+    if (geo_err) CU(cudaMemcpyAsync(geo_err, f->d_cyc_maps, sizeof(float) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (pho_err)
+        CU(cudaMemcpyAsync(pho_err, f->d_cyc_maps + px, sizeof(float) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (texmask) CU(cudaMemcpyAsync(texmask, f->d_cyc_tm, px, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if ((st = check_device_error(ctx)) != PFD_OK) return st;
+    if (stats) fold_cycle_stats(rec, hist, stats);
     return PFD_OK;
 }
+
+pfd_status pfd_cycle_check_stats(pfd_ctx* ctx, int frame_id, pfd_cycle_stats* stats)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!stats) return fail(ctx, PFD_EINVAL, "cycle_check_stats: NULL output");
+    if (!f->cyc_done) return fail(ctx, PFD_ESTATE, "cycle_check_stats before pfd_cycle_check");
+    DeviceGuard g(ctx->device);
+    std::vector<pfd::CycleTileRec> rec(f->V);
+    unsigned int hist[pfd::kCycleHistBins];
+    CU(cudaMemcpyAsync(rec.data(), f->d_cyc_recs, sizeof(pfd::CycleTileRec) * rec.size(), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaMemcpyAsync(hist, f->d_cyc_hist, sizeof(hist), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    pfd_status st = check_device_error(ctx);
+    if (st != PFD_OK) return st;
+    fold_cycle_stats(rec, hist, stats);
+    return PFD_OK;
+}
+
 
 static const int kMaxSlices = 1024;
 
@@ -1613,11 +1641,12 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     st = noalloc_scratch(ctx, ctx->device, &scratch);
     if (st != PFD_OK) return st;
     P.cost_scratch = scratch;
-    P.cvec_ok = cvec_usable(*f, *params, phase);
+    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase);
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
-    cvec_swept(*f, *params, phase);
+    if (ctx->counting) f->cvec_valid = 0;        // tap counting evaluates everything and stores nothing
+    else cvec_swept(*f, *params, phase);
     return PFD_OK;
 }

@@ -635,7 +635,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                 for (int s = 0; s < 8; ++s) {
                     if (!C.flag[s] || C.src[s] >= 0) continue;
                     const float4 q = prev.plane[vbase + C.pos[s]];
-                    int r = 0;
+                    int r = COUNT ? nh : 0;                  // tap counting evaluates every candidate, as the reference
                     for (; r < nh; ++r) {
                         const float4 o = S.plane[r];
                         if (__float_as_uint(o.x) == __float_as_uint(q.x) && __float_as_uint(o.y) == __float_as_uint(q.y) &&
@@ -650,9 +650,10 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             }
             slots = __shfl_sync(kFullMask, slots, 0);
             nh = __shfl_sync(kFullMask, nh, 0);
-            if (P.cvec_ok && lane < nc) S.cost[lane] = P.cvec[idx * K + lane];
+            const bool use_cvec = !COUNT && P.cvec_ok;
+            if (use_cvec && lane < nc) S.cost[lane] = P.cvec[idx * K + lane];
             __syncwarp();
-            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nh, nc, lane, P.cvec_ok ? 1ull : 0ull, ~0u);
+            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nh, nc, lane, use_cvec ? 1ull : 0ull, ~0u);
 #define SLOT(s) ((int)((slots >> (4 * (s))) & 15ull))
 #define COSTA(s, k) S.cost[SLOT(s) * K + (k)]
 
@@ -746,83 +747,115 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             // and rebuilt below when a proposal wins.  The refinement's random draws do
             // not depend on the best plane, so they are taken now, in their order.
             const int nsel = __popc(tsel);
-            int qn = -1, kn = -1;
-            if (lane < nsel) {
-                kn = nth_set_bit(tsel, lane);
-                const int nvid = F.nb_ids[vid * K + kn];
-                if (nvid >= 0) qn = proposal_pos(T.geo[kn], x, y, W, H, best_plane);
-            }
-            const unsigned actm = __ballot_sync(kFullMask, qn >= 0);
-            if (qn >= 0) {
-                const int nvid = F.nb_ids[vid * K + kn];
-                S.plane[__popc(actm & ((1u << lane) - 1u))] =
-                    proposal_plane(T.geo[kn], prev.plane + (size_t)nvid * P.ppv, qn, x, y, W);
-            }
-            if (lane < nsel) S.aux[lane] = qn;
-            const int nact = __popc(actm);
             (void)g2.uniform();                          // depth_rand: drawn, never used
             const float4 rn = random_normal(g2);
             const float u1 = g2.uniform(), u2 = g2.uniform(), u3 = g2.uniform();
             const float u4 = g2.uniform();
             const float4 c0 = random_plane(g2, P.depth_min, P.depth_max);
-            float4 cand[5];
-            refine_candidates(x, y, best_plane, c0, rn, u1, u2, u3, u4, P.pert_pi, cand);
-            // the candidate equal to the best plane has the best cost and cannot win
-            bool skip3 = __float_as_uint(cand[3].w) == __float_as_uint(best_plane.w);
-            const int r0 = nact;                         // rows of the refinement candidates
-            if (lane == 0)
-                for (int i = 0; i < 5; ++i) S.plane[r0 + i] = cand[i];
-            __syncwarp();
-            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull, tsel);
-            weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
-
-            bool changed = false, partial = false;
-            int hs = 0;                                  // speculative row of proposal n
-            for (int n = 0; n < nsel; ++n) {
-                const int k = nth_set_bit(tsel, n);
-                const int nvid = F.nb_ids[vid * K + k];
-                const int spec_q = S.aux[n];
-                int q = spec_q;
-                if (changed) q = (nvid >= 0) ? proposal_pos(T.geo[k], x, y, W, H, best_plane) : -1;
-                float c = kCostMax;
-                int cmin = -1;
-                float4 proxy = make_float4(0.f, 0.f, 1.f, 0.f);
-                if (q >= 0 && q == spec_q) {
-                    c = S.wres[hs];
-                    cmin = S.wmin[hs];
-                    proxy = S.plane[hs];
-                } else if (q >= 0) {
-                    // the best plane moved the sample position: rebuild this proposal in its
-                    // own row (or the spare row after the refinement candidates) and evaluate it
-                    const int row = (spec_q >= 0) ? hs : r0 + 5;
-                    proxy = proposal_plane(T.geo[k], prev.plane + (size_t)nvid * P.ppv, q, x, y, W);
-                    __syncwarp();
-                    if (lane == 0) S.plane[row] = proxy;
-                    __syncwarp();
-                    eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull, tsel);
-                    weigh_hyps(S, K, row + 1, nc, vw_lo, vw_hi, lane, tsel);
-                    c = S.wres[row];
-                    cmin = S.wmin[row];
+            bool partial = false;
+            if constexpr (!COUNT) {
+                int qn = -1, kn = -1;
+                if (lane < nsel) {
+                    kn = nth_set_bit(tsel, lane);
+                    const int nvid = F.nb_ids[vid * K + kn];
+                    if (nvid >= 0) qn = proposal_pos(T.geo[kn], x, y, W, H, best_plane);
                 }
-                if (spec_q >= 0) ++hs;
-                if (q >= 0 && c < best_cost) { best_cost = c; best_plane = proxy; best_min = cmin; changed = true; partial = true; }
-            }
-            if (changed) {
-                // candidates 2-4 follow the best plane: rebuild and evaluate them again
+                const unsigned actm = __ballot_sync(kFullMask, qn >= 0);
+                if (qn >= 0) {
+                    const int nvid = F.nb_ids[vid * K + kn];
+                    S.plane[__popc(actm & ((1u << lane) - 1u))] =
+                        proposal_plane(T.geo[kn], prev.plane + (size_t)nvid * P.ppv, qn, x, y, W);
+                }
+                if (lane < nsel) S.aux[lane] = qn;
+                const int nact = __popc(actm);
+                float4 cand[5];
                 refine_candidates(x, y, best_plane, c0, rn, u1, u2, u3, u4, P.pert_pi, cand);
-                skip3 = __float_as_uint(cand[3].w) == __float_as_uint(best_plane.w);
+                // the candidate equal to the best plane has the best cost and cannot win
+                bool skip3 = __float_as_uint(cand[3].w) == __float_as_uint(best_plane.w);
+                const int r0 = nact;                         // rows of the refinement candidates
+                if (lane == 0)
+                    for (int i = 0; i < 5; ++i) S.plane[r0 + i] = cand[i];
+                __syncwarp();
+                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull, tsel);
+                weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
+
+                bool changed = false;
+                int hs = 0;                                  // speculative row of proposal n
+                for (int n = 0; n < nsel; ++n) {
+                    const int k = nth_set_bit(tsel, n);
+                    const int nvid = F.nb_ids[vid * K + k];
+                    const int spec_q = S.aux[n];
+                    int q = spec_q;
+                    if (changed) q = (nvid >= 0) ? proposal_pos(T.geo[k], x, y, W, H, best_plane) : -1;
+                    float c = kCostMax;
+                    int cmin = -1;
+                    float4 proxy = make_float4(0.f, 0.f, 1.f, 0.f);
+                    if (q >= 0 && q == spec_q) {
+                        c = S.wres[hs];
+                        cmin = S.wmin[hs];
+                        proxy = S.plane[hs];
+                    } else if (q >= 0) {
+                        // the best plane moved the sample position: rebuild this proposal in its
+                        // own row (or the spare row after the refinement candidates) and evaluate it
+                        const int row = (spec_q >= 0) ? hs : r0 + 5;
+                        proxy = proposal_plane(T.geo[k], prev.plane + (size_t)nvid * P.ppv, q, x, y, W);
+                        __syncwarp();
+                        if (lane == 0) S.plane[row] = proxy;
+                        __syncwarp();
+                        eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull, tsel);
+                        weigh_hyps(S, K, row + 1, nc, vw_lo, vw_hi, lane, tsel);
+                        c = S.wres[row];
+                        cmin = S.wmin[row];
+                    }
+                    if (spec_q >= 0) ++hs;
+                    if (q >= 0 && c < best_cost) { best_cost = c; best_plane = proxy; best_min = cmin; changed = true; partial = true; }
+                }
+                if (changed) {
+                    // candidates 2-4 follow the best plane: rebuild and evaluate them again
+                    refine_candidates(x, y, best_plane, c0, rn, u1, u2, u3, u4, P.pert_pi, cand);
+                    skip3 = __float_as_uint(cand[3].w) == __float_as_uint(best_plane.w);
+                    __syncwarp();
+                    if (lane == 0)
+                        for (int i = 2; i < 5; ++i) S.plane[r0 + i] = cand[i];
+                    __syncwarp();
+                    const uint64_t redo = (7ull << (r0 + 2)) & ~(skip3 ? (1ull << (r0 + 3)) : 0ull);
+                    eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo, tsel);
+                    weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
+                }
+                for (int i = 0; i < 5; ++i) {
+                    if (i == 3 && skip3) continue;
+                    const float c = S.wres[r0 + i];
+                    if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = S.wmin[r0 + i]; partial = true; }
+                }
+            } else {
+                // tap counting: the reference's own evaluations, proposals one by one from the
+                // best plane so far, then all five refinement candidates, on every view
+                for (int n = 0; n < nsel; ++n) {
+                    const int k = nth_set_bit(tsel, n);
+                    const int nvid = F.nb_ids[vid * K + k];
+                    const int q = (nvid >= 0) ? proposal_pos(T.geo[k], x, y, W, H, best_plane) : -1;
+                    if (q < 0) continue;
+                    const float4 proxy = proposal_plane(T.geo[k], prev.plane + (size_t)nvid * P.ppv, q, x, y, W);
+                    __syncwarp();
+                    if (lane == 0) S.plane[0] = proxy;
+                    __syncwarp();
+                    eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
+                    weigh_hyps(S, K, 1, nc, vw_lo, vw_hi, lane, ~0u);
+                    const float c = S.wres[0];
+                    if (c < best_cost) { best_cost = c; best_plane = proxy; best_min = S.wmin[0]; }
+                }
+                float4 cand[5];
+                refine_candidates(x, y, best_plane, c0, rn, u1, u2, u3, u4, P.pert_pi, cand);
                 __syncwarp();
                 if (lane == 0)
-                    for (int i = 2; i < 5; ++i) S.plane[r0 + i] = cand[i];
+                    for (int i = 0; i < 5; ++i) S.plane[i] = cand[i];
                 __syncwarp();
-                const uint64_t redo = (7ull << (r0 + 2)) & ~(skip3 ? (1ull << (r0 + 3)) : 0ull);
-                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo, tsel);
-                weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
-            }
-            for (int i = 0; i < 5; ++i) {
-                if (i == 3 && skip3) continue;
-                const float c = S.wres[r0 + i];
-                if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = S.wmin[r0 + i]; partial = true; }
+                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, 5, nc, lane, 0ull, ~0u);
+                weigh_hyps(S, K, 5, nc, vw_lo, vw_hi, lane, ~0u);
+                for (int i = 0; i < 5; ++i) {
+                    const float c = S.wres[i];
+                    if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = S.wmin[i]; }
+                }
             }
             if (partial) {
                 // proposals and refinement candidates were evaluated on the selected views
@@ -840,7 +873,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             }
             // the stored vector of the new current plane (unchanged when the current
             // plane stays and its stored vector was used)
-            if (P.cvec && lane < nc && !(best_row == 0 && P.cvec_ok)) P.cvec[idx * K + lane] = best_vec;
+            if (!COUNT && P.cvec && lane < nc && !(best_row == 0 && P.cvec_ok)) P.cvec[idx * K + lane] = best_vec;
             if (lane == 0) {
                 float4 best_disp = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (best_min >= 0)

@@ -79,6 +79,27 @@ def test_cycle_check_is_read_only_and_repeatable(pfd, ctx, frame):
     assert a[0] == b[0] and b[1] is None
 
 
+def test_enqueued_cycle_check_folds_the_same_statistics(pfd, ctx, frame):
+    """Enqueued without outputs, the check does not synchronise; its
+    statistics, folded later by pfd_cycle_check_stats (here after a filter has
+    changed the state behind it), are the ones of the state it saw."""
+    w, fid = frame
+    cfg = pfd.CycleCfg()
+    sync_stats = ctx.cycle_check(fid, cfg, PITCH, maps=False)[0]
+    P = pfd.PmParams(base=PITCH, patch_size=11, max_iterations=2)
+    other = ctx.frame_upload(w.frame.raw, w.centers, w.tilekeys, w.mi, w.mi, w.nb_ids, w.nb_counts)
+    ctx.patchmatch(other, P, seed=8)
+    assert ctx.cycle_check(other, cfg, PITCH, maps=False, stats=False) is None
+    ctx.filter(other, pfd.FilterCfg(), PITCH, download=False)
+    assert ctx.cycle_check_stats(other) == sync_stats
+    ctx.frame_free(other)
+    fresh = ctx.frame_upload(w.frame.raw, w.centers, w.tilekeys, w.mi, w.mi, w.nb_ids, w.nb_counts)
+    with pytest.raises(pfd.PfdError) as e:
+        ctx.cycle_check_stats(fresh)
+    assert e.value.code == -7
+    ctx.frame_free(fresh)
+
+
 def test_cycle_check_errors(pfd, ctx, frame):
     w, fid = frame
     with pytest.raises(pfd.PfdError) as e:

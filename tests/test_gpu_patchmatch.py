@@ -173,6 +173,36 @@ def test_sweeps_after_state_changes_bitexact(pfd, oracle, ctx):
     ctx.frame_free(fid)
 
 
+def test_tap_count_is_the_reference_work(pfd, oracle, ctx):
+    """The calibration pass (tap counting on) evaluates what the reference's
+    algorithm evaluates, with none of the device's shortcuts (shared rows for
+    equal planes, the stored vector of the current plane, selected views only
+    for proposals and refinement, speculative proposals), so its count of
+    in-bounds NCC taps, the roofline's algorithmic unit, equals the oracle's
+    count for every sweep; the state stays bit-exact."""
+    pitch, K = 23.2, 12
+    w = _workload(pfd, 260, 200, pitch, K=K, seed=12)
+    fid = _upload(ctx, w)
+    P = pfd.PmParams(base=pitch, patch_size=15, max_iterations=2)
+    orc = oracle.Oracle(w.gray, w.centers, w.nb_ids, w.nb_counts)
+    seed = 17
+    ctx.pm_init(fid, P, seed)
+    st = orc.init(P, seed)
+    for it in range(2):
+        for ph in range(2):
+            counting = (it + ph) % 2 == 1             # counting and plain sweeps interleaved
+            ctx.set_tap_counting(counting)
+            ctx.read_tap_count()
+            ctx.pm_sweep(fid, P, seed, it, ph)
+            dev_taps = ctx.read_tap_count()
+            st, taps = orc.sweep_taps(P, seed, it, ph, st)
+            _state_equal(ctx.download(fid), st, f"sweep {it}.{ph}")
+            if counting:
+                assert dev_taps == taps, f"sweep {it}.{ph}: device {dev_taps} taps, reference {taps}"
+    ctx.set_tap_counting(False)
+    ctx.frame_free(fid)
+
+
 def test_patchmatch_virtual_depth_parity(pfd, oracle, ctx):
     """Full pfd_patchmatch (3 iterations): >= 99.5% of valid pixels within 0.01
     virtual depth of the oracle (virtual depth = pitch / disparity)."""
