@@ -282,6 +282,23 @@ pfd_status pfd_cycle_check_stats(pfd_ctx* ctx, int frame_id, pfd_cycle_stats* st
 pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_slices, int out_w, int out_h,
                        float* out);
 
+/* ---- matching-neighbour selection -----------------------------------------
+ * SelectNeighbors::CollectMIANeighImagesForMatch (MINeighbor/SelectNeighbors.cpp:
+ * 113-193) for every micro-image: up to five rings of lenses found by the
+ * reference's walk over the key grid, each candidate scored by
+ * MISimilarityMeasure::MeasureSimilarity (Util/MISimilarityMeasure.cpp:173-284,
+ * computed on the device for every candidate), candidates rejected by the RANSAC
+ * line fitted at the third ring (MVStereo/LFDepthInfo.cpp:136-211), the search
+ * stopped at a ring with two or more outliers, and the survivors sorted by the
+ * normalised baseline score (SelectNeighbors.cpp:770-832, LFDepthInfo.cpp:214-241):
+ * m_NeighsSortVecForMatch.
+ *   centers [n][2], tilekeys [n][2] (column, row) inside mla_u_size x mla_v_size
+ *   images  [n][mi_h][mi_w] gray micro-images (MLA_Problem::m_Image_gray)
+ *   nb_ids  [n][max_nb] view ids best first (-1 padded), nb_counts [n] (<= max_nb <= 128) */
+pfd_status pfd_select_neighbors(pfd_ctx* ctx, const float* centers, const int* tilekeys, int n_views, int mla_u_size,
+                                int mla_v_size, float pitch, const uint8_t* images, int mi_w, int mi_h, int max_nb,
+                                int* nb_ids, int* nb_counts);
+
 /* ---- micro-lens centres -------------------------------------------------
  * DepthSolver::ComputeMLACentersFromWhiteImage (DepthSolver.cpp:710-870) on the
  * device: the reference's Otsu threshold (:486-546, which histograms the first W

@@ -234,6 +234,14 @@ int orc_mla_centers(const uint8_t* bgr, int W, int H, int step, float baseline, 
                     int* out_col, int* out_row, float* out_cx, float* out_cy, float* out_area, int* out_abandon,
                     int max_out, int* threshold_out);
 
+/* Matching-neighbour lists, SelectNeighbors::CollectMIANeighImagesForMatch
+ * (MINeighbor/SelectNeighbors.cpp:113-193) with MISimilarityMeasure::MeasureSimilarity
+ * and MLA_Problem's RANSAC outlier test (oracle/select.cpp). */
+int orc_similarity(const uint8_t* src_bin, const uint8_t* nb_bin, int W, int H, float dx, float dy);
+int orc_select_neighbors(int n_views, const float* centers, const int* tilekeys, int u_size, int v_size, float pitch,
+                         const uint8_t* images, int mi_w, int mi_h, int max_out, int* nb_ids, int* nb_counts,
+                         float* nb_sim);
+
 /* Virtual-to-real depth (FocalStack/LFRefocus.cpp:2515-2593,
  * FocalStack/VirtualToRealDepthFunc.cpp:3390-3450), FP64. */
 float orc_vd_to_rd(float v_depth, const double c[3]);

@@ -125,6 +125,8 @@ def lib() -> ctypes.CDLL:
         L.orc_pm_sweep_taps.argtypes = [ctypes.POINTER(OrcFrame), ctypes.POINTER(OrcParams), ctypes.c_uint64, _I, _I,
                                         ctypes.POINTER(OrcState), ctypes.POINTER(OrcState), _I]
         L.orc_pm_sweep_taps.restype = ctypes.c_longlong
+        L.orc_similarity.argtypes = [_P, _P, _I, _I, _F, _F]
+        L.orc_select_neighbors.argtypes = [_I, _P, _P, _I, _I, _F, _P, _I, _I, _I, _P, _P, _P]
         L.orc_mla_otsu.argtypes = [_P, _I, _I, _I]
         L.orc_mla_contours.argtypes = [_P, _I, _I, _I, _I, _P, _P, _P, _I]
         L.orc_mla_centers.argtypes = [_P, _I, _I, _I, _F, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P]
@@ -322,6 +324,29 @@ def fuse_virtual_depth(orc: "Oracle", plane, lists, list_counts, is_ref, raw_w: 
                                      ctypes.byref(prm), raw_w, raw_h, _p(vd), _p(cf), _p(aif), _p(pts))
     assert n >= 0
     return vd, cf, aif, pts[:n]
+
+
+def similarity(src_bin, nb_bin, dx: float, dy: float) -> int:
+    """MISimilarityMeasure::MeasureSimilarity on two binary (0/255) images."""
+    a = np.ascontiguousarray(src_bin, np.uint8)
+    b = np.ascontiguousarray(nb_bin, np.uint8)
+    return int(lib().orc_similarity(_p(a), _p(b), a.shape[1], a.shape[0], dx, dy))
+
+
+def select_neighbors(centers, tilekeys, u_size: int, v_size: int, pitch: float, images=None, max_out: int = 128):
+    """m_NeighsSortVecForMatch per view: (ids [V][max_out], counts [V], similarity [V][max_out])."""
+    c = np.ascontiguousarray(centers, np.float32)
+    k = np.ascontiguousarray(tilekeys, np.int32)
+    V = c.shape[0]
+    im = None if images is None else np.ascontiguousarray(images, np.uint8)
+    mh, mw = (im.shape[1], im.shape[2]) if im is not None else (0, 0)
+    ids = np.full((V, max_out), -1, np.int32)
+    cnt = np.zeros(V, np.int32)
+    sim = np.zeros((V, max_out), np.float32)
+    rc = lib().orc_select_neighbors(V, _p(c), _p(k), u_size, v_size, pitch, _p(im), mw, mh, max_out, _p(ids), _p(cnt),
+                                    _p(sim))
+    assert rc == 0
+    return ids, cnt, sim
 
 
 def _bgr(img):

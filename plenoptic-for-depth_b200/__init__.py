@@ -207,6 +207,7 @@ def lib() -> ctypes.CDLL:
             "pfd_cycle_check": [_P, _I, ctypes.POINTER(CycleCfgC), _F, ctypes.POINTER(CycleStatsC), _P, _P, _P],
             "pfd_cycle_check_stats": [_P, _I, ctypes.POINTER(CycleStatsC)],
             "pfd_mla_lattice_fit": [_P, _P, _I, _I, _P],
+            "pfd_select_neighbors": [_P, _P, _P, _I, _I, _I, _F, _P, _I, _I, _I, _P, _P],
             "pfd_mla_centers": [_P, _P, _I, _I, _I, _F, _I, _I, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
             "pfd_fuse_virtual_depth": [_P, _I, ctypes.POINTER(FuseParamsC), _P, _P, _I, _P, _P, _P, _P, _P, _P,
                                        ctypes.POINTER(ctypes.c_longlong)],
@@ -482,6 +483,21 @@ class Context:
         self._check(self._L.pfd_reprojection_error(self._h, fid, ctypes.byref(c), float(baseline_unit), _ptr(err)),
                     "pfd_reprojection_error")
         return err
+
+    def select_neighbors(self, centers, tilekeys, mla_u_size: int, mla_v_size: int, pitch: float, images,
+                         max_nb: int = 128):
+        """SelectNeighbors::CollectMIANeighImagesForMatch with the device
+        similarities: (nb_ids [V][max_nb], nb_counts [V])."""
+        c = np.ascontiguousarray(centers, np.float32)
+        k = np.ascontiguousarray(tilekeys, np.int32)
+        im = np.ascontiguousarray(images, np.uint8)
+        V = c.shape[0]
+        ids = np.full((V, max_nb), -1, np.int32)
+        cnt = np.zeros(V, np.int32)
+        self._check(self._L.pfd_select_neighbors(self._h, _ptr(c), _ptr(k), V, mla_u_size, mla_v_size, float(pitch),
+                                                 _ptr(im), im.shape[2], im.shape[1], max_nb, _ptr(ids), _ptr(cnt)),
+                    "pfd_select_neighbors")
+        return ids, cnt
 
     def mla_centers(self, white, baseline: float, mla_u_size: int, mla_v_size: int):
         """DepthSolver::ComputeMLACentersFromWhiteImage on a white image (H x W x 3

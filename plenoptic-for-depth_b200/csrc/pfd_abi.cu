@@ -21,6 +21,8 @@
 #include "vdrd_kernels.h"
 #include "fuse_kernels.h"
 #include "mla_kernels.h"
+#include "neighbors.h"
+#include "select_kernels.h"
 
 namespace {
 
@@ -1312,6 +1314,72 @@ pfd_status pfd_fuse_virtual_depth(pfd_ctx* ctx, int frame_id, const pfd_fuse_par
         }
     }
     if (vd_map || conf || aif || points || n_points) return check_device_error(ctx);
+    return PFD_OK;
+}
+
+// ---- matching-neighbour selection ---------------------------------------------
+
+pfd_status pfd_select_neighbors(pfd_ctx* ctx, const float* centers, const int* tilekeys, int n_views, int mla_u_size,
+                                int mla_v_size, float pitch, const uint8_t* images, int mi_w, int mi_h, int max_nb,
+                                int* nb_ids, int* nb_counts)
+{
+    if (!ctx) return PFD_EINVAL;
+    if (!centers || !tilekeys || !images || !nb_ids || !nb_counts || n_views < 1)
+        return fail(ctx, PFD_EINVAL, "select_neighbors: NULL argument or no views");
+    if (!(pitch > 0.0f) || mi_w < 2 || mi_h < 2 || mi_w > 64 || mi_h > 64 || max_nb < 1 || max_nb > 128)
+        return fail(ctx, PFD_EINVAL, "select_neighbors: bad pitch, window or max_nb");
+    if (mla_u_size < 1 || mla_v_size < 1 || (long long)mla_u_size * mla_v_size > (1LL << 28))
+        return fail(ctx, PFD_EINVAL, "select_neighbors: bad lens grid %d x %d", mla_u_size, mla_v_size);
+    pfd::LensGrid G;
+    if (!G.build(centers, tilekeys, n_views, mla_u_size, mla_v_size))
+        return fail(ctx, PFD_EINVAL, "select_neighbors: a tile key lies outside the grid or is repeated");
+    std::vector<std::vector<std::vector<int>>> R;
+    pfd::collect_rings(G, pitch, 5, R);
+    // every candidate of every ring: the search may stop early, the similarities are cheap
+    std::vector<int2> pairs;
+    std::vector<size_t> first((size_t)n_views * 5 + 1, 0);
+    for (int v = 0; v < n_views; ++v)
+        for (int k = 0; k < 5; ++k) {
+            first[(size_t)v * 5 + k] = pairs.size();
+            for (int n : R[v][k]) pairs.push_back(make_int2(v, n));
+        }
+    first[(size_t)n_views * 5] = pairs.size();
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const size_t ppv = (size_t)mi_w * mi_h;
+    std::vector<int> sims(pairs.size());
+    uint8_t* d_img = nullptr;
+    float2* d_c = nullptr;
+    int2* d_pairs = nullptr;
+    int* d_out = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&d_img, ppv * n_views, s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_c, sizeof(float2) * n_views, s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_pairs, sizeof(int2) * std::max<size_t>(pairs.size(), 1), s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_out, sizeof(int) * std::max<size_t>(pairs.size(), 1), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_img, images, ppv * n_views, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_c, centers, sizeof(float2) * n_views, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && !pairs.empty())
+        e = cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = pfd::launch_similarity(d_img, (int)ppv, mi_w, mi_h, d_c, d_pairs, (int)pairs.size(), d_out, s);
+    if (e == cudaSuccess && !pairs.empty())
+        e = cudaMemcpyAsync(sims.data(), d_out, sizeof(int) * pairs.size(), cudaMemcpyDeviceToHost, s);
+    for (void* q : { (void*)d_img, (void*)d_c, (void*)d_pairs, (void*)d_out })
+        if (q) cudaFreeAsync(q, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, PFD_ECUDA, "select_neighbors: %s", cudaGetErrorString(e));
+    }
+    ctx->launches += 1;
+    std::vector<int> list;
+    for (int v = 0; v < n_views; ++v) {
+        auto sim = [&](int ring, int i) { return (float)(double)sims[first[(size_t)v * 5 + ring] + i]; };
+        pfd::select_for_view(G, pitch, v, R[v], sim, list);
+        const int n = std::min((int)list.size(), max_nb);
+        for (int k = 0; k < max_nb; ++k) nb_ids[(size_t)v * max_nb + k] = k < n ? list[k] : -1;
+        nb_counts[v] = n;
+    }
     return PFD_OK;
 }
 
