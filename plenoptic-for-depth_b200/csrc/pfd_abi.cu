@@ -129,10 +129,12 @@ pfd_status frame_alloc(pfd_ctx* ctx, Frame& f, void** p, size_t bytes)
     if (ctx->budget && ctx->used + pending + bytes > ctx->budget)
         return fail(ctx, PFD_ENOMEM, "HBM budget exceeded: %zu in use + %zu requested > %zu",
                     ctx->used + pending, bytes, ctx->budget);
-    cudaError_t e = cudaMalloc(p, bytes);
+    // stream-ordered: no device-wide synchronisation, so frames of other contexts
+    // (other streams) keep running while this one allocates or frees
+    cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return fail(ctx, PFD_ENOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+        return fail(ctx, PFD_ENOMEM, "cudaMallocAsync(%zu): %s", bytes, cudaGetErrorString(e));
     }
     f.allocs.push_back(*p);
     f.bytes += bytes;
@@ -144,17 +146,16 @@ pfd_status frame_alloc(pfd_ctx* ctx, Frame& f, void** p, size_t bytes)
 void frame_free_one(pfd_ctx* ctx, Frame& f, void* p, size_t bytes)
 {
     if (!p) return;
-    cudaStreamSynchronize(ctx->stream);
-    cudaFree(p);
+    cudaFreeAsync(p, ctx->stream);
     for (size_t i = 0; i < f.allocs.size(); ++i)
         if (f.allocs[i] == p) { f.allocs.erase(f.allocs.begin() + (long)i); break; }
     f.bytes -= bytes;
     if (f.registered) ctx->used -= bytes;
 }
 
-void frame_release(Frame& f)
+void frame_release(Frame& f, cudaStream_t s)
 {
-    for (void* p : f.allocs) cudaFree(p);
+    for (void* p : f.allocs) cudaFreeAsync(p, s);
     f.allocs.clear();
     f.bytes = 0;
 }
@@ -274,6 +275,17 @@ pfd_status pfd_create(pfd_ctx** out, int device, size_t hbm_budget_bytes)
     ctx = new (std::nothrow) pfd_ctx;
     if (!ctx) return PFD_ENOMEM;
     ctx->device = device;
+    {
+        // frames come and go with every request: keep their memory in this process's
+        // pool instead of handing it back to the driver at each synchronisation
+        DeviceGuard g0(device);
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
     ctx->budget = hbm_budget_bytes;
     DeviceGuard g(device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -297,8 +309,9 @@ void pfd_destroy(pfd_ctx* ctx)
     if (!ctx) return;
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (auto& kv : ctx->frames) frame_release(kv.second);
+    for (auto& kv : ctx->frames) frame_release(kv.second, ctx->stream);
     ctx->frames.clear();
+    cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->d_err);
     cudaFree(ctx->d_taps);
     if (ctx->d_scratch) cudaFree(ctx->d_scratch);
@@ -406,7 +419,7 @@ pfd_status pfd_frame_create(pfd_ctx* ctx, int* frame_id, int W, int H, const flo
         A((void**)&f.s[b].disp, sizeof(float4) * px);
         A((void**)&f.s[b].sel, sizeof(uint32_t) * px);
     }
-    if (st != PFD_OK) { frame_release(f); return st; }
+    if (st != PFD_OK) { frame_release(f, ctx->stream); return st; }
     cudaStream_t s = ctx->stream;
     auto H2D = [&](void* d, const void* h, size_t b) {
         if (st == PFD_OK && cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, s) != cudaSuccess) st = PFD_ECUDA;
@@ -428,7 +441,7 @@ pfd_status pfd_frame_create(pfd_ctx* ctx, int* frame_id, int W, int H, const flo
     }
     if (st != PFD_OK) {
         cudaGetLastError();
-        frame_release(f);
+        frame_release(f, ctx->stream);
         return fail(ctx, st, "frame_create: upload failed");
     }
     f.h_keys.assign(tilekeys, tilekeys + 2 * (size_t)n_views);
@@ -532,9 +545,8 @@ pfd_status pfd_frame_free(pfd_ctx* ctx, int frame_id)
     auto it = ctx->frames.find(frame_id);
     if (it == ctx->frames.end()) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
     DeviceGuard g(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
     ctx->used -= it->second.bytes;
-    frame_release(it->second);
+    frame_release(it->second, ctx->stream);           // ordered after the frame's queued work
     ctx->frames.erase(it);
     return PFD_OK;
 }
@@ -1600,6 +1612,33 @@ pfd_status pfd_mla_lattice_fit(pfd_ctx* ctx, const pfd_mla_lens* lenses, int n, 
     fit[4] = std::sqrt(ss / (double)use.size());
     fit[5] = (double)use.size();
     return PFD_OK;
+}
+
+pfd_status pfd_download_async(pfd_ctx* ctx, int frame_id, float* plane, float* cost, float* disp, uint32_t* sel)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "download before PatchMatch");
+    DeviceGuard g(ctx->device);
+    const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
+    const pfd::StateDev& s = f->s[f->cur];
+    if (plane) CU(cudaMemcpyAsync(plane, s.plane, sizeof(float4) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (cost) CU(cudaMemcpyAsync(cost, s.cost, sizeof(float) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (disp) CU(cudaMemcpyAsync(disp, s.disp, sizeof(float4) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    if (sel) CU(cudaMemcpyAsync(sel, s.sel, sizeof(uint32_t) * px, cudaMemcpyDeviceToHost, ctx->stream));
+    return PFD_OK;
+}
+
+size_t pfd_frame_bytes(int W, int H, int n_views, int mi_w, int mi_h, int max_nb, int has_blur)
+{
+    if (W < 1 || H < 1 || n_views < 1 || mi_w < 1 || mi_h < 1 || max_nb < 1) return 0;
+    const size_t V = (size_t)n_views, px = V * mi_w * mi_h, tiles = V * (((size_t)mi_w * mi_h + 15) & ~(size_t)15);
+    size_t b = (size_t)W * H + tiles * (has_blur ? 2 : 1) + 3 * sizeof(int2) * V + sizeof(int) * V * (max_nb + 1);
+    b += sizeof(float) * px * max_nb;                              // stored cost vectors
+    b += 2 * (sizeof(float4) + sizeof(float) + sizeof(float4) + sizeof(uint32_t)) * px;   // ping-pong state
+    b += px + sizeof(int) * V;                                     // filter reasons and schedule
+    return b;
 }
 
 pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane, float* cost, float* disp, uint32_t* sel)
