@@ -314,7 +314,8 @@ void pfd_destroy(pfd_ctx* ctx)
     cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->d_err);
     cudaFree(ctx->d_taps);
-    if (ctx->d_scratch) cudaFree(ctx->d_scratch);
+    if (ctx->d_scratch) cudaFreeAsync(ctx->d_scratch, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -592,14 +593,14 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
     if (need > ctx->scratch_bytes) {
         if (ctx->budget && ctx->used - ctx->scratch_bytes + need > ctx->budget)
             return fail(ctx, PFD_ENOMEM, "HBM budget exceeded by %zu bytes of sweep scratch", need);
-        CU(cudaStreamSynchronize(ctx->stream));
-        if (ctx->d_scratch) cudaFree(ctx->d_scratch);
+        // stream-ordered, like the frames: other contexts' work keeps running
+        if (ctx->d_scratch) cudaFreeAsync(ctx->d_scratch, ctx->stream);
         ctx->used -= ctx->scratch_bytes;
         ctx->d_scratch = nullptr;
         ctx->scratch_bytes = 0;
-        if (cudaMalloc(&ctx->d_scratch, need) != cudaSuccess) {
+        if (cudaMallocAsync((void**)&ctx->d_scratch, need, ctx->stream) != cudaSuccess) {
             cudaGetLastError();
-            return fail(ctx, PFD_ENOMEM, "cudaMalloc(%zu) for sweep scratch failed", need);
+            return fail(ctx, PFD_ENOMEM, "cudaMallocAsync(%zu) for sweep scratch failed", need);
         }
         ctx->scratch_bytes = need;
         ctx->used += need;
