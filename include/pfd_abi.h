@@ -116,6 +116,20 @@ pfd_status pfd_frame_set_raw_device(pfd_ctx* ctx, int frame_id, const uint8_t* r
  * views in frame order.  The frame then has no raw image (pfd_refocus needs one).
  * Returns when the host buffer may be reused. */
 pfd_status pfd_frame_set_micro_images(pfd_ctx* ctx, int frame_id, const uint8_t* images);
+/* The blur channel computed on the device from the frame's raw image:
+ * ImageQualityEstimate::QuantizeBlurByLaplacian (Util/ImageQualityEstimate.cpp:
+ * 211-230) then DepthSolver::SliceAndIndicatlizeForMI (DepthSolver.cpp:
+ * 2709-2754).  Every view's blur tile becomes the raw frame's Laplacian (ksize
+ * 1, borders reflected without repeating the edge) over its window, saturated
+ * to 8 bits (MLA_Problem::m_Image_Blureness); it replaces any blur channel given
+ * to pfd_frame_create, and the frame's costs carry the blur penalty from then
+ * on.  blur_out [n_views][mi_h][mi_w] (may be NULL) receives the channel;
+ * blureness [n_views] (may be NULL) MLA_Problem::m_BlurenessValue, the window's
+ * pixels whose Laplacian exceeds 10 (ComputeBlurenessValue,
+ * MVStereo/LFDepthInfo.cpp:65-83).  With either output the call waits for the
+ * device.  Needs a raw frame (pfd_frame_set_raw); the PatchMatch state must be
+ * initialised again afterwards. */
+pfd_status pfd_frame_compute_blur(pfd_ctx* ctx, int frame_id, uint8_t* blur_out, uint32_t* blureness);
 /* pfd_frame_create + pfd_frame_set_raw. */
 pfd_status pfd_frame_upload(pfd_ctx* ctx, int* frame_id, const uint8_t* raw, int W, int H, int raw_pitch,
                             const float* centers, const int* tilekeys, int n_views,
@@ -152,6 +166,20 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
  * the GPU, from other streams or other contexts, race and corrupt each other. */
 pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed,
                                 int iter, int phase);
+
+/* How the NCC moments are accumulated by the context's later pfd_pm_init,
+ * pfd_pm_sweep(_noalloc), pfd_patchmatch and pfd_ncc_costs calls.
+ * PFD_NCC_REFERENCE (the default): the reference's FP32 sums of w r, w r^2,
+ * w s, w s^2 and w r s (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:110-174),
+ * bit for bit; their variances E[r^2] - E[r]^2 lose digits to cancellation on
+ * patches of low contrast.  PFD_NCC_SHIFTED: the same FP32 sums of the texels
+ * and samples minus the patch's centre texel (exact subtractions: both are
+ * multiples of 1/256 below 2^16); the NCC is unchanged in exact arithmetic
+ * and its FP32 error against an FP64 evaluation is far smaller.  Not in the
+ * reference: results differ from its bits. */
+#define PFD_NCC_REFERENCE 0
+#define PFD_NCC_SHIFTED   1
+pfd_status pfd_set_ncc_moments(pfd_ctx* ctx, int mode);
 
 /* Per-hypothesis cost vectors: ComputeMultiViewCostVector_Frame
  * (AdaptMIPMFrame.cu:181-225) for n (view, pixel, plane) hypotheses.

@@ -127,6 +127,9 @@ static float ncc_frame(const orc_frame* f, const orc_params* p, int vid, int nvi
 
     float s_r = 0.0f, s_rr = 0.0f, s_s = 0.0f, s_ss = 0.0f, s_rs = 0.0f, s_w = 0.0f;
     const float rc = R[py * W + px];
+    /* shifted moments (not in the reference): texels and samples minus the
+     * centre texel, exact subtractions; shift 0 is the reference's sums */
+    const float sh = p->shifted ? rc : 0.0f;
     const float ss2 = (2.0f * p->sigma_spatial) * p->sigma_spatial;
     const float cc2 = (2.0f * p->sigma_color) * p->sigma_color;
 
@@ -141,7 +144,7 @@ static float ncc_frame(const orc_frame* f, const orc_params* p, int vid, int nvi
             if (!(sx >= 0.0f && sx < (float)W && sy >= 0.0f && sy < (float)H)) continue;
             if (taps) ++*taps;
             const float r = R[yr * W + xr];
-            const float s = canon_tex_fetch(S, W, H, sx, sy);
+            const float s = canon_tex_fetch(S, W, H, sx, sy) - sh;
             if (RB) {
                 *blur_x += RB[yr * W + xr] / 255.0f;
                 *blur_y += canon_tex_fetch(SB, W, H, sx, sy) / 255.0f;
@@ -150,10 +153,11 @@ static float ncc_frame(const orc_frame* f, const orc_params* p, int vid, int nvi
             const float sd = sqrtf(fmaf(fj, fj, fi * fi));
             const float cd = fabsf(r - rc);
             const float w = canon_expf((-sd) / ss2 - cd / cc2);
-            const float wr = w * r;
+            const float rs = r - sh;
+            const float wr = w * rs;
             const float ws = w * s;
-            s_r  = fmaf(w, r, s_r);
-            s_rr = fmaf(wr, r, s_rr);
+            s_r  = fmaf(w, rs, s_r);
+            s_rr = fmaf(wr, rs, s_rr);
             s_s  = fmaf(w, s, s_s);
             s_ss = fmaf(ws, s, s_ss);
             s_rs = fmaf(wr, s, s_rs);
@@ -804,7 +808,28 @@ static double tex_exact(const float* img, int W, int H, double sx, double sy)
     return (1 - ax) * (1 - ay) * t00 + ax * (1 - ay) * t10 + (1 - ax) * ay * t01 + ax * ay * t11;
 }
 
-double orc_ncc_fp64(const orc_frame* f, const orc_params* p, int vid, int k, int px, int py, const float* plane)
+/* The texture's own sampling in double: the sample point rounded to 1/256 of a
+ * texel and the 8-bit bilinear weights of canon_tex_fetch, so the only
+ * difference from the device is the arithmetic. */
+static double tex_quantised(const float* img, int W, int H, double sx, double sy)
+{
+    const int qx = (int)floor((sx + 0.5) * 256.0 - 127.5);
+    const int qy = (int)floor((sy + 0.5) * 256.0 - 127.5);
+    int ix = qx >> 8, iy = qy >> 8;
+    const int a = qx & 255, b = qy & 255;
+    int ix1 = ix + 1, iy1 = iy + 1;
+    if (ix < 0) ix = 0; if (ix > W - 1) ix = W - 1;
+    if (iy < 0) iy = 0; if (iy > H - 1) iy = H - 1;
+    if (ix1 < 0) ix1 = 0; if (ix1 > W - 1) ix1 = W - 1;
+    if (iy1 < 0) iy1 = 0; if (iy1 > H - 1) iy1 = H - 1;
+    const int w11 = (a * b + 128) >> 8;
+    const int w10 = a - w11, w01 = b - w11, w00 = 256 - a - b + w11;
+    return (w00 * (double)img[iy * W + ix] + w10 * (double)img[iy * W + ix1] + w01 * (double)img[iy1 * W + ix] +
+            w11 * (double)img[iy1 * W + ix1]) / 256.0;
+}
+
+static double ncc_fp64(const orc_frame* f, const orc_params* p, int vid, int k, int px, int py, const float* plane,
+                       int sampling)
 {
     const int W = f->mi_w, H = f->mi_h;
     const long ppv = (long)W * H;
@@ -819,7 +844,19 @@ double orc_ncc_fp64(const orc_frame* f, const orc_params* p, int vid, int k, int
     const double d0 = A * px + B * py + C;
     const double stx = (c0x - c1x) / p->base, sty = (c0y - c1y) / p->base;
     const double ax = px + stx * d0, ay = py + sty * d0;
-    if (!(ax >= 0 && ax < W && ay >= 0 && ay < H)) return 2.0;
+    /* sampling 2: the FP32 path's anchor, tap disparities and sample points */
+    const f4 h = mk4(plane[0], plane[1], plane[2], plane[3]);
+    const f3 dpf = disparity_plane(px, py, h);
+    const float stxf = (f->centers[2 * vid] - f->centers[2 * nvid]) * (1.0f / fmaxf(p->base, 1e-6f));
+    const float styf = (f->centers[2 * vid + 1] - f->centers[2 * nvid + 1]) * (1.0f / fmaxf(p->base, 1e-6f));
+    if (sampling == 2) {
+        float axf, ayf;
+        f4 db;
+        geo_map_hex(f->centers + 2 * vid, f->centers + 2 * nvid, px, py, h, px, py, p->base, &axf, &ayf, &db);
+        if (!(axf >= 0.0f && axf < (float)W && ayf >= 0.0f && ayf < (float)H)) return 2.0;
+    } else if (!(ax >= 0 && ax < W && ay >= 0 && ay < H)) {
+        return 2.0;
+    }
     const int radius = p->patch_size / 2;
     const double rc = R[py * W + px];
     const double ss2 = 2.0 * p->sigma_spatial * p->sigma_spatial, cc2 = 2.0 * p->sigma_color * p->sigma_color;
@@ -828,11 +865,19 @@ double orc_ncc_fp64(const orc_frame* f, const orc_params* p, int vid, int k, int
         for (int j = -radius; j <= radius; j += p->radius_increment) {
             const int xr = px + i, yr = py + j;
             if (xr < 0 || xr >= W || yr < 0 || yr >= H) continue;
-            const double d = A * xr + B * yr + C;
-            const double sx = xr + stx * d, sy = yr + sty * d;
-            if (!(sx >= 0 && sx < W && sy >= 0 && sy < H)) continue;
+            double sx, sy;
+            if (sampling == 2) {
+                const float d = fmaf(dpf.y, (float)yr, dpf.x * (float)xr) + dpf.z;
+                const float fx = fmaf(stxf, d, (float)xr), fy = fmaf(styf, d, (float)yr);
+                if (!(fx >= 0.0f && fx < (float)W && fy >= 0.0f && fy < (float)H)) continue;
+                sx = fx; sy = fy;
+            } else {
+                const double d = A * xr + B * yr + C;
+                sx = xr + stx * d; sy = yr + sty * d;
+                if (!(sx >= 0 && sx < W && sy >= 0 && sy < H)) continue;
+            }
             const double r = R[yr * W + xr];
-            const double s = tex_exact(S, W, H, sx, sy);
+            const double s = sampling ? tex_quantised(S, W, H, sx, sy) : tex_exact(S, W, H, sx, sy);
             const double wgt = exp(-sqrt((double)(i * i + j * j)) / ss2 - fabs(r - rc) / cc2);
             s_r += wgt * r; s_rr += wgt * r * r; s_s += wgt * s; s_ss += wgt * s * s; s_rs += wgt * r * s; s_w += wgt;
         }
@@ -842,6 +887,25 @@ double orc_ncc_fp64(const orc_frame* f, const orc_params* p, int vid, int k, int
     if (vr < 1e-5 || vs < 1e-5) return 2.0;
     const double c = 1.0 - (s_rs / s_w - mr * ms) / sqrt(vr * vs);
     return c < 0 ? 0 : (c > 2 ? 2 : c);
+}
+
+double orc_ncc_fp64(const orc_frame* f, const orc_params* p, int vid, int k, int px, int py, const float* plane)
+{
+    return ncc_fp64(f, p, vid, k, px, py, plane, 0);
+}
+
+void orc_ncc_fp64_batch(const orc_frame* f, const orc_params* p, const int* vids, const int* pxy,
+                        const float* planes, int n, int sampling, int nthreads, double* out)
+{
+    const int K = f->max_nb;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int h = 0; h < n; ++h)
+        for (int k = 0; k < K; ++k)
+            out[(long)h * K + k] = k < f->nb_counts[vids[h]]
+                                       ? ncc_fp64(f, p, vids[h], k, pxy[2 * h], pxy[2 * h + 1], planes + 4 * (long)h,
+                                                  sampling)
+                                       : 2.0;
 }
 
 /* ------------------------------------------------------------------------ */

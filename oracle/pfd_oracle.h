@@ -50,6 +50,7 @@ typedef struct {
     float depth_min;
     float depth_max;
     float base;                  /* Base: lens pitch in pixels (AdaptMIPMFrame.cpp:138) */
+    int shifted;                 /* 0: the reference's NCC moments; 1: moments of (texel - centre texel) */
 } orc_params;
 
 /* Per-pixel state, the four ping-pong buffers of AdaptMIPMFrame
@@ -71,6 +72,15 @@ int orc_cost_vectors(const orc_frame* f, const orc_params* p, const int* vids, c
  * bilinear sampling: the precision oracle. */
 double orc_ncc_fp64(const orc_frame* f, const orc_params* p, int vid, int k, int px, int py,
                     const float* plane);
+/* orc_ncc_fp64 for n hypotheses and all max_nb neighbours (2.0 past a view's
+ * count) into out [n][max_nb].  sampling 0: exact bilinear at sample points
+ * computed in double; 1: the texture's own sampling (point rounded to 1/256
+ * texel, 8-bit weights) at those points, in double; 2: the texture's sampling
+ * at the FP32 path's own anchor and sample points (canonical float
+ * arithmetic), everything after the sample in double, which leaves the
+ * accumulation of the weights and moments as the only difference from FP32. */
+void orc_ncc_fp64_batch(const orc_frame* f, const orc_params* p, const int* vids, const int* pxy,
+                        const float* planes, int n, int sampling, int nthreads, double* out);
 
 /* RandomInitializationForFrame (AdaptMIPMFrame.cu:474-518) over all pixels. */
 int orc_pm_init(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int nthreads);
@@ -259,6 +269,15 @@ void  orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
  * for the hypotheses given (the algorithmic unit of the roofline). */
 long long orc_count_taps(const orc_frame* f, const orc_params* p, const int* vids, const int* pxy,
                          const float* planes, int n);
+
+/* Blur channel (oracle/blur.c).  orc_laplacian: cv::Laplacian(gray, CV_32F),
+ * ksize 1, into score [H][W].  orc_blur_tiles: every view's window (origin
+ * [V][2]) of the saturated score into tiles [V][mi_h][mi_w], and in counts [V]
+ * (may be NULL) the window's pixels with score > 10.  Returns 0, or -1 for a
+ * window outside the frame. */
+void orc_laplacian(const uint8_t* gray, int W, int H, int pitch, float* score);
+int orc_blur_tiles(const uint8_t* gray, int W, int H, int pitch, const int* origin, int V, int mi_w, int mi_h,
+                   uint8_t* tiles, uint32_t* counts);
 
 #ifdef __cplusplus
 }

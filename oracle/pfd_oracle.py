@@ -27,7 +27,8 @@ class OrcFrame(ctypes.Structure):
 
 class OrcParams(ctypes.Structure):
     _fields_ = [("max_iterations", _I), ("patch_size", _I), ("radius_increment", _I), ("top_k", _I),
-                ("sigma_spatial", _F), ("sigma_color", _F), ("depth_min", _F), ("depth_max", _F), ("base", _F)]
+                ("sigma_spatial", _F), ("sigma_color", _F), ("depth_min", _F), ("depth_max", _F), ("base", _F),
+                ("shifted", _I)]
 
 
 class OrcFilterCfg(ctypes.Structure):
@@ -91,6 +92,7 @@ def lib() -> ctypes.CDLL:
         L.orc_count_taps.restype = ctypes.c_longlong
         L.orc_ncc_fp64.argtypes = [FP, PP, _I, _I, _I, _I, _P]
         L.orc_ncc_fp64.restype = ctypes.c_double
+        L.orc_ncc_fp64_batch.argtypes = [FP, PP, _P, _P, _P, _I, _I, _I, _P]
         L.orc_pm_init.argtypes = [FP, PP, ctypes.c_uint64, SP, _I]
         L.orc_pm_init_views.argtypes = [FP, PP, ctypes.c_uint64, SP, _I, _I, _I]
         L.orc_pm_sweep.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I]
@@ -130,6 +132,8 @@ def lib() -> ctypes.CDLL:
         L.orc_mla_otsu.argtypes = [_P, _I, _I, _I]
         L.orc_mla_contours.argtypes = [_P, _I, _I, _I, _I, _P, _P, _P, _I]
         L.orc_mla_centers.argtypes = [_P, _I, _I, _I, _F, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P]
+        L.orc_laplacian.argtypes = [_P, _I, _I, _I, _P]
+        L.orc_blur_tiles.argtypes = [_P, _I, _I, _I, _P, _I, _I, _I, _P, _P]
         _lib = L
     return _lib
 
@@ -141,7 +145,8 @@ def _p(a):
 class Oracle:
     """One frame of views for the oracle.  gray: [V][h][w] uint8/float."""
 
-    def __init__(self, gray, centers, nb_ids, nb_counts, blur=None):
+    def __init__(self, gray, centers, nb_ids, nb_counts, blur=None, shifted=False):
+        self.shifted = bool(shifted)     # NCC moments of (texel - centre texel) instead of the reference's
         self.gray = np.ascontiguousarray(gray, dtype=np.float32)
         self.blur = None if blur is None else np.ascontiguousarray(blur, dtype=np.float32)
         self.centers = np.ascontiguousarray(centers, dtype=np.float32)
@@ -153,12 +158,11 @@ class Oracle:
         self.f = OrcFrame(V, w, h, self.K, _p(self.gray), _p(self.blur), _p(self.centers), _p(self.nb_ids),
                           _p(self.nb_counts))
 
-    @staticmethod
-    def params(p) -> OrcParams:
-        """From the package's PmParams (same fields)."""
+    def params(self, p) -> OrcParams:
+        """From the package's PmParams (same fields) and the oracle's moment mode."""
         c = p.c()
         return OrcParams(c.max_iterations, c.patch_size, c.radius_increment, c.top_k, c.sigma_spatial, c.sigma_color,
-                         c.depth_min, c.depth_max, c.base)
+                         c.depth_min, c.depth_max, c.base, 1 if self.shifted else 0)
 
     def new_state(self):
         n = self.V * self.h * self.w
@@ -190,6 +194,18 @@ class Oracle:
         pl = np.ascontiguousarray(plane, np.float32)
         p = self.params(params)
         return float(lib().orc_ncc_fp64(ctypes.byref(self.f), ctypes.byref(p), vid, k, px, py, _p(pl)))
+
+    def ncc_fp64_batch(self, params, vids, pxy, planes, sampling=0, nthreads=0) -> np.ndarray:
+        """[n][max_nb] FP64 NCC costs (sampling 0: exact bilinear; 1: the texture's
+        quantised sampling)."""
+        p = self.params(params)
+        v = np.ascontiguousarray(vids, np.int32)
+        q = np.ascontiguousarray(pxy, np.int32)
+        pl = np.ascontiguousarray(planes, np.float32)
+        out = np.zeros((len(v), self.K), np.float64)
+        lib().orc_ncc_fp64_batch(ctypes.byref(self.f), ctypes.byref(p), _p(v), _p(q), _p(pl), len(v), sampling,
+                                 nthreads, _p(out))
+        return out
 
     def init(self, params, seed, nthreads=0, views=None):
         arr, st = self.new_state()
@@ -388,6 +404,36 @@ def mla_centers(img, baseline: float, mla_u_size: int, mla_v_size: int):
                               _p(row), _p(cx), _p(cy), _p(ar), _p(ab), cap, ctypes.byref(t))
     assert n >= 0
     return dict(col=col[:n], row=row[:n], cx=cx[:n], cy=cy[:n], area=ar[:n], abandon=ab[:n]), t.value
+
+
+def laplacian(gray) -> np.ndarray:
+    """cv::Laplacian(gray, CV_32F) with ksize 1 (oracle/blur.c)."""
+    g = np.ascontiguousarray(gray, np.uint8)
+    out = np.zeros(g.shape, np.float32)
+    lib().orc_laplacian(_p(g), g.shape[1], g.shape[0], g.strides[0], _p(out))
+    return out
+
+
+def window_origins(centers, mi_w: int, mi_h: int) -> np.ndarray:
+    """Left-down corners of the matching windows: the centre minus (mi - 1) / 2 in
+    double, stored as float, truncated to int (DepthSolver.cpp:1894-1895, 1977-1978)."""
+    c = np.asarray(centers, np.float32).reshape(-1, 2).astype(np.float64)
+    ox = (c[:, 0] - (mi_w - 1) * 0.5).astype(np.float32)
+    oy = (c[:, 1] - (mi_h - 1) * 0.5).astype(np.float32)
+    return np.ascontiguousarray(np.stack([ox, oy], 1).astype(np.int32))
+
+
+def blur_tiles(gray, origins, mi_w: int, mi_h: int):
+    """Per-view blur channel [V][mi_h][mi_w] (u8) and blureness values [V] (oracle/blur.c)."""
+    g = np.ascontiguousarray(gray, np.uint8)
+    o = np.ascontiguousarray(origins, np.int32).reshape(-1, 2)
+    V = o.shape[0]
+    tiles = np.zeros((V, mi_h, mi_w), np.uint8)
+    counts = np.zeros(V, np.uint32)
+    rc = lib().orc_blur_tiles(_p(g), g.shape[1], g.shape[0], g.strides[0], _p(o), V, mi_w, mi_h, _p(tiles),
+                              _p(counts))
+    assert rc == 0, "window outside the frame"
+    return tiles, counts
 
 
 def vd_to_rd_points(vd, c):

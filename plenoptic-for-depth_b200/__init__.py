@@ -192,6 +192,8 @@ def lib() -> ctypes.CDLL:
             "pfd_frame_set_raw": [_P, _I, _P, _I],
             "pfd_frame_set_raw_device": [_P, _I, _P, _I],
             "pfd_frame_set_micro_images": [_P, _I, _P],
+            "pfd_frame_compute_blur": [_P, _I, _P, _P],
+            "pfd_set_ncc_moments": [_P, _I],
             "pfd_state_upload": [_P, _I, _P, _P, _P, _P],
             "pfd_frame_upload": [_P, ctypes.POINTER(_I), _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _I, _P],
             "pfd_frame_free": [_P, _I],
@@ -334,6 +336,19 @@ class Context:
             raise ValueError(f"micro-images must be {(f['V'], f['mi_h'], f['mi_w'])}, got {im.shape}")
         self._check(self._L.pfd_frame_set_micro_images(self._h, fid, _ptr(im)), "pfd_frame_set_micro_images")
 
+    def frame_compute_blur(self, fid: int, copy_back: bool = True):
+        """The blur channel from the frame's raw image, on the device
+        (pfd_frame_compute_blur).  Returns (tiles [V][mi_h][mi_w] u8, blureness
+        [V] u32) when copy_back, else None without waiting for the device."""
+        f = self._frames[fid]
+        if not copy_back:
+            self._check(self._L.pfd_frame_compute_blur(self._h, fid, None, None), "pfd_frame_compute_blur")
+            return None
+        tiles = np.zeros((f["V"], f["mi_h"], f["mi_w"]), np.uint8)
+        counts = np.zeros(f["V"], np.uint32)
+        self._check(self._L.pfd_frame_compute_blur(self._h, fid, _ptr(tiles), _ptr(counts)), "pfd_frame_compute_blur")
+        return tiles, counts
+
     def state_upload(self, fid: int, plane, cost, disp, sel) -> None:
         f = self._frames[fid]
         n = f["V"] * f["mi_w"] * f["mi_h"]
@@ -383,6 +398,12 @@ class Context:
         self._check(self._L.pfd_ncc_costs(self._h, fid, ctypes.byref(p), _ptr(v), _ptr(xy), _ptr(pl), v.shape[0],
                                           _ptr(out)), "pfd_ncc_costs")
         return out
+
+    def set_ncc_moments(self, shifted: bool) -> None:
+        """NCC moments of (texel - centre texel) (PFD_NCC_SHIFTED) or the
+        reference's raw moments (PFD_NCC_REFERENCE, the default) for the
+        context's later initialisations, sweeps and cost queries."""
+        self._check(self._L.pfd_set_ncc_moments(self._h, 1 if shifted else 0), "pfd_set_ncc_moments")
 
     def set_tap_counting(self, on: bool) -> None:
         self._check(self._L.pfd_set_tap_counting(self._h, 1 if on else 0), "pfd_set_tap_counting")

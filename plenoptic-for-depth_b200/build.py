@@ -23,7 +23,7 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "-ccbin", "/usr/bin/g++",
 ]
 
-CU_SOURCES = ["pm_kernels.cu", "pm_sweep.cu", "check_kernels.cu", "refocus_kernels.cu", "vdrd_kernels.cu", "fuse_kernels.cu", "mla_kernels.cu", "select_kernels.cu", "pfd_abi.cu", "diag.cu"]
+CU_SOURCES = ["pm_kernels.cu", "pm_sweep.cu", "check_kernels.cu", "refocus_kernels.cu", "vdrd_kernels.cu", "fuse_kernels.cu", "mla_kernels.cu", "select_kernels.cu", "blur_kernels.cu", "pfd_abi.cu", "diag.cu"]
 CPP_SOURCES = ["neighbors.cpp", "server.cpp"]
 SYNTH_LIB = os.path.join(OUT, "libpfd_synth.so")
 HOST_DIR = os.path.join(PKG_DIR, "host")

@@ -23,6 +23,7 @@
 #include "mla_kernels.h"
 #include "neighbors.h"
 #include "select_kernels.h"
+#include "blur_kernels.h"
 
 namespace {
 
@@ -48,6 +49,7 @@ struct Frame {
     float* d_cvec = nullptr;
     unsigned cvec_valid = 0;
     pfd_pm_params cvec_key = {};
+    int cvec_moments = PFD_NCC_REFERENCE;     // the NCC moments cvec was computed with
     bool has_state = false;
     size_t bytes = 0;
     bool registered = false;          // bytes already counted in the context's total
@@ -83,6 +85,7 @@ struct pfd_ctx {
     int* d_err = nullptr;
     unsigned long long* d_taps = nullptr;   // tap counter of calibration runs
     bool counting = false;
+    int ncc_moments = PFD_NCC_REFERENCE;    // accumulation of the NCC moments (pfd_set_ncc_moments)
     unsigned long long launches = 0;        // kernels this context has launched
     float* d_scratch = nullptr;             // sweep candidate costs, per resident CTA
     size_t scratch_bytes = 0;
@@ -181,9 +184,10 @@ pfd_status check_params(pfd_ctx* ctx, const Frame& f, const pfd_pm_params* p)
     return PFD_OK;
 }
 
-pfd::PmParams make_params(const Frame& f, const pfd_pm_params* p, uint64_t seed)
+pfd::PmParams make_params(const pfd_ctx* ctx, const Frame& f, const pfd_pm_params* p, uint64_t seed)
 {
     pfd::PmParams P;
+    P.shifted = ctx->ncc_moments == PFD_NCC_SHIFTED ? 1 : 0;
     P.W = f.mi_w; P.H = f.mi_h; P.ppv = f.mi_w * f.mi_h;
     P.K = f.K;
     P.radius = p->patch_size / 2;
@@ -219,14 +223,15 @@ bool same_cost_params(const pfd_pm_params& a, const pfd_pm_params& b)
 
 // Before a sweep of `phase`: may it use the stored vectors?  After it: the
 // updated colour's vectors are valid under `p`.
-bool cvec_usable(const Frame& f, const pfd_pm_params& p, int phase)
+bool cvec_usable(const Frame& f, const pfd_pm_params& p, int phase, int moments)
 {
-    return ((f.cvec_valid >> phase) & 1u) && same_cost_params(f.cvec_key, p);
+    return ((f.cvec_valid >> phase) & 1u) && same_cost_params(f.cvec_key, p) && f.cvec_moments == moments;
 }
-void cvec_swept(Frame& f, const pfd_pm_params& p, int phase)
+void cvec_swept(Frame& f, const pfd_pm_params& p, int phase, int moments)
 {
-    if (!same_cost_params(f.cvec_key, p)) f.cvec_valid = 0;
+    if (!same_cost_params(f.cvec_key, p) || f.cvec_moments != moments) f.cvec_valid = 0;
     f.cvec_key = p;
+    f.cvec_moments = moments;
     f.cvec_valid |= 1u << phase;
 }
 
@@ -324,6 +329,15 @@ pfd_status pfd_set_tap_counting(pfd_ctx* ctx, int enable)
 {
     if (!ctx) return PFD_EINVAL;
     ctx->counting = enable != 0;
+    return PFD_OK;
+}
+
+pfd_status pfd_set_ncc_moments(pfd_ctx* ctx, int mode)
+{
+    if (!ctx) return PFD_EINVAL;
+    if (mode != PFD_NCC_REFERENCE && mode != PFD_NCC_SHIFTED)
+        return fail(ctx, PFD_EINVAL, "NCC moment mode %d is neither PFD_NCC_REFERENCE nor PFD_NCC_SHIFTED", mode);
+    ctx->ncc_moments = mode;
     return PFD_OK;
 }
 
@@ -503,6 +517,53 @@ pfd_status pfd_frame_set_micro_images(pfd_ctx* ctx, int frame_id, const uint8_t*
     return PFD_OK;
 }
 
+pfd_status pfd_frame_compute_blur(pfd_ctx* ctx, int frame_id, uint8_t* blur_out, uint32_t* blureness)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!f->has_raw) return fail(ctx, PFD_EINVAL, "compute_blur: frame %d has no raw image", frame_id);
+    DeviceGuard g(ctx->device);
+    const size_t ppv_tiles = (size_t)f->V * f->tile_stride;
+    if (!f->d_blur) {
+        const pfd_status st = frame_alloc(ctx, *f, (void**)&f->d_blur, ppv_tiles);
+        if (st != PFD_OK) return st;
+    }
+    uint32_t* d_counts = nullptr;
+    if (blureness) CU(cudaMallocAsync((void**)&d_counts, sizeof(uint32_t) * f->V, ctx->stream));
+    const cudaError_t e = pfd::launch_blur(f->d_raw, f->W, f->W, f->H, f->d_origin, f->V, f->mi_w, f->mi_h,
+                                           f->tile_stride, f->d_blur, d_counts, ctx->stream);
+    if (e != cudaSuccess) {
+        if (d_counts) cudaFreeAsync(d_counts, ctx->stream);
+        return fail(ctx, PFD_ECUDA, "launch_blur: %s", cudaGetErrorString(e));
+    }
+    ctx->launches += 1;
+    f->has_blur = true;
+    f->has_state = false;
+    f->cvec_valid = 0;
+    pfd_status st = PFD_OK;
+    if (blur_out) {
+        const size_t ppv = (size_t)f->mi_w * f->mi_h;
+        if (cudaMemcpy2DAsync(blur_out, ppv, f->d_blur, f->tile_stride, ppv, f->V, cudaMemcpyDeviceToHost,
+                              ctx->stream) != cudaSuccess)
+            st = PFD_ECUDA;
+    }
+    if (d_counts) {
+        if (st == PFD_OK && cudaMemcpyAsync(blureness, d_counts, sizeof(uint32_t) * f->V, cudaMemcpyDeviceToHost,
+                                            ctx->stream) != cudaSuccess)
+            st = PFD_ECUDA;
+        cudaFreeAsync(d_counts, ctx->stream);
+    }
+    if (blur_out || blureness) {
+        if (st == PFD_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) st = PFD_ECUDA;
+    }
+    if (st != PFD_OK) {
+        cudaGetLastError();
+        return fail(ctx, st, "compute_blur: copy-back failed");
+    }
+    return PFD_OK;
+}
+
 pfd_status pfd_state_upload(pfd_ctx* ctx, int frame_id, const float* plane, const float* cost, const float* disp,
                             const uint32_t* sel)
 {
@@ -560,7 +621,7 @@ pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, 
     pfd_status st = check_params(ctx, *f, params);
     if (st != PFD_OK) return st;
     DeviceGuard g(ctx->device);
-    pfd::PmParams P = make_params(*f, params, seed);
+    pfd::PmParams P = make_params(ctx, *f, params, seed);
     if (ctx->counting) P.tap_counter = ctx->d_taps;
     f->cur = 0;
     f->cvec_valid = 0;
@@ -569,6 +630,7 @@ pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, 
     f->has_state = true;
     f->cvec_valid = 3u;
     f->cvec_key = *params;
+    f->cvec_moments = ctx->ncc_moments;
     return PFD_OK;
 }
 
@@ -583,7 +645,7 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
     if (phase != 0 && phase != 1) return fail(ctx, PFD_EINVAL, "phase must be 0 or 1");
     if (iter < 0) return fail(ctx, PFD_EINVAL, "iter must be >= 0");
     DeviceGuard g(ctx->device);
-    pfd::PmParams P = make_params(*f, params, seed);
+    pfd::PmParams P = make_params(ctx, *f, params, seed);
     if (ctx->counting) P.tap_counter = ctx->d_taps;
     if (pfd::sweep_warp_smem_bytes(P, f->has_blur) > 227 * 1024)
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
@@ -606,13 +668,13 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
         ctx->used += need;
     }
     P.cost_scratch = ctx->d_scratch;
-    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase);
+    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, ctx->ncc_moments);
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
     if (ctx->counting) f->cvec_valid = 0;        // tap counting evaluates everything and stores nothing
-    else cvec_swept(*f, *params, phase);
+    else cvec_swept(*f, *params, phase, ctx->ncc_moments);
     return PFD_OK;
 }
 
@@ -680,7 +742,7 @@ pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params
     H2D(d_pxy, h_pxy.data(), sizeof(int) * 2 * (size_t)n);
     H2D(d_out, h_out.data(), sizeof(int) * (size_t)n);
     H2D(d_plane, h_plane.data(), sizeof(float) * 4 * (size_t)n);
-    const pfd::PmParams P = make_params(*f, params, 0);
+    const pfd::PmParams P = make_params(ctx, *f, params, 0);
     if (rc == PFD_OK &&
         pfd::launch_ncc(frame_dev(*f), P, nseg, npb, d_segv, d_segs, d_segl, d_pxy, d_plane, d_out, d_cost,
                         ctx->d_err, s) != cudaSuccess)
@@ -1722,7 +1784,7 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     if (phase != 0 && phase != 1) return fail(ctx, PFD_EINVAL, "phase must be 0 or 1");
     if (iter < 0) return fail(ctx, PFD_EINVAL, "iter must be >= 0");
     DeviceGuard g(ctx->device);
-    pfd::PmParams P = make_params(*f, params, seed);
+    pfd::PmParams P = make_params(ctx, *f, params, seed);
     if (ctx->counting) P.tap_counter = ctx->d_taps;
     if (pfd::sweep_warp_smem_bytes(P, f->has_blur) > 227 * 1024)
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
@@ -1749,12 +1811,12 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     st = noalloc_scratch(ctx, ctx->device, &scratch);
     if (st != PFD_OK) return st;
     P.cost_scratch = scratch;
-    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase);
+    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, ctx->ncc_moments);
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
     if (ctx->counting) f->cvec_valid = 0;        // tap counting evaluates everything and stores nothing
-    else cvec_swept(*f, *params, phase);
+    else cvec_swept(*f, *params, phase, ctx->ncc_moments);
     return PFD_OK;
 }

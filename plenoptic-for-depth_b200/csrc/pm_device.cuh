@@ -33,6 +33,7 @@ struct PmParams {
     float* cost_scratch;    // sweep: per warp, the cost vectors of its current pixel
     float* cvec;            // [V * ppv][K]: cost vector of each pixel's current plane (init and sweeps write it)
     int cvec_ok;            // sweep: cvec holds the vectors of the updated colour's current planes
+    int shifted;            // 0: the reference's raw NCC moments; 1: moments of (pixel - centre pixel)
 };
 
 struct FrameDev {
@@ -291,6 +292,10 @@ __device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int
         bsx[c] = bsy[c] = 0.0f;
     }
     const float rc = T.R[py * W + px];
+    // shifted moments: texels and samples minus the centre texel; both are
+    // multiples of 1/256 below 2^16, so the subtraction is exact, and with
+    // shift 0 every sum is bit for bit the reference's
+    const float sh = P.shifted ? rc : 0.0f;
     const int r = P.radius, inc = P.inc, ntap = P.ntap;
     // Taps are visited by absolute window position (X, Y), X outer, Y inner,
     // over the union of the warp's patches.  Each lane keeps only positions
@@ -323,7 +328,8 @@ __device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int
             const float cd = fabsf(__fsub_rn(rv, rc));
             const int cdi = __float_as_int(__fadd_rn(cd, 8388608.0f)) & 0xFF;
             const float w = refok ? pfd_expf_nonpos(__fsub_rn(T.a_s[t], T.a_c[cdi])) : 0.0f;
-            const float wr = __fmul_rn(w, rv);
+            const float rvs = __fsub_rn(rv, sh);
+            const float wr = __fmul_rn(w, rvs);
             const float d = __fadd_rn(__fmaf_rn(dp.y, fyr, axr), dp.z);
             (void)xr;
             float rb = 0.0f;
@@ -340,12 +346,12 @@ __device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int
                 const uint32_t rel = (uint32_t)(((tby >> 8) * S + (tbx >> 8)) << 3);
                 const uint32_t addr = v ? base[c] + rel : T.q_addr;
                 const int2 p0 = lds_int2(addr), p1 = lds_int2(addr + (uint32_t)S * 8u);
-                const float s = tex_blend(tbx, tby, p0, p1);
+                const float s = __fsub_rn(tex_blend(tbx, tby, p0, p1), sh);
                 const float wv = v ? w : 0.0f;
                 const float wrv = v ? wr : 0.0f;
                 const float ws = __fmul_rn(wv, s);
-                sr[c]  = __fmaf_rn(wv, rv, sr[c]);
-                srr[c] = __fmaf_rn(wrv, rv, srr[c]);
+                sr[c]  = __fmaf_rn(wv, rvs, sr[c]);
+                srr[c] = __fmaf_rn(wrv, rvs, srr[c]);
                 ss[c]  = __fmaf_rn(wv, s, ss[c]);
                 sss[c] = __fmaf_rn(ws, s, sss[c]);
                 srs[c] = __fmaf_rn(wrv, s, srs[c]);

@@ -275,6 +275,7 @@ __device__ __forceinline__ void build_table(const Quad& T, const PmParams& P, co
 {
     const int W = P.W, inc = P.inc;
     const float rc = T.R[py * W + px];
+    const float sh = P.shifted ? rc : 0.0f;      // shifted moments: texels minus the centre texel (exact)
     const int n = pw.nX * pw.nY;
     for (int t = lane; t < n; t += 32) {
         const int ix = t / pw.nY, iy = t - ix * pw.nY;
@@ -285,16 +286,17 @@ __device__ __forceinline__ void build_table(const Quad& T, const PmParams& P, co
         const int ti = (pw.ii0 + ix) * P.ntap + (pw.jj0 + iy);
         const float w = pfd_expf_nonpos(__fsub_rn(T.a_s[ti], T.a_c[cdi]));
         const float rb = BLUR ? __fdiv_rn(T.RB[Y * W + X], 255.0f) : 0.0f;
-        tab[t] = make_float4(w, __fmul_rn(w, rv), rv, rb);
+        const float rvs = __fsub_rn(rv, sh);
+        tab[t] = make_float4(w, __fmul_rn(w, rvs), rvs, rb);
     }
 }
 
 // One lane's NCC (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:73-179) of the
 // pixel under plane dp against neighbour k.  Every lane of the warp walks the
 // same taps; a lane skips the taps it does not keep.
-template <bool BLUR, bool COUNT>
+template <bool BLUR, bool COUNT, bool SHIFT>
 __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, const float4* tab, const PixWin& pw,
-                                          float3 dp, int k, bool active, unsigned& ntaps)
+                                          float3 dp, int k, bool active, float sh, unsigned& ntaps)
 {
     const NbGeo& g = T.geo[k];
     const float stx = g.stx, sty = g.sty;
@@ -319,7 +321,8 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
             if (v) {                         // a skipped tap leaves the sums as they are
                 const int tbx = tex_coord_bits(sx), tby = tex_coord_bits(sy);
                 const uint32_t rel = (((uint32_t)(tby >> 8) * qs + (uint32_t)(tbx >> 8)) << 2);
-                const float s = quad_blend(tbx, tby, lds_u32(base + rel));
+                float s = quad_blend(tbx, tby, lds_u32(base + rel));
+                if (SHIFT) s = __fsub_rn(s, sh);
                 const float wv = e.x, wrv = e.y, rv = e.z;
                 const float ws = __fmul_rn(wv, s);
                 sr = __fmaf_rn(wv, rv, sr);
@@ -363,7 +366,7 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
 // skip: S.cost[h * K + k] for the neighbours k < nc whose bit is set in vmask
 // (the other entries are left as they are).  A neighbour whose anchor leaves
 // the window gets 2 without evaluation.
-template <bool BLUR, bool COUNT>
+template <bool BLUR, bool COUNT, bool SHIFT>
 __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const WarpBlock& S, const PixWin& pw,
                                        int px, int py, int nh, int nc, int lane, uint64_t skip, uint32_t vmask)
 {
@@ -393,12 +396,13 @@ __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const W
     }
     __syncwarp();
     unsigned ntaps = 0;
+    const float sh = SHIFT ? T.R[py * P.W + px] : 0.0f;
     for (int p0 = 0; p0 < np; p0 += 32) {
         const bool act = p0 + lane < np;
         const int n = act ? S.pair[p0 + lane] : 0;
         const int h = n / nc, k = n - h * nc;
         const float4 d = S.dp[h];
-        const float c = ncc_lane<BLUR, COUNT>(T, P, S.tab, pw, make_float3(d.x, d.y, d.z), k, act, ntaps);
+        const float c = ncc_lane<BLUR, COUNT, SHIFT>(T, P, S.tab, pw, make_float3(d.x, d.y, d.z), k, act, sh, ntaps);
         if (act) S.cost[h * K + k] = c;
     }
     if (COUNT) {
@@ -555,7 +559,7 @@ __device__ __forceinline__ void refine_candidates(int x, int y, float4 best, flo
 
 }  // namespace
 
-template <bool BLUR, bool COUNT>
+template <bool BLUR, bool COUNT, bool SHIFT>
 __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, PmParams P, StateDev prev,
                                                                      StateDev next, int iter, int phase, int* err)
 {
@@ -653,7 +657,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             const bool use_cvec = !COUNT && P.cvec_ok;
             if (use_cvec && lane < nc) S.cost[lane] = P.cvec[idx * K + lane];
             __syncwarp();
-            eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, nh, nc, lane, use_cvec ? 1ull : 0ull, ~0u);
+            eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, nh, nc, lane, use_cvec ? 1ull : 0ull, ~0u);
 #define SLOT(s) ((int)((slots >> (4 * (s))) & 15ull))
 #define COSTA(s, k) S.cost[SLOT(s) * K + (k)]
 
@@ -776,7 +780,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                 if (lane == 0)
                     for (int i = 0; i < 5; ++i) S.plane[r0 + i] = cand[i];
                 __syncwarp();
-                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull, tsel);
+                eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull, tsel);
                 weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
 
                 bool changed = false;
@@ -802,7 +806,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                         __syncwarp();
                         if (lane == 0) S.plane[row] = proxy;
                         __syncwarp();
-                        eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull, tsel);
+                        eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull, tsel);
                         weigh_hyps(S, K, row + 1, nc, vw_lo, vw_hi, lane, tsel);
                         c = S.wres[row];
                         cmin = S.wmin[row];
@@ -819,7 +823,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                         for (int i = 2; i < 5; ++i) S.plane[r0 + i] = cand[i];
                     __syncwarp();
                     const uint64_t redo = (7ull << (r0 + 2)) & ~(skip3 ? (1ull << (r0 + 3)) : 0ull);
-                    eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo, tsel);
+                    eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo, tsel);
                     weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
                 }
                 for (int i = 0; i < 5; ++i) {
@@ -839,7 +843,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                     __syncwarp();
                     if (lane == 0) S.plane[0] = proxy;
                     __syncwarp();
-                    eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
+                    eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
                     weigh_hyps(S, K, 1, nc, vw_lo, vw_hi, lane, ~0u);
                     const float c = S.wres[0];
                     if (c < best_cost) { best_cost = c; best_plane = proxy; best_min = S.wmin[0]; }
@@ -850,7 +854,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                 if (lane == 0)
                     for (int i = 0; i < 5; ++i) S.plane[i] = cand[i];
                 __syncwarp();
-                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, 5, nc, lane, 0ull, ~0u);
+                eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, 5, nc, lane, 0ull, ~0u);
                 weigh_hyps(S, K, 5, nc, vw_lo, vw_hi, lane, ~0u);
                 for (int i = 0; i < 5; ++i) {
                     const float c = S.wres[i];
@@ -865,7 +869,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                 __syncwarp();
                 if (lane == 0) S.plane[0] = best_plane;
                 __syncwarp();
-                eval_hyps<BLUR, COUNT>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
+                eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
                 weigh_hyps(S, K, 1, nc, vw_lo, vw_hi, lane, ~0u);
                 best_min = S.wmin[0];
                 best_vec = lane < nc ? S.cost[lane] : 0.0f;
@@ -913,7 +917,8 @@ cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int smem = sweep_warp_smem_bytes(P, blur);
-    const void* k = blur ? (const void*)pm_sweep_warp_kernel<true, false> : (const void*)pm_sweep_warp_kernel<false, false>;
+    const void* k = blur ? (const void*)pm_sweep_warp_kernel<true, false, false>
+                         : (const void*)pm_sweep_warp_kernel<false, false, false>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem);
@@ -932,11 +937,18 @@ cudaError_t launch_sweep_warp(const FrameDev& F, const PmParams& P, const StateD
     const int grid = std::max(1, std::min(n_ctas, F.V));
     FrameDev f = F; PmParams p = P; StateDev a = prev, b = next; int it = iter, ph = phase; int* e = err;
     void* args[] = { &f, &p, &a, &b, &it, &ph, &e };
-    if (P.tap_counter)
-        return blur ? launch_k(pm_sweep_warp_kernel<true, true>, grid, kThreads, smem, st, args)
-                    : launch_k(pm_sweep_warp_kernel<false, true>, grid, kThreads, smem, st, args);
-    return blur ? launch_k(pm_sweep_warp_kernel<true, false>, grid, kThreads, smem, st, args)
-                : launch_k(pm_sweep_warp_kernel<false, false>, grid, kThreads, smem, st, args);
+    if (P.tap_counter) {
+        if (P.shifted)
+            return blur ? launch_k(pm_sweep_warp_kernel<true, true, true>, grid, kThreads, smem, st, args)
+                        : launch_k(pm_sweep_warp_kernel<false, true, true>, grid, kThreads, smem, st, args);
+        return blur ? launch_k(pm_sweep_warp_kernel<true, true, false>, grid, kThreads, smem, st, args)
+                    : launch_k(pm_sweep_warp_kernel<false, true, false>, grid, kThreads, smem, st, args);
+    }
+    if (P.shifted)
+        return blur ? launch_k(pm_sweep_warp_kernel<true, false, true>, grid, kThreads, smem, st, args)
+                    : launch_k(pm_sweep_warp_kernel<false, false, true>, grid, kThreads, smem, st, args);
+    return blur ? launch_k(pm_sweep_warp_kernel<true, false, false>, grid, kThreads, smem, st, args)
+                : launch_k(pm_sweep_warp_kernel<false, false, false>, grid, kThreads, smem, st, args);
 }
 
 }  // namespace pfd
