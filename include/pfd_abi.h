@@ -181,6 +181,31 @@ pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd_pm_params*
 #define PFD_NCC_SHIFTED   1
 pfd_status pfd_set_ncc_moments(pfd_ctx* ctx, int mode);
 
+/* The PatchMatch rules of the context's later pfd_pm_init, pfd_pm_sweep(_noalloc),
+ * pfd_patchmatch and pfd_ncc_costs calls.
+ * PFD_MATCHER_FRAME (the default): AdaptMIPMFrame (MIStereo/AdaptMIPMFrame.cu).
+ * PFD_MATCHER_ACMM: one pyramid level of AdaptMIPMFrameACMM
+ * (MIStereo/AdaptMIPMFrameACMM.cu), the matcher MIStereoMatch::
+ * StereoMatchingForMIA_FrameCrossViews_ACMM runs (MIStereoMatch.cpp:698-740):
+ * the same initialisation and half-sweeps with a blur penalty gain of 0.8
+ * instead of 2 (:99), and each updated pixel stores the mean of the top_k
+ * lowest costs of its final plane over every view, those views as its
+ * selected-view mask and the lowest-cost view's disp (RecomputeSupportCostDisp_
+ * Frame, :259-280, called at :890); pfd_patchmatch then ends with
+ * pfd_acmm_post_refine.  The matcher builds its two-level pyramid only for
+ * windows of 24 pixels and more (AdaptMIPMFrameACMM.cpp:312-321); the coarse
+ * level and the warm start are not provided here: this is the matcher at one
+ * level, which is all of it for windows below 24 pixels (pitch < 34 px).
+ * The caller passes the level's parameters (the reference uses patch 5,
+ * 5 iterations and top_k 6 at one level, :155-180). */
+#define PFD_MATCHER_FRAME 0
+#define PFD_MATCHER_ACMM  1
+pfd_status pfd_set_matcher(pfd_ctx* ctx, int matcher);
+/* PostRefineMetadataFrame (AdaptMIPMFrameACMM.cu:903-929): every pixel keeps
+ * its plane and gets the cost, selected views and disp of it as the ACMM
+ * write-back computes them, under the context's matcher and moment mode. */
+pfd_status pfd_acmm_post_refine(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params);
+
 /* Per-hypothesis cost vectors: ComputeMultiViewCostVector_Frame
  * (AdaptMIPMFrame.cu:181-225) for n (view, pixel, plane) hypotheses.
  * vids[n], pxy[n][2] (x, y inside the window), planes[n][4] (nx, ny, nz, d);

@@ -190,7 +190,9 @@ static void cost_vector(const orc_frame* f, const orc_params* p, int vid, int px
         float c = ncc_frame(f, p, vid, nvid, px, py, h, &bx, &by, &db, taps);
         const float t = bx - by;
         const float bw = canon_expf((-0.007368f * t) * t);
-        c = clamp_cost(fmaf(2.0f, 1.0f - bw, c));
+        /* blur penalty gain: 2 in the Frame matcher, 0.8 in the ACMM one
+         * (AdaptMIPMFrameACMM.cu:99) */
+        c = clamp_cost(fmaf(p->acmm ? 0.8f : 2.0f, 1.0f - bw, c));
         cv[k] = c;
         dv[k] = db;
     }
@@ -658,6 +660,18 @@ static void update_pixel(const orc_frame* f, const orc_params* p, uint64_t seed,
     }
     refine(f, p, vid, x, y, &g, vw, &best_plane, &best_cost, &best_disp, taps);
 
+    if (p->acmm) {
+        /* ACMM write-back (AdaptMIPMFrameACMM.cu:880-900): DetailRestorer_FrameACMM
+         * returns at once without a warm start; RecomputeSupportCostDisp_Frame
+         * (:259-280) evaluates the final plane on every view and stores the
+         * top-k mean, the top-k view mask and the lowest-cost view's disp */
+        float cv[MAX_NB];
+        f4 dv[MAX_NB];
+        cost_vector(f, p, vid, x, y, best_plane, cv, dv, taps);
+        int bi = -1;
+        tsel = topk_views(cv, nc, p->top_k, &best_cost, &bi);
+        best_disp = bi >= 0 ? dv[bi] : mk4(0, 0, 0, 0);
+    }
     st4(next->plane, idx, best_plane);
     next->cost[idx] = best_cost;
     st4(next->disp, idx, best_disp);
@@ -789,7 +803,34 @@ int orc_patchmatch(const orc_frame* f, const orc_params* p, uint64_t seed, orc_s
     }
     /* an even number of half-sweeps leaves the result in out */
     free(tmp.plane); free(tmp.cost); free(tmp.disp); free(tmp.sel);
+    if (rc == 0 && p->acmm) rc = orc_acmm_post_refine(f, p, out, nthreads);
     return rc;
+}
+
+/* PostRefineMetadataFrame (AdaptMIPMFrameACMM.cu:903-929): cost, selected views
+ * and disp of every pixel recomputed from its plane (RecomputeSupportCostDisp_Frame). */
+int orc_acmm_post_refine(const orc_frame* f, const orc_params* p, orc_state* st, int nthreads)
+{
+    if (!f || !p || f->max_nb > MAX_NB) return -1;
+    const int W = f->mi_w;
+    const long ppv = (long)W * f->mi_h, total = ppv * f->n_views;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+#endif
+    for (long t = 0; t < total; ++t) {
+        const int vid = (int)(t / ppv), rem = (int)(t % ppv);
+        float cv[MAX_NB];
+        f4 dv[MAX_NB];
+        cost_vector(f, p, vid, rem % W, rem / W, ld4(st->plane, t), cv, dv, NULL);
+        float mean = 2.0f;
+        int bi = -1;
+        st->sel[t] = topk_views(cv, f->nb_counts[vid], p->top_k, &mean, &bi);
+        st->cost[t] = mean;
+        st4(st->disp, t, bi >= 0 ? dv[bi] : mk4(0, 0, 0, 0));
+    }
+    (void)nthreads;
+    return 0;
 }
 
 /* ------------------------------------------------------------------------ */

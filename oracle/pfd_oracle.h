@@ -51,6 +51,7 @@ typedef struct {
     float depth_max;
     float base;                  /* Base: lens pitch in pixels (AdaptMIPMFrame.cpp:138) */
     int shifted;                 /* 0: the reference's NCC moments; 1: moments of (texel - centre texel) */
+    int acmm;                    /* 1: the ACMM matcher's rules (AdaptMIPMFrameACMM.cu), single pyramid level */
 } orc_params;
 
 /* Per-pixel state, the four ping-pong buffers of AdaptMIPMFrame
@@ -102,8 +103,12 @@ int orc_pm_sweep_views(const orc_frame* f, const orc_params* p, uint64_t seed, i
                        const orc_state* prev, orc_state* next, int v0, int v1, int nthreads);
 
 /* RunPatchMatchCUDAForFrame_Impl (AdaptMIPMFrame.cu:949-995): init, then
- * max_iterations x (phase 0, phase 1).  Result in out. */
+ * max_iterations x (phase 0, phase 1).  Result in out.  With p->acmm,
+ * RunPatchMatchCUDAForFrameACMM_Impl (AdaptMIPMFrameACMM.cu:931-990) for one
+ * pyramid level: the same, then orc_acmm_post_refine. */
 int orc_patchmatch(const orc_frame* f, const orc_params* p, uint64_t seed, orc_state* out, int nthreads);
+/* PostRefineMetadataFrame (AdaptMIPMFrameACMM.cu:903-929) over every pixel of st. */
+int orc_acmm_post_refine(const orc_frame* f, const orc_params* p, orc_state* st, int nthreads);
 
 /* ---- consistency pass (oracle/checks.c) ---- */
 

@@ -28,7 +28,7 @@ class OrcFrame(ctypes.Structure):
 class OrcParams(ctypes.Structure):
     _fields_ = [("max_iterations", _I), ("patch_size", _I), ("radius_increment", _I), ("top_k", _I),
                 ("sigma_spatial", _F), ("sigma_color", _F), ("depth_min", _F), ("depth_max", _F), ("base", _F),
-                ("shifted", _I)]
+                ("shifted", _I), ("acmm", _I)]
 
 
 class OrcFilterCfg(ctypes.Structure):
@@ -98,6 +98,7 @@ def lib() -> ctypes.CDLL:
         L.orc_pm_sweep.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I]
         L.orc_pm_sweep_views.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I, _I, _I]
         L.orc_patchmatch.argtypes = [FP, PP, ctypes.c_uint64, SP, _I]
+        L.orc_acmm_post_refine.argtypes = [FP, PP, SP, _I]
         L.orc_expf.argtypes = [_F]
         L.orc_expf.restype = _F
         L.orc_uniform.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
@@ -145,8 +146,9 @@ def _p(a):
 class Oracle:
     """One frame of views for the oracle.  gray: [V][h][w] uint8/float."""
 
-    def __init__(self, gray, centers, nb_ids, nb_counts, blur=None, shifted=False):
+    def __init__(self, gray, centers, nb_ids, nb_counts, blur=None, shifted=False, acmm=False):
         self.shifted = bool(shifted)     # NCC moments of (texel - centre texel) instead of the reference's
+        self.acmm = bool(acmm)           # the ACMM matcher's rules (one pyramid level)
         self.gray = np.ascontiguousarray(gray, dtype=np.float32)
         self.blur = None if blur is None else np.ascontiguousarray(blur, dtype=np.float32)
         self.centers = np.ascontiguousarray(centers, dtype=np.float32)
@@ -162,7 +164,7 @@ class Oracle:
         """From the package's PmParams (same fields) and the oracle's moment mode."""
         c = p.c()
         return OrcParams(c.max_iterations, c.patch_size, c.radius_increment, c.top_k, c.sigma_spatial, c.sigma_color,
-                         c.depth_min, c.depth_max, c.base, 1 if self.shifted else 0)
+                         c.depth_min, c.depth_max, c.base, 1 if self.shifted else 0, 1 if self.acmm else 0)
 
     def new_state(self):
         n = self.V * self.h * self.w
@@ -240,6 +242,14 @@ class Oracle:
                                        ctypes.byref(st), nthreads)
         assert taps >= 0
         return arr, int(taps)
+
+    def acmm_post_refine(self, params, state, nthreads=0):
+        """PostRefineMetadataFrame over a copy of state (dict of arrays)."""
+        arr = {k: np.ascontiguousarray(v).copy() for k, v in state.items()}
+        st = OrcState(_p(arr["plane"]), _p(arr["cost"]), _p(arr["disp"]), _p(arr["sel"]))
+        p = self.params(params)
+        assert lib().orc_acmm_post_refine(ctypes.byref(self.f), ctypes.byref(p), ctypes.byref(st), nthreads) == 0
+        return arr
 
     def patchmatch(self, params, seed, nthreads=0):
         arr, st = self.new_state()

@@ -194,6 +194,8 @@ def lib() -> ctypes.CDLL:
             "pfd_frame_set_micro_images": [_P, _I, _P],
             "pfd_frame_compute_blur": [_P, _I, _P, _P],
             "pfd_set_ncc_moments": [_P, _I],
+            "pfd_set_matcher": [_P, _I],
+            "pfd_acmm_post_refine": [_P, _I, ctypes.POINTER(PmParamsC)],
             "pfd_state_upload": [_P, _I, _P, _P, _P, _P],
             "pfd_frame_upload": [_P, ctypes.POINTER(_I), _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _I, _P],
             "pfd_frame_free": [_P, _I],
@@ -404,6 +406,15 @@ class Context:
         reference's raw moments (PFD_NCC_REFERENCE, the default) for the
         context's later initialisations, sweeps and cost queries."""
         self._check(self._L.pfd_set_ncc_moments(self._h, 1 if shifted else 0), "pfd_set_ncc_moments")
+
+    def set_matcher(self, acmm: bool) -> None:
+        """PatchMatch rules of the context's later calls: the ACMM matcher at one
+        pyramid level (PFD_MATCHER_ACMM) or the Frame matcher (the default)."""
+        self._check(self._L.pfd_set_matcher(self._h, 1 if acmm else 0), "pfd_set_matcher")
+
+    def acmm_post_refine(self, fid: int, params: "PmParams") -> None:
+        p = params.c()
+        self._check(self._L.pfd_acmm_post_refine(self._h, fid, ctypes.byref(p)), "pfd_acmm_post_refine")
 
     def set_tap_counting(self, on: bool) -> None:
         self._check(self._L.pfd_set_tap_counting(self._h, 1 if on else 0), "pfd_set_tap_counting")

@@ -49,7 +49,7 @@ struct Frame {
     float* d_cvec = nullptr;
     unsigned cvec_valid = 0;
     pfd_pm_params cvec_key = {};
-    int cvec_moments = PFD_NCC_REFERENCE;     // the NCC moments cvec was computed with
+    int cvec_mode = 0;                        // cost_mode() of the context that computed cvec
     bool has_state = false;
     size_t bytes = 0;
     bool registered = false;          // bytes already counted in the context's total
@@ -86,6 +86,7 @@ struct pfd_ctx {
     unsigned long long* d_taps = nullptr;   // tap counter of calibration runs
     bool counting = false;
     int ncc_moments = PFD_NCC_REFERENCE;    // accumulation of the NCC moments (pfd_set_ncc_moments)
+    int matcher = PFD_MATCHER_FRAME;        // PatchMatch rules (pfd_set_matcher)
     unsigned long long launches = 0;        // kernels this context has launched
     float* d_scratch = nullptr;             // sweep candidate costs, per resident CTA
     size_t scratch_bytes = 0;
@@ -188,6 +189,9 @@ pfd::PmParams make_params(const pfd_ctx* ctx, const Frame& f, const pfd_pm_param
 {
     pfd::PmParams P;
     P.shifted = ctx->ncc_moments == PFD_NCC_SHIFTED ? 1 : 0;
+    // the ACMM matcher's blur penalty gain and write-back (AdaptMIPMFrameACMM.cu:99,880-900)
+    P.acmm = ctx->matcher == PFD_MATCHER_ACMM ? 1 : 0;
+    P.blur_gain = P.acmm ? 0.8f : 2.0f;
     P.W = f.mi_w; P.H = f.mi_h; P.ppv = f.mi_w * f.mi_h;
     P.K = f.K;
     P.radius = p->patch_size / 2;
@@ -223,15 +227,19 @@ bool same_cost_params(const pfd_pm_params& a, const pfd_pm_params& b)
 
 // Before a sweep of `phase`: may it use the stored vectors?  After it: the
 // updated colour's vectors are valid under `p`.
-bool cvec_usable(const Frame& f, const pfd_pm_params& p, int phase, int moments)
+// Everything of the context that shapes a cost vector besides the parameters:
+// the moment mode and the matcher (its blur penalty gain).
+int cost_mode(const pfd_ctx* ctx) { return ctx->ncc_moments | (ctx->matcher << 1); }
+
+bool cvec_usable(const Frame& f, const pfd_pm_params& p, int phase, int mode)
 {
-    return ((f.cvec_valid >> phase) & 1u) && same_cost_params(f.cvec_key, p) && f.cvec_moments == moments;
+    return ((f.cvec_valid >> phase) & 1u) && same_cost_params(f.cvec_key, p) && f.cvec_mode == mode;
 }
-void cvec_swept(Frame& f, const pfd_pm_params& p, int phase, int moments)
+void cvec_swept(Frame& f, const pfd_pm_params& p, int phase, int mode)
 {
-    if (!same_cost_params(f.cvec_key, p) || f.cvec_moments != moments) f.cvec_valid = 0;
+    if (!same_cost_params(f.cvec_key, p) || f.cvec_mode != mode) f.cvec_valid = 0;
     f.cvec_key = p;
-    f.cvec_moments = moments;
+    f.cvec_mode = mode;
     f.cvec_valid |= 1u << phase;
 }
 
@@ -338,6 +346,15 @@ pfd_status pfd_set_ncc_moments(pfd_ctx* ctx, int mode)
     if (mode != PFD_NCC_REFERENCE && mode != PFD_NCC_SHIFTED)
         return fail(ctx, PFD_EINVAL, "NCC moment mode %d is neither PFD_NCC_REFERENCE nor PFD_NCC_SHIFTED", mode);
     ctx->ncc_moments = mode;
+    return PFD_OK;
+}
+
+pfd_status pfd_set_matcher(pfd_ctx* ctx, int matcher)
+{
+    if (!ctx) return PFD_EINVAL;
+    if (matcher != PFD_MATCHER_FRAME && matcher != PFD_MATCHER_ACMM)
+        return fail(ctx, PFD_EINVAL, "matcher %d is neither PFD_MATCHER_FRAME nor PFD_MATCHER_ACMM", matcher);
+    ctx->matcher = matcher;
     return PFD_OK;
 }
 
@@ -630,7 +647,7 @@ pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, 
     f->has_state = true;
     f->cvec_valid = 3u;
     f->cvec_key = *params;
-    f->cvec_moments = ctx->ncc_moments;
+    f->cvec_mode = cost_mode(ctx);
     return PFD_OK;
 }
 
@@ -668,13 +685,13 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
         ctx->used += need;
     }
     P.cost_scratch = ctx->d_scratch;
-    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, ctx->ncc_moments);
+    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, cost_mode(ctx));
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
     if (ctx->counting) f->cvec_valid = 0;        // tap counting evaluates everything and stores nothing
-    else cvec_swept(*f, *params, phase, ctx->ncc_moments);
+    else cvec_swept(*f, *params, phase, cost_mode(ctx));
     return PFD_OK;
 }
 
@@ -683,7 +700,28 @@ pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* param
     pfd_status st = pfd_pm_init(ctx, frame_id, params, seed);
     for (int it = 0; st == PFD_OK && it < params->max_iterations; ++it)
         for (int ph = 0; ph < 2 && st == PFD_OK; ++ph) st = pfd_pm_sweep(ctx, frame_id, params, seed, it, ph);
+    if (st == PFD_OK && ctx->matcher == PFD_MATCHER_ACMM) st = pfd_acmm_post_refine(ctx, frame_id, params);
     return st;
+}
+
+pfd_status pfd_acmm_post_refine(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    pfd_status st = check_params(ctx, *f, params);
+    if (st != PFD_OK) return st;
+    if (!f->has_state) return fail(ctx, PFD_ESTATE, "post-refine before pfd_pm_init");
+    DeviceGuard g(ctx->device);
+    pfd::PmParams P = make_params(ctx, *f, params, 0);
+    if (ctx->counting) P.tap_counter = ctx->d_taps;
+    CU(pfd::launch_init(frame_dev(*f), P, f->s[f->cur], ctx->d_err, ctx->stream, true));
+    ctx->launches += 1;
+    // the pass stores every pixel's vector of its current plane
+    f->cvec_valid = 3u;
+    f->cvec_key = *params;
+    f->cvec_mode = cost_mode(ctx);
+    return PFD_OK;
 }
 
 pfd_status pfd_ncc_costs(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, const int* vids, const int* pxy,
@@ -1811,12 +1849,12 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     st = noalloc_scratch(ctx, ctx->device, &scratch);
     if (st != PFD_OK) return st;
     P.cost_scratch = scratch;
-    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, ctx->ncc_moments);
+    P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, cost_mode(ctx));
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;
     if (ctx->counting) f->cvec_valid = 0;        // tap counting evaluates everything and stores nothing
-    else cvec_swept(*f, *params, phase, ctx->ncc_moments);
+    else cvec_swept(*f, *params, phase, cost_mode(ctx));
     return PFD_OK;
 }

@@ -34,6 +34,8 @@ struct PmParams {
     float* cvec;            // [V * ppv][K]: cost vector of each pixel's current plane (init and sweeps write it)
     int cvec_ok;            // sweep: cvec holds the vectors of the updated colour's current planes
     int shifted;            // 0: the reference's raw NCC moments; 1: moments of (pixel - centre pixel)
+    float blur_gain;        // blur penalty gain: 2 (Frame matcher), 0.8 (ACMM matcher)
+    int acmm;               // 1: ACMM write-back (top-k cost, views and disp of the final plane)
 };
 
 struct FrameDev {
@@ -385,7 +387,7 @@ __device__ __forceinline__ void ncc_chunk(const Tiles& T, const PmParams& P, int
         if (BLUR) {
             const float tb = __fsub_rn(bsx[c], bsy[c]);
             const float bw = pfd_expf(__fmul_rn(__fmul_rn(-0.007368f, tb), tb));
-            v = clamp_cost(__fmaf_rn(2.0f, __fsub_rn(1.0f, bw), v));
+            v = clamp_cost(__fmaf_rn(P.blur_gain, __fsub_rn(1.0f, bw), v));
         }
         cost[c] = v;
     }

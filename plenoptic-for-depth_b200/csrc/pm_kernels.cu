@@ -203,8 +203,11 @@ __global__ void pm_slice_kernel(const uint8_t* raw, int raw_pitch, const int2* o
 // RandomInitializationForFrame.  One thread per pixel; every lane of a warp
 // takes part in the warp-collective cost evaluation.
 // --------------------------------------------------------------------------
+// With refit set, the pixel keeps its plane from out.plane and only its cost,
+// selected views and disp are recomputed: PostRefineMetadataFrame of the ACMM
+// matcher (AdaptMIPMFrameACMM.cu:903-929), which is the same top-k evaluation.
 template <bool BLUR, bool COUNT>
-__global__ void __launch_bounds__(256) pm_init_kernel(FrameDev F, PmParams P, StateDev out, int* err)
+__global__ void __launch_bounds__(256) pm_init_kernel(FrameDev F, PmParams P, StateDev out, int* err, int refit)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int vid = blockIdx.x;
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(256) pm_init_kernel(FrameDev F, PmParams P, St
     DrawStream g;
     g.init(P.seed, 0u, (uint32_t)idx);
     float4 h = make_float4(0.f, 0.f, 1.f, 0.f);
-    if (act) h = random_plane(g, P.depth_min, P.depth_max);
+    if (act) h = refit ? out.plane[idx] : random_plane(g, P.depth_min, P.depth_max);
     float* cs = (float*)(smem + L.off_cost) + t;           // [k][npb]
     cost_vector<BLUR, COUNT>(T, P, x, y, act, h, nc, cs, npb);
     if (!act) return;
@@ -254,7 +257,7 @@ __global__ void __launch_bounds__(256) pm_init_kernel(FrameDev F, PmParams P, St
     }
     float4 disp = make_float4(0.f, 0.f, 0.f, 0.f);
     if (best_idx >= 0) disp = geo_disp(T.geo[best_idx], x, y, to_disparity(x, y, disparity_plane(x, y, h)));
-    out.plane[idx] = h;
+    if (!refit) out.plane[idx] = h;
     out.cost[idx] = mean;
     out.disp[idx] = disp;
     out.sel[idx] = mask;
@@ -306,14 +309,15 @@ cudaError_t launch_slice(const uint8_t* raw, int raw_pitch, const int2* origin, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_init(const FrameDev& F, const PmParams& P, const StateDev& out, int* err, cudaStream_t st)
+cudaError_t launch_init(const FrameDev& F, const PmParams& P, const StateDev& out, int* err, cudaStream_t st,
+                        bool refit)
 {
     const bool blur = F.blur != nullptr;
     const int npb = P.ppv < 256 ? ((P.ppv + 31) / 32) * 32 : 256;
     const int smem = SmemPlan::make(P.W, P.H, P.K, npb, P.ntap, blur, 1, false, P.tile_stride).total;
     dim3 grid(F.V, (P.ppv + npb - 1) / npb);
-    FrameDev f = F; PmParams p = P; StateDev o = out; int* e = err;
-    void* args[] = { &f, &p, &o, &e };
+    FrameDev f = F; PmParams p = P; StateDev o = out; int* e = err; int r = refit ? 1 : 0;
+    void* args[] = { &f, &p, &o, &e, &r };
     if (P.tap_counter)
         return blur ? launch(pm_init_kernel<true, true>, grid, npb, smem, st, args)
                     : launch(pm_init_kernel<false, true>, grid, npb, smem, st, args);

@@ -11,7 +11,10 @@ namespace pfd {
 
 cudaError_t launch_slice(const uint8_t* raw, int raw_pitch, const int2* origin, int V, int W, int H,
                          int tile_stride, uint8_t* tiles, cudaStream_t st);
-cudaError_t launch_init(const FrameDev& F, const PmParams& P, const StateDev& out, int* err, cudaStream_t st);
+// refit: keep each pixel's plane and recompute only its cost, selected views
+// and disp (the ACMM matcher's post-refine pass).
+cudaError_t launch_init(const FrameDev& F, const PmParams& P, const StateDev& out, int* err, cudaStream_t st,
+                        bool refit = false);
 cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, const int* seg_vid,
                        const int* seg_start, const int* seg_len, const int* hyp_pxy, const float4* hyp_plane,
                        const int* hyp_out, float* costs, int* err, cudaStream_t st);

@@ -356,7 +356,7 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
     if (BLUR) {
         const float tb = __fsub_rn(bsx, bsy);
         const float bw = pfd_expf(__fmul_rn(__fmul_rn(-0.007368f, tb), tb));
-        c = clamp_cost(__fmaf_rn(2.0f, __fsub_rn(1.0f, bw), c));
+        c = clamp_cost(__fmaf_rn(P.blur_gain, __fsub_rn(1.0f, bw), c));
     }
     return c;
 }
@@ -861,11 +861,13 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
                     if (c < best_cost) { best_cost = c; best_plane = cand[i]; best_min = S.wmin[i]; }
                 }
             }
-            if (partial) {
+            if (partial || (COUNT && P.acmm)) {
                 // proposals and refinement candidates were evaluated on the selected views
                 // only, which fixes their weighted cost; the winner's lowest-cost view runs
                 // over every view, and its vector is stored, so the whole vector is
-                // evaluated again (one NCC per lane, a single pass over the taps)
+                // evaluated again (one NCC per lane, a single pass over the taps).  Tap
+                // counting in the ACMM matcher evaluates it always: that matcher's
+                // write-back evaluates the final plane on every view.
                 __syncwarp();
                 if (lane == 0) S.plane[0] = best_plane;
                 __syncwarp();
@@ -878,14 +880,49 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             // the stored vector of the new current plane (unchanged when the current
             // plane stays and its stored vector was used)
             if (!COUNT && P.cvec && lane < nc && !(best_row == 0 && P.cvec_ok)) P.cvec[idx * K + lane] = best_vec;
+            // ACMM write-back (AdaptMIPMFrameACMM.cu:880-900, RecomputeSupportCostDisp_Frame
+            // :259-280): the final plane's vector over every view (best_vec) gives the
+            // stored cost (mean of the top-k), the selected views (the top-k mask) and the
+            // disp of the lowest-cost view; DetailRestorer_FrameACMM does nothing
+            // without a warm start
+            float acv[kMaxNb];
+            if (P.acmm)
+                for (int i = 0; i < nc; ++i) acv[i] = __shfl_sync(kFullMask, best_vec, i);
             if (lane == 0) {
+                uint32_t sel_out = tsel;
+                float cost_out = best_cost;
+                int disp_view = best_min;
+                if (P.acmm) {
+                    disp_view = -1;
+                    int valid = 0;
+                    for (int i = 0; i < nc; ++i)
+                        if (acv[i] < 2.0f) {
+                            ++valid;
+                            if (disp_view < 0 || acv[i] < acv[disp_view]) disp_view = i;
+                        }
+                    cost_out = 2.0f;
+                    sel_out = 0;
+                    if (valid > 0) {
+                        const int kk = min(valid, P.top_k);
+                        float tmp[kMaxNb];
+                        for (int i = 0; i < nc; ++i) tmp[i] = acv[i];
+                        for (int i = 0; i < kk; ++i)
+                            for (int j = i + 1; j < nc; ++j)
+                                if (tmp[j] < tmp[i]) { const float t = tmp[i]; tmp[i] = tmp[j]; tmp[j] = t; }
+                        float m = 0.0f;
+                        for (int i = 0; i < kk; ++i) m = __fadd_rn(m, tmp[i]);
+                        cost_out = __fdiv_rn(m, (float)kk);
+                        for (int i = 0; i < nc; ++i)
+                            if (acv[i] <= tmp[kk - 1]) sel_out |= 1u << i;
+                    }
+                }
                 float4 best_disp = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (best_min >= 0)
-                    best_disp = geo_disp(T.geo[best_min], x, y, to_disparity(x, y, disparity_plane(x, y, best_plane)));
+                if (disp_view >= 0)
+                    best_disp = geo_disp(T.geo[disp_view], x, y, to_disparity(x, y, disparity_plane(x, y, best_plane)));
                 next.plane[idx] = best_plane;
-                next.cost[idx] = best_cost;
+                next.cost[idx] = cost_out;
                 next.disp[idx] = best_disp;
-                next.sel[idx] = tsel;
+                next.sel[idx] = sel_out;
             }
             __syncwarp();
         }
