@@ -28,7 +28,7 @@ CPP_SOURCES = ["neighbors.cpp", "server.cpp"]
 SYNTH_LIB = os.path.join(OUT, "libpfd_synth.so")
 HOST_DIR = os.path.join(PKG_DIR, "host")
 HOST_LIB = os.path.join(OUT, "libpfd_host.so")
-HOST_SOURCES = ["lf_types.cpp", "frame_views.cpp", "AdaptMIPMFrame.cpp", "MIDisparityFilter.cpp", "MICycleCheck.cpp"]
+HOST_SOURCES = ["lf_types.cpp", "frame_views.cpp", "AdaptMIPMFrame.cpp", "AdaptMIPMFrameACMM.cpp", "MIDisparityFilter.cpp", "MICycleCheck.cpp"]
 GXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-parameter",
              "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include"]
 

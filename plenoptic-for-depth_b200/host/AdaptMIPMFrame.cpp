@@ -192,7 +192,8 @@ void AdaptMIPMFrame::RunPatchMatchCUDAForFrame()
     p.depth_min = params.depth_min;
     p.depth_max = params.depth_max;
     p.base = params.Base;
-    pfd_status st = pfd_patchmatch(m_ctx, m_frame_id, &p, m_seed);
+    pfd_status st = pfd_set_matcher(m_ctx, PFD_MATCHER_FRAME);
+    if (st == PFD_OK) st = pfd_patchmatch(m_ctx, m_frame_id, &p, m_seed);
     if (st == PFD_OK)
         st = pfd_download(m_ctx, m_frame_id, &plane_final_host[0].x, cost_final_host.data(), &disp_final_host[0].x,
                           selected_final_host.data());

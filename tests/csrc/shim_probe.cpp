@@ -6,11 +6,13 @@
 // MIStereoMatch::StereoMatchingForMIA_FrameCrossViews and FilterAndStatic use
 // them, and returns the results as flat arrays, so the Python tests can compare
 // them with the engine's C ABI called directly.
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <vector>
 
 #include "../../include/pfd/AdaptMIPMFrame.h"
+#include "../../include/pfd/AdaptMIPMFrameACMM.h"
 #include "../../include/pfd/MICycleCheck.h"
 #include "../../include/pfd/MIDisparityFilter.h"
 #include "../../include/pfd_abi.h"
@@ -182,6 +184,36 @@ int shim_check_layout(int n, int mi, float pitch, const int* keys, const float* 
         }
     }
     return (int)v.keys.size();
+}
+
+// MIStereoMatch::StereoMatchingForMIA_FrameCrossViews_ACMM through the class:
+// AdaptMIPMFrameACMM Initialize / RunPatchMatchCUDAForFrameACMM /
+// WriteBackResults / ReleaseMemory with the reference's own parameters and the
+// given seed.  dn_match [n][mi*mi][13] as in shim_run; levels receives
+// GetNumLevels().  Returns 0, or -1 with msg (256 bytes) filled.
+int shim_run_acmm(int n, int mi, float pitch, const int* keys, const float* centers, const uint8_t* flags,
+                  const uint8_t* gray, const int* nb_off, const int* nb_keys, const float* dn_init,
+                  unsigned long long seed, float* dn_match, int* levels, char* msg)
+{
+    Scene s;
+    build(s, n, mi, pitch, keys, centers, flags, gray, nb_off, nb_keys, dn_init);
+    AdaptMIPMFrameACMM acmm(s.lfp);
+    acmm.SetRandomSeed(seed);
+    const bool ok = acmm.Initialize(s.info, s.problems);
+    *levels = acmm.GetNumLevels();
+    if (!ok) {
+        std::snprintf(msg, 256, "%s", acmm.LastError().c_str());
+        return -1;
+    }
+    acmm.RunPatchMatchCUDAForFrameACMM();
+    if (!acmm.LastError().empty()) {
+        std::snprintf(msg, 256, "%s", acmm.LastError().c_str());
+        return -1;
+    }
+    acmm.WriteBackResults(s.dns);
+    acmm.ReleaseMemory();
+    dump_dns(s, mi, dn_match);
+    return 0;
 }
 
 // The matching path end to end through the classes:

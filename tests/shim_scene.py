@@ -30,7 +30,9 @@ def load_probe(pfd):
         L.shim_run.argtypes = ([ctypes.c_int, ctypes.c_int, ctypes.c_float] + [_P] * 7 +
                                [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                 ctypes.c_ulonglong] + [_P] * 8)
-        for f in (L.shim_match_layout, L.shim_check_layout, L.shim_run):
+        L.shim_run_acmm.argtypes = ([ctypes.c_int, ctypes.c_int, ctypes.c_float] + [_P] * 7 +
+                                    [ctypes.c_ulonglong] + [_P] * 3)
+        for f in (L.shim_match_layout, L.shim_check_layout, L.shim_run, L.shim_run_acmm):
             f.restype = ctypes.c_int
         _probe = L
     return _probe

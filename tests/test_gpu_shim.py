@@ -197,3 +197,41 @@ def test_disparity_filter_matches_the_engine_and_the_oracle(pfd, oracle, shim):
     assert fs[10] == s / e.size
     assert fs[11] == np.sqrt(sq / e.size)
     assert fs[12] == _quantile(np.sort(e), 0.9)
+
+
+def test_adapt_mipm_frame_acmm_matches_the_engine(pfd, oracle):
+    """AdaptMIPMFrameACMM with the reference's own level parameters (one level
+    below a 24-pixel window: patch 5, 5 iterations, top_k 6, PatchMatchParamsLF's
+    sigmas 5 and 3) against PFD_MATCHER_ACMM called directly on the same views,
+    and both against the oracle's ACMM mode."""
+    L = load_probe(pfd)
+    w, sc = irregular_scene(pfd)
+    n, ppv = sc.n, sc.mi * sc.mi
+    dn = np.full((n, ppv, 13), np.nan, np.float32)
+    levels = ctypes.c_int(0)
+    msg = ctypes.create_string_buffer(256)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = L.shim_run_acmm(*sc.args(), p(sc.dn_init), SEED, p(dn), ctypes.byref(levels), msg)
+    assert rc == 0, msg.value.decode()
+    assert levels.value == 1
+    views, lists = sc.expected_match_layout()
+    centers, keys, ids, cnt, gray = sc.frame_arrays(views, lists, 16)
+    P = pfd.PmParams(base=sc.pitch, patch_size=5, max_iterations=5, top_k=6, sigma_spatial=5.0, sigma_color=3.0)
+    with pfd.Context(0) as ctx:
+        fid = ctx.frame_upload(w.frame.raw, centers, keys, sc.mi, sc.mi, ids, cnt)
+        ctx.set_matcher(True)
+        ctx.patchmatch(fid, P, seed=SEED)
+        plane, cost, disp, sel = ctx.download(fid)
+        ctx.frame_free(fid)
+    st = oracle.Oracle(gray, centers, ids, cnt, acmm=True).patchmatch(P, SEED)
+    assert _same(plane, st["plane"]) and _same(cost, st["cost"]) and _same(sel, st["sel"])
+    assert np.mean(cost < 1.0) > 0.3
+    for v, pi in enumerate(views):
+        s = slice(v * ppv, (v + 1) * ppv)
+        if not sc.flags[pi] & HAS_DN:
+            continue
+        assert _same(dn[pi, :, 0:4], plane[s]), f"problem {pi}: ph_cuda differs"
+        assert _same(dn[pi, :, 5], cost[s]), f"problem {pi}: c_cuda differs"
+        assert _same(dn[pi, :, 6:10], disp[s]), f"problem {pi}: disp_v_cuda differs"
+        assert np.array_equal(dn[pi, :, 10].view(np.uint32), sel[s]), f"problem {pi}: selected_views differs"
+        assert np.all(dn[pi, :, 11] == 1.0)                   # eSS_ACMH_Finished

@@ -86,3 +86,21 @@ def test_empty_maps(pfd):
     assert nv == -1                      # Initialize fails: no valid micro-images
     nv, view_of, _, _ = _layout(L, L.shim_check_layout, sc, 32)
     assert nv == 0 and view_of[0] == -1  # the checks check nothing
+
+
+def test_acmm_class_refuses_two_level_windows(pfd):
+    """AdaptMIPMFrameACMM counts its pyramid levels as BuildBlurAlignedPyramids
+    does (AdaptMIPMFrameACMM.cpp:312-321): a 24-pixel window (pitch 34) takes
+    two, which is not built, so Initialize fails before any device work."""
+    import ctypes
+    L = load_probe(pfd)
+    w, sc = irregular_scene(pfd, width=420, height=320, pitch=34.0)
+    assert sc.mi == 24
+    n, ppv = sc.n, sc.mi * sc.mi
+    dn = np.zeros((n, ppv, 13), np.float32)
+    levels = ctypes.c_int(0)
+    msg = ctypes.create_string_buffer(256)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = L.shim_run_acmm(*sc.args(), p(sc.dn_init), 1, p(dn), ctypes.byref(levels), msg)
+    assert rc == -1 and levels.value == 2
+    assert b"two-level" in msg.value
