@@ -408,11 +408,41 @@ def run_engine(args, rank, world, local_rank):
             smp = cs.run()
             result["cpu_baseline"] = {"value": round(1.0 / smp["frame_s"], 8), "unit": "frames/s", "cores": nth,
                                       "kind": "port", "sample": cs.describe(smp)}
+    if result is not None and world == 1:
+        result["acmm"] = acmm_leg(pfd, ctx, fid, raw_dev, stream, seed)
     ctx.frame_free(fid)
     ctx.close()
     if result is not None and world == 1 and not args.no_serving:
         result["serving"] = serving_leg(pfd)
     return result
+
+
+def acmm_leg(pfd, ctx, fid, raw_dev, stream, seed, reps=3):
+    """The ACMM matcher (PFD_MATCHER_ACMM, one pyramid level) on the same
+    resident frame with the parameters AdaptMIPMFrameACMM uses at one level
+    (patch 5, 5 iterations, top_k 6, PatchMatchParamsLF's sigmas 5 and 3):
+    initialisation, 10 half-sweeps and the post-refine pass, device-timed."""
+    import torch
+    P = pfd.PmParams(base=WORKLOAD["pitch"], patch_size=5, max_iterations=5, top_k=6, sigma_spatial=5.0,
+                     sigma_color=3.0)
+    ctx.set_matcher(True)
+    try:
+        ctx.frame_set_raw_device(fid, raw_dev.data_ptr(), raw_dev.shape[1])
+        ctx.patchmatch(fid, P, seed)                  # warm-up
+        ctx.sync()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            ctx.patchmatch(fid, P, seed)
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b) / reps
+    finally:
+        ctx.set_matcher(False)
+    return {"matcher": "AdaptMIPMFrameACMM, one pyramid level", "patch": 5, "iterations": 5, "top_k": 6,
+            "ms_per_frame": round(ms, 2), "frames_per_s": round(1000.0 / ms, 3),
+            "covers": "init + 10 half-sweeps + post-refine (matching only, no checks or focal stack)"}
 
 
 def serving_leg(pfd, n_req=16, slots=4, seed=7):

@@ -195,6 +195,9 @@ def lib() -> ctypes.CDLL:
             "pfd_frame_compute_blur": [_P, _I, _P, _P],
             "pfd_set_ncc_moments": [_P, _I],
             "pfd_set_matcher": [_P, _I],
+            "pfd_read_intrinsics_xml": [ctypes.c_char_p, _P],
+            "pfd_read_calib_xml": [ctypes.c_char_p, _P, _I, ctypes.POINTER(_I)],
+            "pfd_write_calib_xml": [_P, _P, _I, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)],
             "pfd_acmm_post_refine": [_P, _I, ctypes.POINTER(PmParamsC)],
             "pfd_state_upload": [_P, _I, _P, _P, _P, _P],
             "pfd_frame_upload": [_P, ctypes.POINTER(_I), _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _I, _P],
@@ -265,6 +268,61 @@ def neighbors_by_baseline(centers: np.ndarray, tilekeys: np.ndarray, pitch: floa
     if rc != PFD_OK:
         raise PfdError(rc, "pfd_neighbors_by_baseline")
     return ids, cnt
+
+
+class IntrinsicsC(ctypes.Structure):
+    _fields_ = [("D", ctypes.c_float), ("d", ctypes.c_float), ("sensor_rotation", ctypes.c_double * 9),
+                ("sensor_translate", ctypes.c_double * 3), ("sensor_pixel_size", ctypes.c_float),
+                ("mainlen_focal_length", ctypes.c_float), ("mla_u_size", _I), ("mla_v_size", _I),
+                ("baseline", ctypes.c_float), ("distor_depth", ctypes.c_double * 3),
+                ("distor_radial", ctypes.c_double * 3), ("distor_tangential", ctypes.c_double * 2),
+                ("has_mia", _I)]
+
+
+MLA_ENTRY = np.dtype([("col", np.int32), ("row", np.int32), ("cx", np.float32), ("cy", np.float32),
+                      ("type", np.int32), ("area", np.float32), ("blur_radius", np.float32)])
+
+
+def read_intrinsics_xml(text: str) -> dict:
+    """intrinsics.xml (include/pfd_calib.h) as a dict of its fields."""
+    out = IntrinsicsC()
+    rc = lib().pfd_read_intrinsics_xml(text.encode(), ctypes.byref(out))
+    if rc != PFD_OK:
+        raise PfdError(rc, "pfd_read_intrinsics_xml")
+    d = {}
+    for name, _t in IntrinsicsC._fields_:
+        v = getattr(out, name)
+        d[name] = list(v) if isinstance(v, ctypes.Array) else v
+    return d
+
+
+def read_calib_xml(text: str) -> np.ndarray:
+    """CalibInfo.xml lenses in the reference's map order (structured array MLA_ENTRY)."""
+    n = _I(0)
+    b = text.encode()
+    rc = lib().pfd_read_calib_xml(b, None, 0, ctypes.byref(n))
+    if rc != PFD_OK:
+        raise PfdError(rc, "pfd_read_calib_xml")
+    out = np.zeros(n.value, MLA_ENTRY)
+    rc = lib().pfd_read_calib_xml(b, _ptr(out), n.value, ctypes.byref(n))
+    if rc != PFD_OK:
+        raise PfdError(rc, "pfd_read_calib_xml")
+    return out
+
+
+def write_calib_xml(lenses: np.ndarray, abandon=None) -> str:
+    """CalibInfo.xml text of the lenses (structured array MLA_ENTRY)."""
+    L = np.ascontiguousarray(lenses, MLA_ENTRY)
+    ab = None if abandon is None else np.ascontiguousarray(abandon, np.int32)
+    n = ctypes.c_size_t(0)
+    rc = lib().pfd_write_calib_xml(_ptr(L), _ptr(ab), len(L), None, 0, ctypes.byref(n))
+    if rc != PFD_OK:
+        raise PfdError(rc, "pfd_write_calib_xml")
+    buf = ctypes.create_string_buffer(n.value + 1)
+    rc = lib().pfd_write_calib_xml(_ptr(L), _ptr(ab), len(L), buf, n.value + 1, ctypes.byref(n))
+    if rc != PFD_OK:
+        raise PfdError(rc, "pfd_write_calib_xml")
+    return buf.value.decode()
 
 
 class Context:

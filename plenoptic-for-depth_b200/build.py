@@ -24,7 +24,7 @@ NVCC_FLAGS = [
 ]
 
 CU_SOURCES = ["pm_kernels.cu", "pm_sweep.cu", "check_kernels.cu", "refocus_kernels.cu", "vdrd_kernels.cu", "fuse_kernels.cu", "mla_kernels.cu", "select_kernels.cu", "blur_kernels.cu", "pfd_abi.cu", "diag.cu"]
-CPP_SOURCES = ["neighbors.cpp", "server.cpp"]
+CPP_SOURCES = ["neighbors.cpp", "server.cpp", "calib_xml.cpp"]
 SYNTH_LIB = os.path.join(OUT, "libpfd_synth.so")
 HOST_DIR = os.path.join(PKG_DIR, "host")
 HOST_LIB = os.path.join(OUT, "libpfd_host.so")
