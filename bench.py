@@ -222,6 +222,24 @@ def cpu_threads() -> int:
 STAGES = ("slice+init", "patchmatch sweeps", "cycle check", "filter", "reprojection map", "focal stack")
 
 
+def job_time(local: float, world: int, device: str) -> float:
+    """Time of the whole job over replicas: the slowest rank's (one all_reduce
+    MAX over the process group; the local time when there is one rank)."""
+    if world <= 1:
+        return float(local)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(local)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(frames_per_rank: int, world: int, job_s: float) -> float:
+    """Whole-job frames/s: every rank matched frames_per_rank frames of its own
+    (replicas, no data exchanged) within the job time."""
+    return world * frames_per_rank / job_s
+
+
 def run_engine(args, rank, world, local_rank):
     import ctypes
     import torch
@@ -312,10 +330,8 @@ def run_engine(args, rank, world, local_rank):
     for name, (a, b) in zip(STAGES, [("t0", "t1"), ("t1", "t2"), ("t2", "t3"), ("t3", "t4"), ("t4", "t5"),
                                      ("t5", "t6")]):
         stage_ms[name] = round(statistics.mean(x.elapsed_time(y) for x, y in zip(ev[a], ev[b])), 3)
+    ms = job_time(ms, world, f"cuda:{local_rank}")
     if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
 
     # e2e through the public API with host buffers: pinned raw frame in; the
@@ -351,15 +367,12 @@ def run_engine(args, rank, world, local_rank):
     for _ in range(e2e_steps):
         e2e_step()
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = job_time(e2e_s, world, f"cuda:{local_rank}")
 
     result = None
     if rank == 0:
         frames = world * args.steps
-        value = frames / (ms / 1e3)
+        value = replica_throughput(args.steps, world, ms / 1e3)
         # roofline of the dominant kernel (the red-black sweep)
         avg_sweep_ms = statistics.mean(sweep_ms)
         taps_per_launch = statistics.mean(sweep_taps)
@@ -386,7 +399,7 @@ def run_engine(args, rank, world, local_rank):
                              (px * 40 * 2 / 1e9 + len(vds) * ow * oh * 4 / 1e9),
                        "stages": list(STAGES)},
             "stage_ms": stage_ms,
-            "e2e": {"value": round(world * e2e_steps / e2e_s, 4), "unit": "frames/s",
+            "e2e": {"value": round(replica_throughput(e2e_steps, world, e2e_s), 4), "unit": "frames/s",
                     "h2d_bytes_per_step": int(w.frame.raw.nbytes),
                     "d2h_bytes_per_step": int(out_plane.numel() * 4 + out_cost.numel() * 4 + out_sel.numel() * 4 +
                                               out_stack.numel() * 4)},
