@@ -466,7 +466,9 @@ def serving_leg(pfd, n_req=16, slots=4, seed=7):
     one-slot server (the plain method: one frame at a time, in arrival order).
     Returns frames/s over the makespan and p50/p99 latency (submission to
     result) for both; results are bit-identical between the two (each request
-    computes exactly what it computes alone)."""
+    computes exactly what it computes alone).  The same requests are then sent
+    as a Poisson stream at 90% of the plain method's throughput, to both
+    servers, for latency under a steady arrival rate."""
     import time
     rs = np.random.RandomState(seed)
     shapes = [(1024, 768), (1024, 768), (2048, 1536), (2048, 1536), (4080, 3068)]
@@ -482,11 +484,15 @@ def serving_leg(pfd, n_req=16, slots=4, seed=7):
         idx = int(rs.choice(len(pool), p=[0.3, 0.3, 0.15, 0.15, 0.1]))
         reqs.append((idx, int(rs.randint(4, 13)), 1000 + r))
 
-    def run(n_slots):
+    def run(n_slots, arrivals=None):
         with pfd.Server(0, hbm_budget=150 << 30, slots=n_slots) as srv:
             t0 = time.perf_counter()
             tickets = []
-            for idx, iters, sd in reqs:
+            for r, (idx, iters, sd) in enumerate(reqs):
+                if arrivals is not None:
+                    delay = t0 + arrivals[r] - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
                 w, pitch, patch = pool[idx]
                 P = pfd.PmParams(base=pitch, patch_size=patch, max_iterations=iters)
                 tickets.append(srv.submit(w, P, sd, filter_cfg=pfd.FilterCfg(), baseline_unit=pitch))
@@ -498,6 +504,11 @@ def serving_leg(pfd, n_req=16, slots=4, seed=7):
     run(slots)                                    # warm-up: contexts, pinned pool, memory pool
     served = run(slots)
     plain = run(1)
+    # the same requests arriving as a Poisson stream at 90% of the plain method's rate
+    rate = 0.9 * plain["frames_per_s"]
+    arrivals = np.cumsum(np.random.RandomState(seed + 1).exponential(1.0 / rate, len(reqs)))
+    served_p = run(slots, arrivals)
+    plain_p = run(1, arrivals)
     sizes = [pool[i][0].frame.raw.shape for i, _, _ in reqs]
     return {"requests": len(reqs), "arrival": "all at once",
             "mix": "%d x 1024x768, %d x 2048x1536, %d x 4080x3068; 4-12 iterations, filter" %
@@ -505,6 +516,7 @@ def serving_leg(pfd, n_req=16, slots=4, seed=7):
                     sum(1 for s in sizes if s[1] == 4080)),
             "served": dict(served, slots=slots), "plain": plain,
             "speedup": round(served["frames_per_s"] / plain["frames_per_s"], 3),
+            "poisson": {"rate_per_s": round(rate, 3), "served": dict(served_p, slots=slots), "plain": plain_p},
             "depth_error": "identical (bit-exact per request)"}
 
 

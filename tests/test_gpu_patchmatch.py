@@ -250,3 +250,36 @@ def test_hbm_budget_enforced(pfd):
             _upload(small, w)
         assert e.value.code == -2
         assert small.bytes_in_use() == 0
+
+
+@pytest.mark.parametrize("K", [16, 32])
+def test_neighbour_count_extremes_bitexact(pfd, oracle, ctx, K):
+    """Lists of 16 (the reference's m_max_neighbors) and 32 neighbours (the
+    selected-view mask width), with views that have none or one: init and a
+    full iteration bit-exact with the oracle (views without neighbours keep
+    their state)."""
+    pitch = 23.0
+    w = _workload(pfd, 300, 240, pitch, K=6, seed=50 + K)
+    ids, cnt = pfd.neighbors_by_baseline(w.centers, w.tilekeys, pitch, K, rings=4)
+    V = w.centers.shape[0]
+    cnt = cnt.copy()
+    cnt[::7] = 0
+    cnt[3::11] = np.minimum(cnt[3::11], 1)
+    ids = ids.copy()
+    for v in range(V):
+        ids[v, cnt[v]:] = -1
+    assert cnt.max() == K
+    fid = ctx.frame_upload(w.frame.raw, w.centers, w.tilekeys, w.mi, w.mi, ids, cnt)
+    P = pfd.PmParams(base=pitch, patch_size=9, max_iterations=1)
+    orc = oracle.Oracle(w.gray, w.centers, ids, cnt)
+    seed = 77
+    try:
+        ctx.pm_init(fid, P, seed)
+        st = orc.init(P, seed)
+        _state_equal(ctx.download(fid), st, f"init K={K}")
+        for ph in range(2):
+            ctx.pm_sweep(fid, P, seed, 0, ph)
+            st = orc.sweep(P, seed, 0, ph, st)
+            _state_equal(ctx.download(fid), st, f"sweep 0.{ph} K={K}")
+    finally:
+        ctx.frame_free(fid)
