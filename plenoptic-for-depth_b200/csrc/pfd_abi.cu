@@ -84,6 +84,7 @@ struct pfd_ctx {
     std::map<int, Frame> frames;
     int* d_err = nullptr;
     unsigned long long* d_taps = nullptr;   // tap counter of calibration runs
+    int* d_vq = nullptr;                    // sweep: next micro-image to take (reset before each launch)
     bool counting = false;
     int ncc_moments = PFD_NCC_REFERENCE;    // accumulation of the NCC moments (pfd_set_ncc_moments)
     int matcher = PFD_MATCHER_FRAME;        // PatchMatch rules (pfd_set_matcher)
@@ -213,6 +214,7 @@ pfd::PmParams make_params(const pfd_ctx* ctx, const Frame& f, const pfd_pm_param
     P.tap_counter = nullptr;
     P.cost_scratch = nullptr;
     P.cvec = f.d_cvec;
+    P.view_queue = ctx->d_vq;
     P.cvec_ok = 0;
     return P;
 }
@@ -305,11 +307,13 @@ pfd_status pfd_create(pfd_ctx** out, int device, size_t hbm_budget_bytes)
         cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess ||
         cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&ctx->d_taps, sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMemset(ctx->d_taps, 0, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaMemset(ctx->d_taps, 0, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_vq, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
         if (ctx->d_err) cudaFree(ctx->d_err);
         if (ctx->d_taps) cudaFree(ctx->d_taps);
+        if (ctx->d_vq) cudaFree(ctx->d_vq);
         delete ctx;
         return PFD_ECUDA;
     }
@@ -327,6 +331,7 @@ void pfd_destroy(pfd_ctx* ctx)
     cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->d_err);
     cudaFree(ctx->d_taps);
+    cudaFree(ctx->d_vq);
     if (ctx->d_scratch) cudaFreeAsync(ctx->d_scratch, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);

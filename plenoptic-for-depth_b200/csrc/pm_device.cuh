@@ -34,6 +34,7 @@ struct PmParams {
     float* cvec;            // [V * ppv][K]: cost vector of each pixel's current plane (init and sweeps write it)
     int cvec_ok;            // sweep: cvec holds the vectors of the updated colour's current planes
     int shifted;            // 0: the reference's raw NCC moments; 1: moments of (pixel - centre pixel)
+    int* view_queue;        // sweep: micro-images are handed out in order from this counter (zeroed per launch)
     float blur_gain;        // blur penalty gain: 2 (Frame matcher), 0.8 (ACMM matcher)
     int acmm;               // 1: ACMM write-back (top-k cost, views and disp of the final plane)
 };

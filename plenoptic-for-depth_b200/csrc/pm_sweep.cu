@@ -590,7 +590,15 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
     }
 
     uint32_t parity = 0;
-    for (int vid = blockIdx.x; vid < F.V; vid += gridDim.x) {
+    // the CTAs take micro-images one at a time from a shared counter, so a CTA that
+    // drew cheap ones takes more (their cost varies with the neighbour count and the
+    // candidates); which CTA updates a micro-image does not change its result
+    for (;;) {
+        __syncthreads();                         // every thread has read the previous id
+        if (threadIdx.x == 0) ctl[1] = atomicAdd(P.view_queue, 1);
+        __syncthreads();
+        const int vid = ctl[1];
+        if (vid >= F.V) break;
         const int nc = min(F.nb_counts[vid], K);
         const size_t vbase = (size_t)vid * P.ppv;
         // the other colour keeps its state; so does every pixel of a view without neighbours
@@ -972,6 +980,8 @@ cudaError_t launch_sweep_warp(const FrameDev& F, const PmParams& P, const StateD
     const int smem = sweep_warp_smem_bytes(P, blur);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     const int grid = std::max(1, std::min(n_ctas, F.V));
+    cudaError_t qe = cudaMemsetAsync(P.view_queue, 0, sizeof(int), st);
+    if (qe != cudaSuccess) return qe;
     FrameDev f = F; PmParams p = P; StateDev a = prev, b = next; int it = iter, ph = phase; int* e = err;
     void* args[] = { &f, &p, &a, &b, &it, &ph, &e };
     if (P.tap_counter) {
