@@ -144,6 +144,18 @@ pfd_status pfd_frame_free(pfd_ctx* ctx, int frame_id);
  * (red half-sweep, black half-sweep), enqueued without host synchronisation.
  * seed keys the Philox streams (the reference seeds cuRAND from clock64()). */
 pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed);
+/* pfd_patchmatch of n frames of the context at once (no counterpart in the
+ * reference, which matches one frame at a time): every frame is initialised,
+ * then each half-sweep is ONE persistent launch over all the frames that still
+ * have iterations left (frames with a blur channel and frames without take one
+ * launch each), in which a CTA that finds one frame's micro-images all taken
+ * moves straight on to the next frame, so small frames and the tails of large
+ * ones do not leave the GPU idle between launches.  params[b] and seeds[b] are
+ * frame b's own (sizes, neighbour counts, patch sizes and iteration counts may
+ * all differ); every frame's result is bit for bit what pfd_patchmatch gives it
+ * alone.  Tap counting (pfd_set_tap_counting) runs the frames one by one. */
+pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const pfd_pm_params* params,
+                                const uint64_t* seeds);
 /* The steps of pfd_patchmatch, separately: RandomInitializationForFrame
  * (AdaptMIPMFrame.cu:474-518) and one CheckerboardUpdateFrame launch (:520-947). */
 pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed);

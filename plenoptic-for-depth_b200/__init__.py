@@ -195,6 +195,7 @@ def lib() -> ctypes.CDLL:
             "pfd_frame_compute_blur": [_P, _I, _P, _P],
             "pfd_set_ncc_moments": [_P, _I],
             "pfd_set_matcher": [_P, _I],
+            "pfd_patchmatch_batch": [_P, _P, _I, _P, _P],
             "pfd_read_intrinsics_xml": [ctypes.c_char_p, _P],
             "pfd_read_calib_xml": [ctypes.c_char_p, _P, _I, ctypes.POINTER(_I)],
             "pfd_write_calib_xml": [_P, _P, _I, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)],
@@ -464,6 +465,14 @@ class Context:
         reference's raw moments (PFD_NCC_REFERENCE, the default) for the
         context's later initialisations, sweeps and cost queries."""
         self._check(self._L.pfd_set_ncc_moments(self._h, 1 if shifted else 0), "pfd_set_ncc_moments")
+
+    def patchmatch_batch(self, fids, params, seeds) -> None:
+        """pfd_patchmatch of several frames, one launch per half-sweep over all of them."""
+        ids = np.ascontiguousarray(fids, np.int32)
+        arr = (PmParamsC * len(ids))(*[p.c() for p in params])
+        sd = np.ascontiguousarray(seeds, np.uint64)
+        self._check(self._L.pfd_patchmatch_batch(self._h, _ptr(ids), len(ids), ctypes.cast(arr, _P), _ptr(sd)),
+                    "pfd_patchmatch_batch")
 
     def set_matcher(self, acmm: bool) -> None:
         """PatchMatch rules of the context's later calls: the ACMM matcher at one

@@ -213,6 +213,8 @@ pfd::PmParams make_params(const pfd_ctx* ctx, const Frame& f, const pfd_pm_param
     P.seed = seed;
     P.tap_counter = nullptr;
     P.cost_scratch = nullptr;
+    P.scratch_floats = 0;
+    P.scratch_stride = pfd::sweep_warp_stride(f.K);
     P.cvec = f.d_cvec;
     P.view_queue = ctx->d_vq;
     P.cvec_ok = 0;
@@ -267,6 +269,9 @@ pfd_status check_device_error(pfd_ctx* ctx)
         if (h == PFD_DEVERR_REFOCUS_LENSES)
             return fail(ctx, PFD_EINVAL, "refocus: more than %d lenses reach one output tile (slice virtual depth "
                         "too large for this lens density)", pfd::kMaxRefocusCand);
+        if (h & PFD_DEVERR_SWEEP_CHECK)
+            return fail(ctx, PFD_ECUDA, "sweep launch refused its work: shared-memory plan, scratch or neighbour "
+                        "ids out of range (flags 0x%x)", h);
         return fail(ctx, PFD_ETIMEDOUT, "device wait timed out (flags 0x%x)", h);
     }
     return PFD_OK;
@@ -656,6 +661,26 @@ pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, 
     return PFD_OK;
 }
 
+// The context's sweep scratch, grown to `need` bytes when smaller.
+static pfd_status ensure_scratch(pfd_ctx* ctx, size_t need)
+{
+    if (need <= ctx->scratch_bytes) return PFD_OK;
+    if (ctx->budget && ctx->used - ctx->scratch_bytes + need > ctx->budget)
+        return fail(ctx, PFD_ENOMEM, "HBM budget exceeded by %zu bytes of sweep scratch", need);
+    // stream-ordered, like the frames: other contexts' work keeps running
+    if (ctx->d_scratch) cudaFreeAsync(ctx->d_scratch, ctx->stream);
+    ctx->used -= ctx->scratch_bytes;
+    ctx->d_scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    if (cudaMallocAsync((void**)&ctx->d_scratch, need, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, PFD_ENOMEM, "cudaMallocAsync(%zu) for sweep scratch failed", need);
+    }
+    ctx->scratch_bytes = need;
+    ctx->used += need;
+    return PFD_OK;
+}
+
 pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed, int iter, int phase)
 {
     if (!ctx) return PFD_EINVAL;
@@ -673,23 +698,10 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
     int n_ctas = 0;
     CU(pfd::sweep_warp_grid(P, f->has_blur, &n_ctas));
-    const size_t need = pfd::sweep_warp_scratch_bytes(P, n_ctas);
-    if (need > ctx->scratch_bytes) {
-        if (ctx->budget && ctx->used - ctx->scratch_bytes + need > ctx->budget)
-            return fail(ctx, PFD_ENOMEM, "HBM budget exceeded by %zu bytes of sweep scratch", need);
-        // stream-ordered, like the frames: other contexts' work keeps running
-        if (ctx->d_scratch) cudaFreeAsync(ctx->d_scratch, ctx->stream);
-        ctx->used -= ctx->scratch_bytes;
-        ctx->d_scratch = nullptr;
-        ctx->scratch_bytes = 0;
-        if (cudaMallocAsync((void**)&ctx->d_scratch, need, ctx->stream) != cudaSuccess) {
-            cudaGetLastError();
-            return fail(ctx, PFD_ENOMEM, "cudaMallocAsync(%zu) for sweep scratch failed", need);
-        }
-        ctx->scratch_bytes = need;
-        ctx->used += need;
-    }
+    st = ensure_scratch(ctx, pfd::sweep_warp_scratch_bytes(P, n_ctas));
+    if (st != PFD_OK) return st;
     P.cost_scratch = ctx->d_scratch;
+    P.scratch_floats = ctx->scratch_bytes / sizeof(float);
     P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, cost_mode(ctx));
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
@@ -706,6 +718,127 @@ pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* param
     for (int it = 0; st == PFD_OK && it < params->max_iterations; ++it)
         for (int ph = 0; ph < 2 && st == PFD_OK; ++ph) st = pfd_pm_sweep(ctx, frame_id, params, seed, it, ph);
     if (st == PFD_OK && ctx->matcher == PFD_MATCHER_ACMM) st = pfd_acmm_post_refine(ctx, frame_id, params);
+    return st;
+}
+
+pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const pfd_pm_params* params,
+                                const uint64_t* seeds)
+{
+    if (!ctx) return PFD_EINVAL;
+    if (n < 1 || n > 4096 || !frame_ids || !params || !seeds)
+        return fail(ctx, PFD_EINVAL, "patchmatch_batch: n must be in [1, 4096] and the arrays non-NULL");
+    std::vector<Frame*> fr(n);
+    for (int b = 0; b < n; ++b) {
+        fr[b] = find_frame(ctx, frame_ids[b]);
+        if (!fr[b]) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_ids[b]);
+        for (int c = 0; c < b; ++c)
+            if (frame_ids[c] == frame_ids[b]) return fail(ctx, PFD_EINVAL, "frame %d listed twice", frame_ids[b]);
+        const pfd_status st = check_params(ctx, *fr[b], &params[b]);
+        if (st != PFD_OK) return st;
+    }
+    if (ctx->counting) {                          // tap counting runs frame by frame
+        for (int b = 0; b < n; ++b) {
+            const pfd_status st = pfd_patchmatch(ctx, frame_ids[b], &params[b], seeds[b]);
+            if (st != PFD_OK) return st;
+        }
+        return PFD_OK;
+    }
+    DeviceGuard g(ctx->device);
+    for (int b = 0; b < n; ++b) {
+        const pfd_status st = pfd_pm_init(ctx, frame_ids[b], &params[b], seeds[b]);
+        if (st != PFD_OK) return st;
+    }
+    // per blur group: the largest shared-memory plan and the grid it allows
+    const bool shift = ctx->ncc_moments == PFD_NCC_SHIFTED;
+    int smem[2] = { 0, 0 }, n_ctas[2] = { 0, 0 }, half_sweeps = 0;
+    bool used[2] = { false, false };
+    size_t scratch = 0;
+    for (int b = 0; b < n; ++b) {
+        const int grp = fr[b]->has_blur ? 1 : 0;
+        const pfd::PmParams P = make_params(ctx, *fr[b], &params[b], seeds[b]);
+        const int sm = pfd::sweep_warp_smem_bytes(P, fr[b]->has_blur);
+        if (sm > 227 * 1024)
+            return fail(ctx, PFD_EINVAL, "frame %d: window %dx%d with %d neighbours does not fit shared memory",
+                        frame_ids[b], fr[b]->mi_w, fr[b]->mi_h, fr[b]->K);
+        smem[grp] = std::max(smem[grp], sm);
+        used[grp] = true;
+        half_sweeps = std::max(half_sweeps, 2 * params[b].max_iterations);
+    }
+    // one warp-scratch stride for every frame (the largest neighbour count's): CTAs of a
+    // launch work on different frames at once, and their regions must not overlap
+    int k_max = 0;
+    for (int b = 0; b < n; ++b) k_max = std::max(k_max, fr[b]->K);
+    const int stride = pfd::sweep_warp_stride(k_max);
+    for (int grp = 0; grp < 2; ++grp) {
+        if (!used[grp]) continue;
+        CU(pfd::sweep_batch_grid(smem[grp], grp == 1, shift, &n_ctas[grp]));
+        pfd::PmParams Pk = {};
+        Pk.K = k_max;                                  // the scratch of n_ctas CTAs at that stride
+        scratch = std::max(scratch, pfd::sweep_warp_scratch_bytes(Pk, n_ctas[grp]));
+    }
+    pfd_status st = ensure_scratch(ctx, scratch);
+    if (st != PFD_OK) return st;
+    if (half_sweeps == 0) return PFD_OK;
+    // one item and one queue counter per (half-sweep, frame), uploaded as the work is enqueued
+    pfd::SweepItem* d_items = nullptr;
+    int* d_queues = nullptr;
+    const size_t n_items = (size_t)half_sweeps * n;
+    if (cudaMallocAsync((void**)&d_items, sizeof(pfd::SweepItem) * n_items, ctx->stream) != cudaSuccess ||
+        cudaMallocAsync((void**)&d_queues, sizeof(int) * n_items, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        if (d_items) cudaFreeAsync(d_items, ctx->stream);
+        return fail(ctx, PFD_ENOMEM, "patchmatch_batch: %zu launch items", n_items);
+    }
+    CU(cudaMemsetAsync(d_queues, 0, sizeof(int) * n_items, ctx->stream));
+    std::vector<pfd::SweepItem> items;
+    const int mode = cost_mode(ctx);
+    for (int s = 0; s < half_sweeps && st == PFD_OK; ++s) {
+        const int iter = s / 2, phase = s % 2;
+        int count[2] = { 0, 0 };
+        items.clear();
+        for (int grp = 0; grp < 2; ++grp)
+            for (int b = 0; b < n; ++b) {
+                Frame& f = *fr[b];
+                if ((f.has_blur ? 1 : 0) != grp || s >= 2 * params[b].max_iterations) continue;
+                pfd::SweepItem it;
+                it.F = frame_dev(f);
+                it.P = make_params(ctx, f, &params[b], seeds[b]);
+                it.P.cost_scratch = ctx->d_scratch;
+                it.P.scratch_floats = ctx->scratch_bytes / sizeof(float);
+                it.P.scratch_stride = stride;
+                it.P.cvec_ok = cvec_usable(f, params[b], phase, mode);
+                it.P.view_queue = d_queues + (size_t)s * n + items.size();
+                it.prev = f.s[f.cur];
+                it.next = f.s[f.cur ^ 1];
+                it.iter = iter;
+                it.phase = phase;
+                items.push_back(it);
+                ++count[grp];
+                f.cur ^= 1;
+                cvec_swept(f, params[b], phase, mode);
+            }
+        pfd::SweepItem* row = d_items + (size_t)s * n;
+        if (cudaMemcpyAsync(row, items.data(), sizeof(pfd::SweepItem) * items.size(), cudaMemcpyHostToDevice,
+                            ctx->stream) != cudaSuccess) {
+            st = fail(ctx, PFD_ECUDA, "patchmatch_batch: item upload");
+            break;
+        }
+        for (int grp = 0, off = 0; grp < 2; off += count[grp], ++grp) {
+            if (!count[grp]) continue;
+            const cudaError_t e = pfd::launch_sweep_batch(row + off, count[grp], grp == 1, shift, smem[grp],
+                                                          n_ctas[grp], ctx->d_err, ctx->stream);
+            if (e != cudaSuccess) {
+                st = fail(ctx, PFD_ECUDA, "launch_sweep_batch: %s", cudaGetErrorString(e));
+                break;
+            }
+            ctx->launches += 1;
+        }
+    }
+    cudaFreeAsync(d_items, ctx->stream);
+    cudaFreeAsync(d_queues, ctx->stream);
+    if (st != PFD_OK) return st;
+    if (ctx->matcher == PFD_MATCHER_ACMM)
+        for (int b = 0; b < n && st == PFD_OK; ++b) st = pfd_acmm_post_refine(ctx, frame_ids[b], &params[b]);
     return st;
 }
 
@@ -1854,6 +1987,7 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     st = noalloc_scratch(ctx, ctx->device, &scratch);
     if (st != PFD_OK) return st;
     P.cost_scratch = scratch;
+    P.scratch_floats = kNoAllocScratchBytes / sizeof(float);
     P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, cost_mode(ctx));
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));

@@ -31,6 +31,8 @@ struct PmParams {
     uint64_t seed;
     unsigned long long* tap_counter;   // calibration runs only: in-bounds NCC taps evaluated
     float* cost_scratch;    // sweep: per warp, the cost vectors of its current pixel
+    size_t scratch_floats;  // sweep: floats cost_scratch holds (checked against the grid)
+    int scratch_stride;     // sweep: floats of cost_scratch per warp, the same for every frame of a launch
     float* cvec;            // [V * ppv][K]: cost vector of each pixel's current plane (init and sweeps write it)
     int cvec_ok;            // sweep: cvec holds the vectors of the updated colour's current planes
     int shifted;            // 0: the reference's raw NCC moments; 1: moments of (pixel - centre pixel)

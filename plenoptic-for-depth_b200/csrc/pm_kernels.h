@@ -6,6 +6,7 @@
 
 // Device-side error flags, OR-ed into the context's error word.
 #define PFD_DEVERR_TMA_TIMEOUT 0x1
+#define PFD_DEVERR_SWEEP_CHECK 0x10      // a sweep launch's shared-memory plan, scratch or neighbour ids did not fit
 
 namespace pfd {
 
@@ -23,8 +24,22 @@ cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, 
 cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas);
 int sweep_warp_smem_bytes(const PmParams& P, bool blur);
 size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas);
+// Floats of global scratch one warp uses for K neighbours (PmParams::scratch_stride).
+int sweep_warp_stride(int K);
 cudaError_t launch_sweep_warp(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
                               int iter, int phase, int n_ctas, int* err, cudaStream_t st);
+// One frame's half-sweep in a launch over several frames (pm_sweep_batch_kernel).
+struct SweepItem {
+    FrameDev F;
+    PmParams P;             // P.view_queue: this frame's counter, zeroed before the launch
+    StateDev prev, next;
+    int iter, phase;
+};
+// Grid of the batch kernel for `smem` bytes of dynamic shared memory per CTA.
+cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, int* n_ctas);
+// items: device array of n frames, all with or all without a blur channel.
+cudaError_t launch_sweep_batch(const SweepItem* items, int n, bool blur, bool shift, int smem, int n_ctas, int* err,
+                               cudaStream_t st);
 // FP32 FFMA throughput probe (diag.cu): best of three timed launches.
 cudaError_t measure_fma_rate(cudaStream_t st, float* ms, double* flops);
 

@@ -87,6 +87,10 @@ struct Plan {
     {
         Plan p;
         int o = 0;
+        // the staging barrier and the control words first: at the same offsets for
+        // every frame, so one barrier serves a launch over several frames
+        p.off_bar = o;   o += 16;
+        p.off_ctl = o;   o += 16;
         const int qb = (H + 1) * (W + 1) * 4;
         p.off_Q = o;     o += a16(K * qb);
         p.off_QB = o;    o += blur ? a16(K * qb) : 0;
@@ -98,8 +102,6 @@ struct Plan {
         p.off_ac = o;    o += 256 * 4;
         p.off_pc = o;    o += a16(W * H * 4);
         p.off_ps = o;    o += a16(W * H * 4);
-        p.off_bar = o;   o += 16;
-        p.off_ctl = o;   o += 16;
         p.off_stage = o; o += a16((1 + K) * tile_stride * (blur ? 2 : 1));
         p.tab_n = (ntap < W ? ntap : W) * (ntap < H ? ntap : H);
         p.maxh = sweep_maxh(K);
@@ -108,14 +110,16 @@ struct Plan {
         p.total = o;
         return p;
     }
-    __device__ WarpBlock warp_block(unsigned char* smem, float* gscratch, int w, int K) const
+    // stride: floats of global scratch per warp; a launch over several frames uses
+    // the largest frame's, so CTAs on different frames never share a region
+    __device__ WarpBlock warp_block(unsigned char* smem, float* gscratch, int w, int K, int stride) const
     {
         unsigned char* b = smem + off_warp + w * warp_bytes;
         WarpBlock S;
         S.tab = (float4*)b;                  b += a16(tab_n * 16);
         S.plane = (float4*)b;
         S.dp = S.plane + maxh;
-        float* g = gscratch + ((size_t)blockIdx.x * kWarps + w) * sweep_warp_words(K);
+        float* g = gscratch + ((size_t)blockIdx.x * kWarps + w) * (size_t)stride;
         S.cost = g;
         S.pair = (uint16_t*)(g + maxh * K);
         S.wres = g + maxh * K + (maxh * K + 1) / 2;
@@ -195,7 +199,7 @@ __device__ bool stage_view(unsigned char* smem, const Plan& L, const FrameDev& F
         mbar_arrive_expect_tx(bar, (uint32_t)(nt * ts * (BLUR ? 2 : 1)));
         for (int i = 0; i < nt; ++i) {
             const int v = (i == 0) ? vid : F.nb_ids[vid * K + i - 1];
-            const int vv = v < 0 ? vid : v;
+            const int vv = (v < 0 || v >= F.V) ? vid : v;
             bulk_copy_g2s(stage + i * ts, F.gray + (size_t)vv * ts, (uint32_t)ts, bar);
             if (BLUR) bulk_copy_g2s(stage + (nt + i) * ts, F.blur + (size_t)vv * ts, (uint32_t)ts, bar);
         }
@@ -204,7 +208,8 @@ __device__ bool stage_view(unsigned char* smem, const Plan& L, const FrameDev& F
     int* okk = (int*)(smem + L.off_ok);
     const float2 c0 = F.centers[vid];
     for (int k = threadIdx.x; k < K; k += blockDim.x) {
-        const int v = (k < nc) ? F.nb_ids[vid * K + k] : -1;
+        int v = (k < nc) ? F.nb_ids[vid * K + k] : -1;
+        if (v >= F.V) { atomicOr(err, PFD_DEVERR_SWEEP_CHECK); v = -1; }
         okk[k] = (v >= 0);
         geo[k] = make_geo(c0, F.centers[v >= 0 ? v : vid], P);
     }
@@ -559,15 +564,31 @@ __device__ __forceinline__ void refine_candidates(int x, int y, float4 best, flo
 
 }  // namespace
 
+// One half-sweep of one frame by this CTA: it takes the frame's micro-images
+// from P.view_queue until none is left.  parity: the staging barrier's phase,
+// carried across frames.  Returns false when a staging wait gave up.
 template <bool BLUR, bool COUNT, bool SHIFT>
-__global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, PmParams P, StateDev prev,
-                                                                     StateDev next, int iter, int phase, int* err)
+__device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev& F, const PmParams& P,
+                                            const StateDev& prev, const StateDev& next, int iter, int phase, int* err,
+                                            uint32_t& parity)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
     const int W = P.W, H = P.H, K = P.K;
     const Plan L = Plan::make(W, H, K, P.ntap, BLUR, P.tile_stride);
+    {
+        // the frame's shared-memory plan and its warps' scratch must fit what the
+        // launch has (checked once per frame; the decision is the same in every thread)
+        uint32_t dyn;
+        asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        const bool fits = L.total <= (int)dyn && P.view_queue != nullptr && P.cost_scratch != nullptr &&
+                          P.scratch_stride >= sweep_warp_words(K) &&
+                          (size_t)gridDim.x * kWarps * (size_t)P.scratch_stride <= P.scratch_floats;
+        if (!fits) {
+            if (threadIdx.x == 0) atomicOr(err, PFD_DEVERR_SWEEP_CHECK);
+            return false;
+        }
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const WarpBlock S = L.warp_block(smem, P.cost_scratch, warp, K);
+    const WarpBlock S = L.warp_block(smem, P.cost_scratch, warp, K, P.scratch_stride);
     float* pc = (float*)(smem + L.off_pc);
     uint32_t* ps = (uint32_t*)(smem + L.off_ps);
     int* ctl = (int*)(smem + L.off_ctl);
@@ -585,11 +606,9 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
             a_s[t] = __fdiv_rn(-sd, P.ss2);
         }
         for (int c = threadIdx.x; c < 256; c += blockDim.x) a_c[c] = __fdiv_rn((float)c, P.cc2);
-        if (threadIdx.x == 0) mbar_init((uint64_t*)(smem + L.off_bar), 1);
         __syncthreads();
     }
 
-    uint32_t parity = 0;
     // the CTAs take micro-images one at a time from a shared counter, so a CTA that
     // drew cheap ones takes more (their cost varies with the neighbour count and the
     // candidates); which CTA updates a micro-image does not change its result
@@ -614,7 +633,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
         }
         if (nc <= 0) { __syncthreads(); continue; }
         Quad T;
-        if (!stage_view<BLUR>(smem, L, F, P, vid, nc, parity, err, T)) return;
+        if (!stage_view<BLUR>(smem, L, F, P, vid, nc, parity, err, T)) return false;
         parity ^= 1u;
         if (threadIdx.x == 0) ctl[0] = 0;
         __syncthreads();
@@ -936,12 +955,49 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
         }
         __syncthreads();                         // shared memory is restaged for the next view
     }
+    return true;
+}
+
+// The staging barrier (offset 0 of every plan), once per launch.
+__device__ __forceinline__ void init_barrier(unsigned char* smem)
+{
+    if (threadIdx.x == 0) mbar_init((uint64_t*)smem, 1);
+    __syncthreads();
+}
+
+template <bool BLUR, bool COUNT, bool SHIFT>
+__global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, PmParams P, StateDev prev,
+                                                                     StateDev next, int iter, int phase, int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    init_barrier(smem);
+    uint32_t parity = 0;
+    sweep_frame<BLUR, COUNT, SHIFT>(smem, F, P, prev, next, iter, phase, err, parity);
+}
+
+// Several frames' half-sweeps in one launch, in list order: a CTA that finds a
+// frame's queue empty moves on to the next frame at once, so one frame's tail
+// overlaps the next one's start.  The dynamic shared memory is the largest of
+// the frames' plans.
+template <bool BLUR, bool SHIFT>
+__global__ void __launch_bounds__(kThreads, 3) pm_sweep_batch_kernel(const SweepItem* items, int n, int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    init_barrier(smem);
+    uint32_t parity = 0;
+    for (int b = 0; b < n; ++b) {
+        const SweepItem it = items[b];
+        if (!sweep_frame<BLUR, false, SHIFT>(smem, it.F, it.P, it.prev, it.next, it.iter, it.phase, err, parity))
+            return;
+    }
 }
 
 int sweep_warp_smem_bytes(const PmParams& P, bool blur)
 {
     return Plan::make(P.W, P.H, P.K, P.ntap, blur, P.tile_stride).total;
 }
+
+int sweep_warp_stride(int K) { return sweep_warp_words(K); }
 
 size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas)
 {
@@ -996,6 +1052,37 @@ cudaError_t launch_sweep_warp(const FrameDev& F, const PmParams& P, const StateD
                     : launch_k(pm_sweep_warp_kernel<false, false, true>, grid, kThreads, smem, st, args);
     return blur ? launch_k(pm_sweep_warp_kernel<true, false, false>, grid, kThreads, smem, st, args)
                 : launch_k(pm_sweep_warp_kernel<false, false, false>, grid, kThreads, smem, st, args);
+}
+
+static const void* batch_kernel(bool blur, bool shift)
+{
+    if (blur) return shift ? (const void*)pm_sweep_batch_kernel<true, true> : (const void*)pm_sweep_batch_kernel<true, false>;
+    return shift ? (const void*)pm_sweep_batch_kernel<false, true> : (const void*)pm_sweep_batch_kernel<false, false>;
+}
+
+cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, int* n_ctas)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void* k = batch_kernel(blur, shift);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    *n_ctas = sms * per_sm;
+    return cudaSuccess;
+}
+
+cudaError_t launch_sweep_batch(const SweepItem* items, int n, bool blur, bool shift, int smem, int n_ctas, int* err,
+                               cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+    const SweepItem* it = items; int nn = n; int* e = err;
+    void* args[] = { &it, &nn, &e };
+    return launch_k(batch_kernel(blur, shift), dim3(std::max(1, n_ctas)), kThreads, smem, st, args);
 }
 
 }  // namespace pfd
