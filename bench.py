@@ -480,7 +480,7 @@ def mixed_requests(pfd, n_req, seed):
     return out
 
 
-def batching_leg(pfd, n_frames=16, seed=7, reps=2):
+def batching_leg(pfd, n_frames=16, seed=7, reps=1):
     """The batching form on resident frames of the mixed distribution: every
     frame's PatchMatch one after another (pfd_patchmatch per frame, the plain
     method) against pfd_patchmatch_batch (one persistent launch per
