@@ -130,6 +130,25 @@ pfd_status pfd_frame_set_micro_images(pfd_ctx* ctx, int frame_id, const uint8_t*
  * device.  Needs a raw frame (pfd_frame_set_raw); the PatchMatch state must be
  * initialised again afterwards. */
 pfd_status pfd_frame_compute_blur(pfd_ctx* ctx, int frame_id, uint8_t* blur_out, uint32_t* blureness);
+/* The richness channel computed on the device from the frame's raw image:
+ * ImageQualityEstimate::QuantizeRichnessByGLCM (Util/ImageQualityEstimate.cpp:
+ * 310-340, calculate_matrix :659-682) then DepthSolver::SliceAndIndicatlizeForMI
+ * (DepthSolver.cpp:2709-2754).  The frame's map holds, at every pixel with
+ * 4 <= row < H - 4 and 4 <= col < W - 4, the contrast of the 3-bit GLCM of
+ * diagonal neighbours in the 8x8 window at (col - 4, row - 4), 0 elsewhere,
+ * normalised by cv::normalize(0, 255, NORM_MINMAX) over the frame.  Outputs,
+ * each [n_views] windows in frame order and each may be NULL:
+ *   score_out  [n_views][mi_h][mi_w] the normalised map's window
+ *              (DepthSolver::GetRichnessScoreMI, :2307-2326);
+ *   binary_out [n_views][mi_h][mi_w] 255 where it exceeds 10, else 0
+ *              (MLA_Problem::m_Image_Richness);
+ *   richness   [n_views] the window's 255s (MLA_Problem::m_RichnessValue,
+ *              ComputeRichnessValue, MVStereo/LFDepthInfo.cpp:86-104).
+ * The matcher does not read the channel (SelectNeighbors weighs richness by 0),
+ * so the frame keeps no copy and its PatchMatch state is untouched.  Waits for
+ * the device.  Needs a raw frame (pfd_frame_set_raw). */
+pfd_status pfd_frame_compute_richness(pfd_ctx* ctx, int frame_id, float* score_out, uint8_t* binary_out,
+                                      uint32_t* richness);
 /* pfd_frame_create + pfd_frame_set_raw. */
 pfd_status pfd_frame_upload(pfd_ctx* ctx, int* frame_id, const uint8_t* raw, int W, int H, int raw_pitch,
                             const float* centers, const int* tilekeys, int n_views,

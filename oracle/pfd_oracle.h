@@ -19,6 +19,7 @@
 #ifndef PFD_ORACLE_H
 #define PFD_ORACLE_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -283,6 +284,17 @@ long long orc_count_taps(const orc_frame* f, const orc_params* p, const int* vid
 void orc_laplacian(const uint8_t* gray, int W, int H, int pitch, float* score);
 int orc_blur_tiles(const uint8_t* gray, int W, int H, int pitch, const int* origin, int V, int mi_w, int mi_h,
                    uint8_t* tiles, uint32_t* counts);
+
+/* Richness channel (oracle/blur.c).  orc_glcm_contrast: the GLCM contrast map
+ * of QuantizeRichnessByGLCM before normalisation, into score [H][W].
+ * orc_normalize_minmax: cv::normalize(NORM_MINMAX) of a float map in place.
+ * orc_richness_tiles: every view's window of the normalised map (score_tiles),
+ * of its threshold at 10 in 8 bits (binary) and the count of 255s (counts);
+ * each may be NULL.  Returns 0, or -1 for a window outside the frame. */
+void orc_glcm_contrast(const uint8_t* gray, int W, int H, int pitch, float* score);
+void orc_normalize_minmax(float* map, size_t n, double lo, double hi);
+int orc_richness_tiles(const uint8_t* gray, int W, int H, int pitch, const int* origin, int V, int mi_w, int mi_h,
+                       float* score_tiles, uint8_t* binary, uint32_t* counts);
 
 #ifdef __cplusplus
 }

@@ -135,6 +135,9 @@ def lib() -> ctypes.CDLL:
         L.orc_mla_centers.argtypes = [_P, _I, _I, _I, _F, _I, _I, _P, _P, _P, _P, _P, _P, _I, _P]
         L.orc_laplacian.argtypes = [_P, _I, _I, _I, _P]
         L.orc_blur_tiles.argtypes = [_P, _I, _I, _I, _P, _I, _I, _I, _P, _P]
+        L.orc_glcm_contrast.argtypes = [_P, _I, _I, _I, _P]
+        L.orc_normalize_minmax.argtypes = [_P, ctypes.c_size_t, ctypes.c_double, ctypes.c_double]
+        L.orc_richness_tiles.argtypes = [_P, _I, _I, _I, _P, _I, _I, _I, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -444,6 +447,36 @@ def blur_tiles(gray, origins, mi_w: int, mi_h: int):
                               _p(counts))
     assert rc == 0, "window outside the frame"
     return tiles, counts
+
+
+def glcm_contrast(gray) -> np.ndarray:
+    """GLCM contrast map of QuantizeRichnessByGLCM before normalisation (oracle/blur.c)."""
+    g = np.ascontiguousarray(gray, np.uint8)
+    out = np.zeros(g.shape, np.float32)
+    lib().orc_glcm_contrast(_p(g), g.shape[1], g.shape[0], g.strides[0], _p(out))
+    return out
+
+
+def normalize_minmax(a, lo: float = 0.0, hi: float = 255.0) -> np.ndarray:
+    """cv::normalize(a, lo, hi, NORM_MINMAX) of a float map (oracle/blur.c)."""
+    out = np.ascontiguousarray(a, np.float32).copy()
+    lib().orc_normalize_minmax(_p(out), out.size, lo, hi)
+    return out
+
+
+def richness_tiles(gray, origins, mi_w: int, mi_h: int):
+    """Per-view normalised GLCM score [V][mi_h][mi_w] (f32), richness channel (u8,
+    0 or 255) and richness values [V] (oracle/blur.c)."""
+    g = np.ascontiguousarray(gray, np.uint8)
+    o = np.ascontiguousarray(origins, np.int32).reshape(-1, 2)
+    V = o.shape[0]
+    score = np.zeros((V, mi_h, mi_w), np.float32)
+    binary = np.zeros((V, mi_h, mi_w), np.uint8)
+    counts = np.zeros(V, np.uint32)
+    rc = lib().orc_richness_tiles(_p(g), g.shape[1], g.shape[0], g.strides[0], _p(o), V, mi_w, mi_h, _p(score),
+                                  _p(binary), _p(counts))
+    assert rc == 0, "window outside the frame"
+    return score, binary, counts
 
 
 def vd_to_rd_points(vd, c):

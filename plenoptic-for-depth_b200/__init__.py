@@ -193,6 +193,7 @@ def lib() -> ctypes.CDLL:
             "pfd_frame_set_raw_device": [_P, _I, _P, _I],
             "pfd_frame_set_micro_images": [_P, _I, _P],
             "pfd_frame_compute_blur": [_P, _I, _P, _P],
+            "pfd_frame_compute_richness": [_P, _I, _P, _P, _P],
             "pfd_set_ncc_moments": [_P, _I],
             "pfd_set_matcher": [_P, _I],
             "pfd_patchmatch_batch": [_P, _P, _I, _P, _P],
@@ -409,6 +410,19 @@ class Context:
         counts = np.zeros(f["V"], np.uint32)
         self._check(self._L.pfd_frame_compute_blur(self._h, fid, _ptr(tiles), _ptr(counts)), "pfd_frame_compute_blur")
         return tiles, counts
+
+    def frame_compute_richness(self, fid: int):
+        """The richness channel from the frame's raw image, on the device
+        (pfd_frame_compute_richness).  Returns (score [V][mi_h][mi_w] f32, the
+        normalised GLCM contrast; binary [V][mi_h][mi_w] u8, 0 or 255; richness
+        [V] u32, the 255s of each window)."""
+        f = self._frames[fid]
+        score = np.zeros((f["V"], f["mi_h"], f["mi_w"]), np.float32)
+        binary = np.zeros((f["V"], f["mi_h"], f["mi_w"]), np.uint8)
+        counts = np.zeros(f["V"], np.uint32)
+        self._check(self._L.pfd_frame_compute_richness(self._h, fid, _ptr(score), _ptr(binary), _ptr(counts)),
+                    "pfd_frame_compute_richness")
+        return score, binary, counts
 
     def state_upload(self, fid: int, plane, cost, disp, sel) -> None:
         f = self._frames[fid]

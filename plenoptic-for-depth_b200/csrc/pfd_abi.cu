@@ -591,6 +591,55 @@ pfd_status pfd_frame_compute_blur(pfd_ctx* ctx, int frame_id, uint8_t* blur_out,
     return PFD_OK;
 }
 
+pfd_status pfd_frame_compute_richness(pfd_ctx* ctx, int frame_id, float* score_out, uint8_t* binary_out,
+                                      uint32_t* richness)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!f->has_raw) return fail(ctx, PFD_EINVAL, "compute_richness: frame %d has no raw image", frame_id);
+    if ((f->H + 15) / 16 > 65535) return fail(ctx, PFD_EINVAL, "compute_richness: frame height %d above 1048560", f->H);
+    DeviceGuard g(ctx->device);
+    const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
+    // one allocation: the 16-bit contrast map, the maximum, then the outputs asked for
+    const size_t map_bytes = ((size_t)f->W * f->H * sizeof(uint16_t) + 255) & ~(size_t)255;
+    const size_t score_bytes = score_out ? ((px * sizeof(float) + 255) & ~(size_t)255) : 0;
+    const size_t binary_bytes = binary_out ? ((px + 255) & ~(size_t)255) : 0;
+    const size_t count_bytes = richness ? sizeof(uint32_t) * f->V : 0;
+    uint8_t* buf = nullptr;
+    CU(cudaMallocAsync((void**)&buf, map_bytes + 256 + score_bytes + binary_bytes + count_bytes, ctx->stream));
+    uint16_t* d_map = (uint16_t*)buf;
+    unsigned* d_max = (unsigned*)(buf + map_bytes);
+    float* d_score = score_out ? (float*)(buf + map_bytes + 256) : nullptr;
+    uint8_t* d_binary = binary_out ? buf + map_bytes + 256 + score_bytes : nullptr;
+    uint32_t* d_counts = richness ? (uint32_t*)(buf + map_bytes + 256 + score_bytes + binary_bytes) : nullptr;
+    pfd_status st = PFD_OK;
+    const cudaError_t e = pfd::launch_richness(f->d_raw, f->W, f->W, f->H, f->d_origin, f->V, f->mi_w, f->mi_h, d_map,
+                                               d_max, d_score, d_binary, d_counts, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(buf, ctx->stream);
+        cudaGetLastError();
+        return fail(ctx, PFD_ECUDA, "launch_richness: %s", cudaGetErrorString(e));
+    }
+    ctx->launches += f->V > 0 ? 2 : 1;
+    if (score_out && cudaMemcpyAsync(score_out, d_score, px * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream) !=
+                         cudaSuccess)
+        st = PFD_ECUDA;
+    if (st == PFD_OK && binary_out &&
+        cudaMemcpyAsync(binary_out, d_binary, px, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
+        st = PFD_ECUDA;
+    if (st == PFD_OK && richness &&
+        cudaMemcpyAsync(richness, d_counts, count_bytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
+        st = PFD_ECUDA;
+    cudaFreeAsync(buf, ctx->stream);
+    if (st == PFD_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) st = PFD_ECUDA;
+    if (st != PFD_OK) {
+        cudaGetLastError();
+        return fail(ctx, st, "compute_richness: copy-back failed");
+    }
+    return PFD_OK;
+}
+
 pfd_status pfd_state_upload(pfd_ctx* ctx, int frame_id, const float* plane, const float* cost, const float* disp,
                             const uint32_t* sel)
 {
