@@ -139,16 +139,32 @@ __device__ __forceinline__ uint32_t lds_u32(uint32_t addr)
 }
 
 // Linear-filter fetch of the measured texture unit (see Tiles in pm_device.cuh)
-// from a quad entry: 256 s = 256 T00 + a (T10 - T00) + b (T01 - T00) + w11 (T11 - T01 - T10 + T00).
-__device__ __forceinline__ float quad_blend(int tbx, int tby, uint32_t q)
+// from a quad entry: 256 s = 256 T00 + a (T10 - T00) + b (T01 - T00) + w11 (T11 - T01 - T10 + T00)
+// with w11 = (a b + 128) >> 8, regrouped per texel as
+// 256 s = T00 w00 + T10 w10 + T01 w01 + T11 w11, w10 = a - w11, w01 = b - w11,
+// w00 = 256 - w10 - b: all four weights lie in [0, 256], so two 16-bit pairs of
+// weights against the quad's four bytes make the sum with two dp2a, exactly.
+struct QuadWeights {
+    uint32_t lo;             // w00 | w10 << 16, against T00, T10 (the quad's low bytes)
+    uint32_t hi;             // w01 | w11 << 16, against T01, T11
+};
+
+__device__ __forceinline__ QuadWeights quad_weights(int tbx, int tby)
 {
     const int a = tbx & 0xFF, b = tby & 0xFF;
     const int w11 = (a * b + 128) >> 8;
-    const int t00 = (int)(q & 0xFFu), t10 = (int)((q >> 8) & 0xFFu);
-    const int t01 = (int)((q >> 16) & 0xFFu), t11 = (int)(q >> 24);
-    const int d1 = t10 - t00;
-    const int s256 = (t00 << 8) + a * d1 + b * (t01 - t00) + w11 * (t11 - t01 - d1);
-    return __fsub_rn(__int_as_float(s256 | 0x47000000), 32768.0f);
+    const int w10 = a - w11, w01 = b - w11;
+    const int w00 = 256 - w10 - b;
+    QuadWeights q;
+    q.lo = (uint32_t)w00 | ((uint32_t)w10 << 16);
+    q.hi = (uint32_t)w01 | ((uint32_t)w11 << 16);
+    return q;
+}
+
+__device__ __forceinline__ float quad_blend(const QuadWeights& w, uint32_t q)
+{
+    const uint32_t s256 = __dp2a_lo(w.lo, q, __dp2a_hi(w.hi, q, 0u));
+    return __fsub_rn(__uint_as_float(s256 | 0x47000000u), 32768.0f);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
@@ -326,7 +342,8 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
             if (v) {                         // a skipped tap leaves the sums as they are
                 const int tbx = tex_coord_bits(sx), tby = tex_coord_bits(sy);
                 const uint32_t rel = (((uint32_t)(tby >> 8) * qs + (uint32_t)(tbx >> 8)) << 2);
-                float s = quad_blend(tbx, tby, lds_u32(base + rel));
+                const QuadWeights qw = quad_weights(tbx, tby);
+                float s = quad_blend(qw, lds_u32(base + rel));
                 if (SHIFT) s = __fsub_rn(s, sh);
                 const float wv = e.x, wrv = e.y, rv = e.z;
                 const float ws = __fmul_rn(wv, s);
@@ -337,7 +354,7 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
                 srs = __fmaf_rn(wrv, s, srs);
                 sw = __fadd_rn(sw, wv);
                 if (BLUR) {
-                    const float sb = quad_blend(tbx, tby, lds_u32(bbase + rel));
+                    const float sb = quad_blend(qw, lds_u32(bbase + rel));
                     bsx = __fadd_rn(bsx, e.w);
                     bsy = __fadd_rn(bsy, __fdiv_rn(sb, 255.0f));
                 }
