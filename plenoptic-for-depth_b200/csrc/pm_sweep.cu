@@ -149,15 +149,16 @@ struct QuadWeights {
     uint32_t hi;             // w01 | w11 << 16, against T01, T11
 };
 
+// hi = w01 + 65536 w11 = b + 65535 w11, and lo + hi = 256 + 65535 a (w00 + w01 =
+// 256 - a, w10 + w11 = a), so lo = 256 + 65535 a - hi: no weight is negative, so
+// no half borrows from the other.
 __device__ __forceinline__ QuadWeights quad_weights(int tbx, int tby)
 {
-    const int a = tbx & 0xFF, b = tby & 0xFF;
-    const int w11 = (a * b + 128) >> 8;
-    const int w10 = a - w11, w01 = b - w11;
-    const int w00 = 256 - w10 - b;
+    const uint32_t a = (uint32_t)tbx & 0xFFu, b = (uint32_t)tby & 0xFFu;
+    const uint32_t w11 = (a * b + 128u) >> 8;
     QuadWeights q;
-    q.lo = (uint32_t)w00 | ((uint32_t)w10 << 16);
-    q.hi = (uint32_t)w01 | ((uint32_t)w11 << 16);
+    q.hi = w11 * 65535u + b;
+    q.lo = a * 65535u + 256u - q.hi;
     return q;
 }
 
