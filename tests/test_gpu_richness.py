@@ -83,3 +83,37 @@ def test_richness_full_sensor_bitexact(pfd, oracle, ctx):
     assert np.array_equal(binary == 255, score > 10) and set(np.unique(binary)) <= {0, 255}
     assert np.array_equal(counts, (binary == 255).reshape(len(counts), -1).sum(1))
     assert score.min() >= 0 and score.max() <= 255
+
+
+def test_compute_richness_needs_a_raw_frame(pfd, ctx):
+    w = pfd.make_workload(200, 160, 23.0, 4, seed=2, max_nb=4)
+    V = w.centers.shape[0]
+    fid = ctx.frame_create(w.frame.raw.shape[1], w.frame.raw.shape[0], w.centers, w.tilekeys, w.mi, w.mi, w.nb_ids,
+                           w.nb_counts)
+    ctx.frame_set_micro_images(fid, w.gray.reshape(V, w.mi, w.mi))
+    with pytest.raises(pfd.PfdError):
+        ctx.frame_compute_richness(fid)
+    ctx.frame_free(fid)
+    with pytest.raises(KeyError):
+        ctx.frame_compute_richness(fid)          # the binding knows the frame is gone
+    assert ctx._L.pfd_frame_compute_richness(ctx._h, fid, None, None, None) != 0
+
+
+def test_richness_leaves_the_patchmatch_state_alone(pfd, ctx):
+    """The channel is not an input of the matcher: a run after it equals a run
+    without it, bit for bit."""
+    w = pfd.make_workload(260, 200, 23.0, 4, seed=31, max_nb=6)
+    P = pfd.PmParams(base=23.0, patch_size=11, max_iterations=1)
+    out = []
+    for rich in (False, True):
+        fid = ctx.frame_upload(w.frame.raw, w.centers, w.tilekeys, w.mi, w.mi, w.nb_ids, w.nb_counts)
+        ctx.pm_init(fid, P, 9)
+        if rich:
+            ctx.frame_compute_richness(fid)
+        for ph in range(2):
+            ctx.pm_sweep(fid, P, 9, 0, ph)
+        out.append(ctx.download(fid))
+        ctx.frame_free(fid)
+    for a, b in zip(*out):
+        a, b = np.asarray(a), np.asarray(b)
+        assert a.tobytes() == b.tobytes()
