@@ -102,11 +102,15 @@ struct Plan {
         p.off_ac = o;    o += 256 * 4;
         p.off_pc = o;    o += a16(W * H * 4);
         p.off_ps = o;    o += a16(W * H * 4);
-        p.off_stage = o; o += a16((1 + K) * tile_stride * (blur ? 2 : 1));
         p.tab_n = (ntap < W ? ntap : W) * (ntap < H ? ntap : H);
         p.maxh = sweep_maxh(K);
         p.warp_bytes = a16(p.tab_n * 16) + a16(2 * p.maxh * 16);
-        p.off_warp = o;  o += kWarps * p.warp_bytes;
+        // the staging buffer shares the warps' area: it is filled (by bulk copies)
+        // and read only between views, while no warp holds a pixel
+        p.off_warp = o;
+        p.off_stage = o;
+        const int stage_bytes = a16((1 + K) * tile_stride * (blur ? 2 : 1));
+        o += (kWarps * p.warp_bytes > stage_bytes) ? kWarps * p.warp_bytes : stage_bytes;
         p.total = o;
         return p;
     }
@@ -213,6 +217,9 @@ __device__ bool stage_view(unsigned char* smem, const Plan& L, const FrameDev& F
     uint64_t* bar = (uint64_t*)(smem + L.off_bar);
     const int nt = 1 + nc;
     if (threadIdx.x == 0) {
+        // the warps' writes to the shared area before the last barrier, ordered
+        // before the bulk copies that overwrite it
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_arrive_expect_tx(bar, (uint32_t)(nt * ts * (BLUR ? 2 : 1)));
         for (int i = 0; i < nt; ++i) {
             const int v = (i == 0) ? vid : F.nb_ids[vid * K + i - 1];
@@ -984,7 +991,7 @@ __device__ __forceinline__ void init_barrier(unsigned char* smem)
 }
 
 template <bool BLUR, bool COUNT, bool SHIFT>
-__global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, PmParams P, StateDev prev,
+__global__ void __launch_bounds__(kThreads, 4) pm_sweep_warp_kernel(FrameDev F, PmParams P, StateDev prev,
                                                                      StateDev next, int iter, int phase, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -998,7 +1005,7 @@ __global__ void __launch_bounds__(kThreads, 3) pm_sweep_warp_kernel(FrameDev F, 
 // overlaps the next one's start.  The dynamic shared memory is the largest of
 // the frames' plans.
 template <bool BLUR, bool SHIFT>
-__global__ void __launch_bounds__(kThreads, 3) pm_sweep_batch_kernel(const SweepItem* items, int n, int* err)
+__global__ void __launch_bounds__(kThreads, 4) pm_sweep_batch_kernel(const SweepItem* items, int n, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     init_barrier(smem);
