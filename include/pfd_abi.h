@@ -188,9 +188,9 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
  * library's device image (held by every GPU that loads the library, until
  * exit) instead of a cudaMalloc'd buffer; inputs and outputs are the frame's
  * state exactly as for pfd_pm_sweep, and the results are the same bit for bit.
- * Limit: the array must hold one CTA's scratch (eight warps, each the cost
- * vectors of one pixel) for every SM, so max_nb <= 30 on a 148-SM B200;
- * larger frames get PFD_EINVAL.
+ * Limit: the array must hold one CTA's scratch (seven warps, each the cost
+ * vectors of one pixel) for every SM: every max_nb up to 32 fits on a 148-SM
+ * B200; a device with more SMs than the array holds CTAs gets PFD_EINVAL.
  * The first call on a device looks up the array's device address, so make
  * that call before any stream capture.  All calls on a device share the one
  * array (nothing in it has to start at zero): calls whose kernels overlap on

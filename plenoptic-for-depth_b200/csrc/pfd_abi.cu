@@ -1960,10 +1960,11 @@ pfd_status pfd_download(pfd_ctx* ctx, int frame_id, float* plane, float* cost, f
 
 // 8 MiB, held by every GPU that loads the library until the process exits.
 // Each warp of the sweep keeps the cost vectors of its current pixel here,
-// (1.5 h max_nb + 3 h) words rounded up to 32 with h = max_nb + 6, eight warps
-// per CTA; the array must hold at least one CTA per SM, so max_nb <= 30 on a
-// 148-SM B200.  Nothing in it needs to start at zero: a sweep writes every
-// entry it reads, earlier for the same pixel.
+// (1.5 h max_nb + 3 h) words rounded up to 32 with h = max_nb + 6, seven warps
+// per CTA; the array must hold at least one CTA per SM, which it does for every
+// max_nb up to 32 on a 148-SM B200 (54.7 KB per CTA at 32 neighbours).  Nothing
+// in it needs to start at zero: a sweep writes every entry it reads, earlier
+// for the same pixel.
 static __device__ __align__(256) float g_noalloc_scratch[(size_t(8) << 20) / sizeof(float)];
 
 namespace {

@@ -36,7 +36,7 @@ namespace pfd {
 
 namespace {
 
-constexpr int kWarps = 8;
+constexpr int kWarps = 7;
 constexpr int kThreads = 32 * kWarps;
 
 struct Quad {
