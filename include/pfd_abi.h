@@ -79,7 +79,8 @@ const char* pfd_last_error(pfd_ctx* ctx);
 void* pfd_stream(pfd_ctx* ctx);
 /* Waits for the context's stream; reports any device-side error flag. */
 pfd_status pfd_sync(pfd_ctx* ctx);
-/* Device memory currently held by the context's frames. */
+/* Device memory currently held by the context: its frames and the sweep's
+ * cudaMalloc'd cost-vector scratch. */
 size_t pfd_bytes_in_use(pfd_ctx* ctx);
 
 /* ---- frames ---------------------------------------------------------------
@@ -191,8 +192,10 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
  * Limit: the array must hold one CTA's scratch (seven warps, each the cost
  * vectors of one pixel) for every SM: every max_nb up to 32 fits on a 148-SM
  * B200; a device with more SMs than the array holds CTAs gets PFD_EINVAL.
- * The first call on a device looks up the array's device address, so make
- * that call before any stream capture.  All calls on a device share the one
+ * Every call looks up the array's device address (cudaGetSymbolAddress, a
+ * host-side lookup), so the address stays right after a cudaDeviceReset; the
+ * first call on a device may also load the library's device code there, so
+ * make that call before any stream capture.  All calls on a device share the one
  * array (nothing in it has to start at zero): calls whose kernels overlap on
  * the GPU, from other streams or other contexts, race and corrupt each other. */
 pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed,
@@ -201,8 +204,9 @@ pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd_pm_params*
 /* How the NCC moments are accumulated by the context's later pfd_pm_init,
  * pfd_pm_sweep(_noalloc), pfd_patchmatch and pfd_ncc_costs calls.
  * PFD_NCC_REFERENCE (the default): the reference's FP32 sums of w r, w r^2,
- * w s, w s^2 and w r s (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:110-174),
- * bit for bit; their variances E[r^2] - E[r]^2 lose digits to cancellation on
+ * w s, w s^2 and w r s (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:110-174)
+ * in the oracle's IEEE canonical arithmetic, bit for bit with the oracle (the
+ * reference's fast-math build differs in the last bits); their variances E[r^2] - E[r]^2 lose digits to cancellation on
  * patches of low contrast.  PFD_NCC_SHIFTED: the same FP32 sums of the texels
  * and samples minus the patch's centre texel (exact subtractions: both are
  * multiples of 1/256 below 2^16); the NCC is unchanged in exact arithmetic
@@ -387,6 +391,16 @@ pfd_status pfd_refocus(pfd_ctx* ctx, int frame_id, const float* slice_vd, int n_
 pfd_status pfd_select_neighbors(pfd_ctx* ctx, const float* centers, const int* tilekeys, int n_views, int mla_u_size,
                                 int mla_v_size, float pitch, const uint8_t* images, int mi_w, int mi_h, int max_nb,
                                 int* nb_ids, int* nb_counts);
+/* The same selection for a frame's own micro-images (the gray tiles cut on
+ * the device from its raw image, or uploaded), which then becomes the frame's
+ * matching lists: the first max_nb (the frame's) of each view's
+ * m_NeighsSortVecForMatch, as AdaptMIPMFrame::BuildViewIndexMap keeps the
+ * first entries of that list (AdaptMIPMFrame.cpp:207-218).  The frame's
+ * PatchMatch state belongs to its old lists and must be initialised again.
+ * nb_ids [n_views][max_list] and nb_counts [n_views] (both NULL, or both
+ * given with max_list <= 128) receive the full lists.  Waits for the device. */
+pfd_status pfd_frame_select_neighbors(pfd_ctx* ctx, int frame_id, int mla_u_size, int mla_v_size, float pitch,
+                                      int max_list, int* nb_ids, int* nb_counts);
 
 /* ---- micro-lens centres -------------------------------------------------
  * DepthSolver::ComputeMLACentersFromWhiteImage (DepthSolver.cpp:710-870) on the

@@ -235,6 +235,7 @@ def lib() -> ctypes.CDLL:
             "pfd_server_last_error": [_P],
             "pfd_frame_bytes": [_I, _I, _I, _I, _I, _I, _I],
             "pfd_select_neighbors": [_P, _P, _P, _I, _I, _I, _F, _P, _I, _I, _I, _P, _P],
+            "pfd_frame_select_neighbors": [_P, _I, _I, _I, _F, _I, _P, _P],
             "pfd_mla_centers": [_P, _P, _I, _I, _I, _F, _I, _I, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
             "pfd_fuse_virtual_depth": [_P, _I, ctypes.POINTER(FuseParamsC), _P, _P, _I, _P, _P, _P, _P, _P, _P,
                                        ctypes.POINTER(ctypes.c_longlong)],
@@ -633,6 +634,23 @@ class Context:
                     "pfd_select_neighbors")
         return ids, cnt
 
+    def frame_select_neighbors(self, fid: int, mla_u_size: int, mla_v_size: int, pitch: float,
+                               max_list: int | None = None):
+        """The selection on the frame's own micro-images; the first max_nb of
+        each list become the frame's matching lists (the PatchMatch state must
+        be initialised again).  With max_list, returns the full lists
+        (nb_ids [V][max_list], nb_counts [V]); otherwise None."""
+        f = self._frames[fid]
+        if max_list is None:
+            self._check(self._L.pfd_frame_select_neighbors(self._h, fid, mla_u_size, mla_v_size, float(pitch), 0,
+                                                           None, None), "pfd_frame_select_neighbors")
+            return None
+        ids = np.full((f["V"], max_list), -1, np.int32)
+        cnt = np.zeros(f["V"], np.int32)
+        self._check(self._L.pfd_frame_select_neighbors(self._h, fid, mla_u_size, mla_v_size, float(pitch), max_list,
+                                                       _ptr(ids), _ptr(cnt)), "pfd_frame_select_neighbors")
+        return ids, cnt
+
     def mla_centers(self, white, baseline: float, mla_u_size: int, mla_v_size: int):
         """DepthSolver::ComputeMLACentersFromWhiteImage on a white image (H x W x 3
         BGR, or H x W gray).  Returns (dict of col, row, cx, cy, area, abandon
@@ -791,6 +809,7 @@ def synth_lib() -> ctypes.CDLL:
         S.pfd_synth_count.argtypes = [ctypes.POINTER(SynthConfigC), ctypes.POINTER(_I), ctypes.POINTER(_I),
                                       ctypes.POINTER(_I)]
         S.pfd_synth_render.argtypes = [ctypes.POINTER(SynthConfigC), _P, _P, _P, _P, _P]
+        S.pfd_synth_vd_map.argtypes = [ctypes.POINTER(SynthConfigC), _P]
         _synth = S
     return _synth
 
@@ -805,6 +824,7 @@ class SynthFrame:
     pitch: float
     n_cols: int
     n_rows: int
+    config: tuple = ()       # the generator's arguments, for synth_vd_map
 
 
 def synth_frame(width: int, height: int, pitch: float, n_planes: int, seed: int, vd_min: float = 2.0,
@@ -824,7 +844,50 @@ def synth_frame(width: int, height: int, pitch: float, n_planes: int, seed: int,
     vd = np.empty(n.value, np.float32)
     if S.pfd_synth_render(ctypes.byref(cfg), _ptr(raw), _ptr(cen), _ptr(keys), _ptr(types), _ptr(vd)) != 0:
         raise ValueError("synthetic rendering failed")
-    return SynthFrame(raw, cen, keys, types, vd, pitch, nc.value, nr.value)
+    return SynthFrame(raw, cen, keys, types, vd, pitch, nc.value, nr.value,
+                      (width, height, pitch, n_planes, vd_min, vd_max, noise_sigma, n_lens_types, tuple(blur_sigma),
+                       texture_cell, seed))
+
+
+def synth_vd_map(frame: SynthFrame) -> np.ndarray:
+    """Ground-truth virtual depth of every raw pixel of a synthetic frame
+    ([H][W] float32; 0 outside the lens circles): the depth of the scene point
+    the pixel shows."""
+    (width, height, pitch, n_planes, vd_min, vd_max, noise_sigma, n_lens_types, blur_sigma, texture_cell,
+     seed) = frame.config
+    cfg = SynthConfigC(width, height, pitch, n_planes, vd_min, vd_max, noise_sigma, n_lens_types,
+                       (_F * 3)(*blur_sigma), texture_cell, seed)
+    out = np.empty((height, width), np.float32)
+    if synth_lib().pfd_synth_vd_map(ctypes.byref(cfg), _ptr(out)) != 0:
+        raise ValueError("bad synthetic frame configuration")
+    return out
+
+
+def depth_error(w: "Workload", plane: np.ndarray, vd_map: np.ndarray | None = None, cost: np.ndarray | None = None):
+    """Matched virtual depth (pitch / disparity, disparity = plane.w) of every
+    micro-image pixel against the scene's true virtual depth at that raw pixel.
+    Pixels count as matched when the disparity is > 0.05 (and the cost < 2 when
+    given).  Returns the fraction matched and, over them, the median absolute
+    and relative error and the fractions within 0.05, 0.5 and 1 virtual-depth
+    units."""
+    if vd_map is None:
+        vd_map = synth_vd_map(w.frame)
+    mi = w.mi
+    o = window_origins(w.centers, mi).astype(np.int64)
+    ys, xs = np.mgrid[0:mi, 0:mi]
+    gt = vd_map[o[:, 1, None, None] + ys[None], o[:, 0, None, None] + xs[None]].reshape(-1)
+    d = plane[:, 3].astype(np.float64)
+    ok = (d > 0.05) & (gt > 0)
+    if cost is not None:
+        ok &= cost < 2.0
+    est = w.frame.pitch / np.maximum(d, 1e-6)
+    err = np.abs(est - gt)[ok]
+    rel = err / gt[ok]
+    if err.size == 0:
+        return {"matched": 0.0}
+    return {"matched": float(ok.mean()), "median_abs": float(np.median(err)), "median_rel": float(np.median(rel)),
+            "within_0.05": float(np.mean(err <= 0.05)), "within_0.5": float(np.mean(err <= 0.5)),
+            "within_1": float(np.mean(err <= 1.0))}
 
 
 def mi_window(pitch: float) -> int:

@@ -20,6 +20,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <functional>
+#include <thread>
 #include <vector>
 
 #include "../../include/pfd_abi.h"
@@ -96,22 +98,39 @@ struct Walk {
 
 }  // namespace
 
+void parallel_views(int n, const std::function<void(int, int)>& body)
+{
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = (int)std::min<unsigned>(std::min(hw, 32u), (unsigned)std::max(1, n / 256));
+    if (nt <= 1) { body(0, n); return; }
+    std::vector<std::thread> th;
+    th.reserve(nt);
+    for (int t = 0; t < nt; ++t) {
+        const int a = (int)((long long)n * t / nt), b = (int)((long long)n * (t + 1) / nt);
+        th.emplace_back(body, a, b);
+    }
+    for (auto& x : th) x.join();
+}
+
 void collect_rings(const LensGrid& G, float pitch, int n_rings, std::vector<std::vector<std::vector<int>>>& rings)
 {
     float delt = 0.15f;
     delt *= pitch;
-    std::vector<char> seen(G.V, 0);
-    std::vector<int> touched;
-    Walk W{ G, pitch, delt, seen, touched };
     rings.assign(G.V, {});
-    for (int v = 0; v < G.V; ++v) {
-        for (int t : touched) seen[t] = 0;
-        touched.clear();
-        seen[v] = 1;
-        touched.push_back(v);
-        rings[v].assign(n_rings, {});
-        for (int k = 0; k < n_rings; ++k) W.ring(k == 0 ? std::vector<int>{ v } : rings[v][k - 1], rings[v][k]);
-    }
+    // views are independent: each thread walks its own range with its own marks
+    parallel_views(G.V, [&](int a, int b) {
+        std::vector<char> seen(G.V, 0);
+        std::vector<int> touched;
+        Walk W{ G, pitch, delt, seen, touched };
+        for (int v = a; v < b; ++v) {
+            for (int t : touched) seen[t] = 0;
+            touched.clear();
+            seen[v] = 1;
+            touched.push_back(v);
+            rings[v].assign(n_rings, {});
+            for (int k = 0; k < n_rings; ++k) W.ring(k == 0 ? std::vector<int>{ v } : rings[v][k - 1], rings[v][k]);
+        }
+    });
 }
 
 }  // namespace pfd
@@ -133,12 +152,14 @@ extern "C" pfd_status pfd_neighbors_by_baseline(const float* centers, const int*
     if (!G.build(centers, tilekeys, n_views, u, v)) return PFD_EINVAL;
     std::vector<std::vector<std::vector<int>>> R;
     pfd::collect_rings(G, pitch, rings, R);
-    std::vector<int> list;
-    for (int i = 0; i < n_views; ++i) {
-        pfd::select_for_view(G, pitch, i, R[i], [](int, int) { return 0.0f; }, list);
-        const int n = std::min((int)list.size(), max_nb);
-        for (int k = 0; k < max_nb; ++k) nb_ids[(size_t)i * max_nb + k] = k < n ? list[k] : -1;
-        nb_counts[i] = n;
-    }
+    pfd::parallel_views(n_views, [&](int a, int b) {
+        std::vector<int> list;
+        for (int i = a; i < b; ++i) {
+            pfd::select_for_view(G, pitch, i, R[i], [](int, int) { return 0.0f; }, list);
+            const int n = std::min((int)list.size(), max_nb);
+            for (int k = 0; k < max_nb; ++k) nb_ids[(size_t)i * max_nb + k] = k < n ? list[k] : -1;
+            nb_counts[i] = n;
+        }
+    });
     return PFD_OK;
 }

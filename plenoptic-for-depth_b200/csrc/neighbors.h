@@ -1,6 +1,7 @@
 // neighbors.h -- matching-neighbour selection, host side (neighbors.cpp).
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 namespace pfd {
@@ -14,6 +15,10 @@ struct LensGrid {
     std::vector<int> id;                          // [row][col] -> view, -1
     bool build(const float* centers, const int* tilekeys, int n_views, int u_size, int v_size);
 };
+
+// body(a, b) over [0, n) split into contiguous ranges, one host thread each
+// (up to 32; one range for small n).
+void parallel_views(int n, const std::function<void(int, int)>& body);
 
 // The five rings of every view (ComputeNearestCircleKeys, SelectNeighbors.cpp:
 // 195-365): rings[v][k] in the reference's push order.

@@ -1043,10 +1043,12 @@ static pfd_status build_steps(pfd_ctx* ctx, Frame& f)
     for (size_t s = 0; s + 1 < counts.size(); ++s)
         if (counts[s + 1] > counts[s]) f.step_start.push_back(counts[s]);
     f.step_start.push_back(V);
-    void* p = nullptr;
-    pfd_status st = frame_alloc(ctx, f, &p, sizeof(int) * (size_t)V);
-    if (st != PFD_OK) { f.step_start.clear(); return st; }
-    f.d_steps = (int*)p;
+    if (!f.d_steps) {                 // kept when new neighbour lists rebuild the schedule
+        void* p = nullptr;
+        pfd_status st = frame_alloc(ctx, f, &p, sizeof(int) * (size_t)V);
+        if (st != PFD_OK) { f.step_start.clear(); return st; }
+        f.d_steps = (int*)p;
+    }
     CU(cudaMemcpyAsync(f.d_steps, order.data(), sizeof(int) * (size_t)V, cudaMemcpyHostToDevice, ctx->stream));
     return PFD_OK;
 }
@@ -1619,6 +1621,59 @@ pfd_status pfd_fuse_virtual_depth(pfd_ctx* ctx, int frame_id, const pfd_fuse_par
 
 // ---- matching-neighbour selection ---------------------------------------------
 
+// The selection given the micro-images on the device (tiles tile_stride bytes
+// apart) and the centres on the host and the device: every ring candidate's
+// similarity on the device, then the per-view ring walk, RANSAC, stop rule and
+// sort on the host threads.  out_ids [n][max_nb], out_counts [n].
+static pfd_status select_lists(pfd_ctx* ctx, const pfd::LensGrid& G, float pitch, const uint8_t* d_img,
+                               int tile_stride, int mi_w, int mi_h, const float2* d_c, int max_nb, int* out_ids,
+                               int* out_counts)
+{
+    const int n_views = G.V;
+    std::vector<std::vector<std::vector<int>>> R;
+    pfd::collect_rings(G, pitch, 5, R);
+    // every candidate of every ring: the search may stop early, the similarities are cheap
+    std::vector<int2> pairs;
+    std::vector<size_t> first((size_t)n_views * 5 + 1, 0);
+    for (int v = 0; v < n_views; ++v)
+        for (int k = 0; k < 5; ++k) {
+            first[(size_t)v * 5 + k] = pairs.size();
+            for (int n : R[v][k]) pairs.push_back(make_int2(v, n));
+        }
+    first[(size_t)n_views * 5] = pairs.size();
+    cudaStream_t s = ctx->stream;
+    std::vector<int> sims(pairs.size());
+    int2* d_pairs = nullptr;
+    int* d_out = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&d_pairs, sizeof(int2) * std::max<size_t>(pairs.size(), 1), s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_out, sizeof(int) * std::max<size_t>(pairs.size(), 1), s);
+    if (e == cudaSuccess && !pairs.empty())
+        e = cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = pfd::launch_similarity(d_img, tile_stride, mi_w, mi_h, d_c, d_pairs, (int)pairs.size(), d_out, s);
+    if (e == cudaSuccess && !pairs.empty())
+        e = cudaMemcpyAsync(sims.data(), d_out, sizeof(int) * pairs.size(), cudaMemcpyDeviceToHost, s);
+    for (void* q : { (void*)d_pairs, (void*)d_out })
+        if (q) cudaFreeAsync(q, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, PFD_ECUDA, "select_neighbors: %s", cudaGetErrorString(e));
+    }
+    ctx->launches += 1;
+    pfd::parallel_views(n_views, [&](int a, int b) {
+        std::vector<int> list;
+        for (int v = a; v < b; ++v) {
+            auto sim = [&](int ring, int i) { return (float)(double)sims[first[(size_t)v * 5 + ring] + i]; };
+            pfd::select_for_view(G, pitch, v, R[v], sim, list);
+            const int n = std::min((int)list.size(), max_nb);
+            for (int k = 0; k < max_nb; ++k) out_ids[(size_t)v * max_nb + k] = k < n ? list[k] : -1;
+            out_counts[v] = n;
+        }
+    });
+    return PFD_OK;
+}
+
 pfd_status pfd_select_neighbors(pfd_ctx* ctx, const float* centers, const int* tilekeys, int n_views, int mla_u_size,
                                 int mla_v_size, float pitch, const uint8_t* images, int mi_w, int mi_h, int max_nb,
                                 int* nb_ids, int* nb_counts)
@@ -1633,53 +1688,68 @@ pfd_status pfd_select_neighbors(pfd_ctx* ctx, const float* centers, const int* t
     pfd::LensGrid G;
     if (!G.build(centers, tilekeys, n_views, mla_u_size, mla_v_size))
         return fail(ctx, PFD_EINVAL, "select_neighbors: a tile key lies outside the grid or is repeated");
-    std::vector<std::vector<std::vector<int>>> R;
-    pfd::collect_rings(G, pitch, 5, R);
-    // every candidate of every ring: the search may stop early, the similarities are cheap
-    std::vector<int2> pairs;
-    std::vector<size_t> first((size_t)n_views * 5 + 1, 0);
-    for (int v = 0; v < n_views; ++v)
-        for (int k = 0; k < 5; ++k) {
-            first[(size_t)v * 5 + k] = pairs.size();
-            for (int n : R[v][k]) pairs.push_back(make_int2(v, n));
-        }
-    first[(size_t)n_views * 5] = pairs.size();
     DeviceGuard g(ctx->device);
     cudaStream_t s = ctx->stream;
     const size_t ppv = (size_t)mi_w * mi_h;
-    std::vector<int> sims(pairs.size());
     uint8_t* d_img = nullptr;
     float2* d_c = nullptr;
-    int2* d_pairs = nullptr;
-    int* d_out = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&d_img, ppv * n_views, s);
     if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_c, sizeof(float2) * n_views, s);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_pairs, sizeof(int2) * std::max<size_t>(pairs.size(), 1), s);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_out, sizeof(int) * std::max<size_t>(pairs.size(), 1), s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_img, images, ppv * n_views, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_c, centers, sizeof(float2) * n_views, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && !pairs.empty())
-        e = cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = pfd::launch_similarity(d_img, (int)ppv, mi_w, mi_h, d_c, d_pairs, (int)pairs.size(), d_out, s);
-    if (e == cudaSuccess && !pairs.empty())
-        e = cudaMemcpyAsync(sims.data(), d_out, sizeof(int) * pairs.size(), cudaMemcpyDeviceToHost, s);
-    for (void* q : { (void*)d_img, (void*)d_c, (void*)d_pairs, (void*)d_out })
-        if (q) cudaFreeAsync(q, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    pfd_status st = PFD_OK;
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return fail(ctx, PFD_ECUDA, "select_neighbors: %s", cudaGetErrorString(e));
+        st = fail(ctx, PFD_ECUDA, "select_neighbors: %s", cudaGetErrorString(e));
+    } else {
+        st = select_lists(ctx, G, pitch, d_img, (int)ppv, mi_w, mi_h, d_c, max_nb, nb_ids, nb_counts);
     }
-    ctx->launches += 1;
-    std::vector<int> list;
-    for (int v = 0; v < n_views; ++v) {
-        auto sim = [&](int ring, int i) { return (float)(double)sims[first[(size_t)v * 5 + ring] + i]; };
-        pfd::select_for_view(G, pitch, v, R[v], sim, list);
-        const int n = std::min((int)list.size(), max_nb);
-        for (int k = 0; k < max_nb; ++k) nb_ids[(size_t)v * max_nb + k] = k < n ? list[k] : -1;
-        nb_counts[v] = n;
+    for (void* q : { (void*)d_img, (void*)d_c })
+        if (q) cudaFreeAsync(q, s);
+    return st;
+}
+
+pfd_status pfd_frame_select_neighbors(pfd_ctx* ctx, int frame_id, int mla_u_size, int mla_v_size, float pitch,
+                                      int max_list, int* nb_ids, int* nb_counts)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!f->has_mi) return fail(ctx, PFD_ESTATE, "frame_select_neighbors: frame %d has no micro-images", frame_id);
+    if (!(pitch > 0.0f)) return fail(ctx, PFD_EINVAL, "frame_select_neighbors: pitch must be > 0");
+    if ((nb_ids != nullptr) != (nb_counts != nullptr) || (nb_ids && (max_list < 1 || max_list > 128)))
+        return fail(ctx, PFD_EINVAL, "frame_select_neighbors: give both lists (max_list 1-128) or neither");
+    if (mla_u_size < 1 || mla_v_size < 1 || (long long)mla_u_size * mla_v_size > (1LL << 28))
+        return fail(ctx, PFD_EINVAL, "frame_select_neighbors: bad lens grid %d x %d", mla_u_size, mla_v_size);
+    pfd::LensGrid G;
+    if (!G.build(f->h_centers.data(), f->h_keys.data(), f->V, mla_u_size, mla_v_size))
+        return fail(ctx, PFD_EINVAL, "frame_select_neighbors: a tile key lies outside the grid or is repeated");
+    DeviceGuard g(ctx->device);
+    const int L = std::max(f->K, nb_ids ? max_list : 0);
+    std::vector<int> ids((size_t)f->V * L), cnt(f->V);
+    pfd_status st = select_lists(ctx, G, pitch, f->d_gray, f->tile_stride, f->mi_w, f->mi_h, f->d_centers, L,
+                                 ids.data(), cnt.data());
+    if (st != PFD_OK) return st;
+    // the matcher's lists: the first K of each (AdaptMIPMFrame::BuildViewIndexMap keeps the first 16 views)
+    for (int v = 0; v < f->V; ++v) {
+        const int n = std::min(cnt[v], f->K);
+        for (int k = 0; k < f->K; ++k) f->h_nb_ids[(size_t)v * f->K + k] = k < n ? ids[(size_t)v * L + k] : -1;
+        f->h_nb_counts[v] = n;
+        if (nb_ids) {
+            const int m = std::min(cnt[v], max_list);
+            for (int k = 0; k < max_list; ++k) nb_ids[(size_t)v * max_list + k] = k < m ? ids[(size_t)v * L + k] : -1;
+            nb_counts[v] = m;
+        }
     }
+    CU(cudaMemcpyAsync(f->d_nb_ids, f->h_nb_ids.data(), sizeof(int) * f->h_nb_ids.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CU(cudaMemcpyAsync(f->d_nb_counts, f->h_nb_counts.data(), sizeof(int) * f->V, cudaMemcpyHostToDevice, ctx->stream));
+    // the host copies are the frame's own (they outlive the copies); the
+    // state, the stored cost vectors and the filter's schedule belong to the
+    // old lists
+    f->has_state = false;
+    f->cvec_valid = 0;
+    f->step_start.clear();
     return PFD_OK;
 }
 
@@ -1970,29 +2040,22 @@ static __device__ __align__(256) float g_noalloc_scratch[(size_t(8) << 20) / siz
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = sizeof(g_noalloc_scratch);
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-float* g_noalloc_addr[kNoAllocMaxDevices] = {};
 
-// Device address of g_noalloc_scratch on `dev`, which must be the current
-// device.  In host code the array's name stands for a host-side shadow, so the
-// kernel gets the address from cudaGetSymbolAddress, looked up once per device.
-pfd_status noalloc_scratch(pfd_ctx* ctx, int dev, float** out)
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// array's name stands for a host-side shadow, so the kernel gets the address
+// from cudaGetSymbolAddress.  It is looked up on every call (a host-side table
+// lookup once the module is loaded): a cached address would outlive a
+// cudaDeviceReset, after which the module is loaded again, possibly elsewhere.
+pfd_status noalloc_scratch(pfd_ctx* ctx, float** out)
 {
-    if (dev < 0 || dev >= kNoAllocMaxDevices)
-        return fail(ctx, PFD_EINVAL, "pfd_pm_sweep_noalloc: device %d outside [0, %d)", dev, kNoAllocMaxDevices);
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        float* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return fail(ctx, PFD_ECUDA, "pfd_pm_sweep_noalloc: cudaGetSymbolAddress of the scratch array: %s",
-                        cudaGetErrorString(e));
-        }
-        g_noalloc_addr[dev] = p;
+    float* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return fail(ctx, PFD_ECUDA, "pfd_pm_sweep_noalloc: cudaGetSymbolAddress of the scratch array: %s",
+                    cudaGetErrorString(e));
     }
-    *out = g_noalloc_addr[dev];
+    *out = p;
     return PFD_OK;
 }
 
@@ -2034,7 +2097,7 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     CU(pfd::sweep_warp_grid(P, f->has_blur, &n_ctas));
     n_ctas = (int)std::min<size_t>((size_t)n_ctas, fit);
     float* scratch = nullptr;
-    st = noalloc_scratch(ctx, ctx->device, &scratch);
+    st = noalloc_scratch(ctx, &scratch);
     if (st != PFD_OK) return st;
     P.cost_scratch = scratch;
     P.scratch_floats = kNoAllocScratchBytes / sizeof(float);

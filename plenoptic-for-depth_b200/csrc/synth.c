@@ -218,3 +218,56 @@ int pfd_synth_render(const pfd_synth_config* c, uint8_t* raw, float* centers, in
     free(P);
     return 0;
 }
+
+/* Ground truth of a frame: vd_map (width*height floats) receives, at every raw
+ * pixel inside a lens's circle, the virtual depth v of the scene point that
+ * pixel shows (the same fixed point X = c + (u - c) v(X) the rendering solves),
+ * and 0 elsewhere.  Lens circles of radius pitch/2 on the hexagonal grid touch
+ * but do not overlap, so each pixel has one lens.  Since a neighbour lens at
+ * baseline b sees that point shifted by b / v, the matched disparity of the
+ * pixel against a neighbour one pitch away is pitch / v. */
+int pfd_synth_vd_map(const pfd_synth_config* c, float* vd_map)
+{
+    int nc, nr;
+    double x0, y0, dy;
+    if (!c || !vd_map || c->n_planes < 1 || c->n_planes > 4096 || !(c->pitch > 2.0f)) return -1;
+    lens_grid(c, &nc, &nr, &x0, &y0, &dy);
+    const int W = c->width, H = c->height, L = nc * nr;
+    const double p = c->pitch, R = 0.5 * p;
+    const double vmin = c->vd_min, vmax = c->vd_max;
+    plane_t* P = (plane_t*)malloc(sizeof(plane_t) * (size_t)c->n_planes);
+    if (!P) return -2;
+    const double g = 3.0 / (double)(W > H ? W : H);
+    for (int i = 0; i < c->n_planes; ++i) {
+        P[i].sx = u01(c->seed, 1, i) * W;
+        P[i].sy = u01(c->seed, 2, i) * H;
+        P[i].a = (2.0 * u01(c->seed, 3, i) - 1.0) * g;
+        P[i].b = (2.0 * u01(c->seed, 4, i) - 1.0) * g;
+        P[i].c = vmin + 1.0 + u01(c->seed, 5, i) * (vmax - vmin - 2.0);
+    }
+    memset(vd_map, 0, sizeof(float) * (size_t)W * H);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int l = 0; l < L; ++l) {
+        const int row = l / nc, col = l % nc;
+        const double cx = x0 + col * p + ((row & 1) ? 0.5 * p : 0.0);
+        const double cy = y0 + row * dy;
+        const int half = (int)ceil(R) + 1;
+        const int ox = (int)floor(cx) - half, oy = (int)floor(cy) - half;
+        for (int j = 0; j <= 2 * half; ++j)
+            for (int i = 0; i <= 2 * half; ++i) {
+                const int ux = ox + i, uy = oy + j;
+                if (ux < 0 || uy < 0 || ux >= W || uy >= H) continue;
+                const double r = sqrt((ux - cx) * (ux - cx) + (uy - cy) * (uy - cy));
+                if (r >= R) continue;
+                double X = cx, Y = cy, v = 0.0;
+                for (int it = 0; it < 8; ++it) {
+                    v = depth_at(P, c->n_planes, vmin, vmax, X, Y);
+                    X = cx + (ux - cx) * v;
+                    Y = cy + (uy - cy) * v;
+                }
+                vd_map[(size_t)uy * W + ux] = (float)depth_at(P, c->n_planes, vmin, vmax, X, Y);
+            }
+    }
+    free(P);
+    return 0;
+}
