@@ -236,6 +236,28 @@ pfd_status pfd_set_ncc_moments(pfd_ctx* ctx, int mode);
 #define PFD_MATCHER_FRAME 0
 #define PFD_MATCHER_ACMM  1
 pfd_status pfd_set_matcher(pfd_ctx* ctx, int matcher);
+/* Launch shape of the context's later half-sweeps (pfd_pm_sweep, pfd_patchmatch,
+ * pfd_patchmatch_batch; no counterpart in the reference, whose sweep is one
+ * thread per pixel in 16x16 blocks).  A shape is a number of warps per CTA and
+ * the CTAs per SM its registers are sized for; every shape computes the same
+ * state bit for bit.  Shape 0 (7 warps, 4 CTAs) is the default.
+ * PFD_SHAPE_AUTOTUNE: the engine's autotuner picks the shape per key (window,
+ * neighbour count, patch size and tap stride, blur channel, moment mode,
+ * matcher) and device: the first half-sweep of a new key runs once in every
+ * shape that fits the key's shared-memory plan, timed on the context's stream
+ * (the stored cost vectors are neither read nor written by these trials, so
+ * each writes the half-sweep's result), and the fastest is kept for the rest
+ * of the process.  pfd_patchmatch_batch uses the shape of each launch's
+ * largest frame.  Tap counting and pfd_pm_sweep_noalloc always run shape 0. */
+#define PFD_SWEEP_SHAPES 4
+#define PFD_SHAPE_AUTOTUNE -1
+pfd_status pfd_set_sweep_shape(pfd_ctx* ctx, int shape);
+/* Warps per CTA and CTAs per SM of shape 0 .. PFD_SWEEP_SHAPES - 1. */
+pfd_status pfd_sweep_shape_info(int shape, int* warps_per_cta, int* ctas_per_sm);
+/* The shape the autotuner chose for the key of (frame, params), or -1 when the
+ * key has not been tuned in this process. */
+pfd_status pfd_tuned_sweep_shape(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, int* shape);
+
 /* PostRefineMetadataFrame (AdaptMIPMFrameACMM.cu:903-929): every pixel keeps
  * its plane and gets the cost, selected views and disp of it as the ACMM
  * write-back computes them, under the context's matcher and moment mode. */
@@ -510,12 +532,8 @@ pfd_status pfd_fit_behavioral_model(pfd_ctx* ctx, const float* real_depth, const
 pfd_status pfd_set_tap_counting(pfd_ctx* ctx, int enable);
 /* Reads and clears the tap counter (synchronises the stream). */
 pfd_status pfd_read_tap_count(pfd_ctx* ctx, unsigned long long* taps);
-/* Number of kernels this context has launched so far (every engine kernel,
- * the FP32 probe included). */
+/* Number of kernels this context has launched so far (every engine kernel). */
 pfd_status pfd_launch_count(pfd_ctx* ctx, unsigned long long* n);
-/* Measured FP32 fused multiply-add throughput of the device, TFLOP/s
- * (independent FFMA chains on every SM; best of three launches). */
-pfd_status pfd_fp32_fma_rate(pfd_ctx* ctx, double* tflops);
 
 #ifdef __cplusplus
 }

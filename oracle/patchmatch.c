@@ -753,17 +753,18 @@ int orc_pm_sweep_views(const orc_frame* f, const orc_params* p, uint64_t seed, i
     return 0;
 }
 
-long long orc_pm_sweep_taps(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
-                            const orc_state* prev, orc_state* next, int nthreads)
+long long orc_pm_sweep_views_taps(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
+                                  const orc_state* prev, orc_state* next, int v0, int v1, int nthreads)
 {
     if (!f || !p || f->max_nb > MAX_NB) return -1;
-    const long ppv = (long)f->mi_w * f->mi_h, total = ppv * f->n_views;
+    const long ppv = (long)f->mi_w * f->mi_h;
+    const long t0 = (long)v0 * ppv, t1 = (long)v1 * ppv;
     long long taps = 0;
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads) reduction(+ : taps)
 #endif
-    for (long t = 0; t < total; ++t) {
+    for (long t = t0; t < t1; ++t) {
         long long mine = 0;
         const int vid = (int)(t / ppv);
         const int rem = (int)(t % ppv);
@@ -772,6 +773,12 @@ long long orc_pm_sweep_taps(const orc_frame* f, const orc_params* p, uint64_t se
     }
     (void)nthreads;
     return taps;
+}
+
+long long orc_pm_sweep_taps(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
+                            const orc_state* prev, orc_state* next, int nthreads)
+{
+    return orc_pm_sweep_views_taps(f, p, seed, iter, phase, prev, next, 0, f->n_views, nthreads);
 }
 
 int orc_pm_sweep(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,

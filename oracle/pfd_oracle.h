@@ -100,6 +100,9 @@ int orc_pm_sweep(const orc_frame* f, const orc_params* p, uint64_t seed, int ite
  * evaluates in it (the roofline's algorithmic unit), or -1. */
 long long orc_pm_sweep_taps(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
                             const orc_state* prev, orc_state* next, int nthreads);
+/* orc_pm_sweep_taps on views [v0, v1) only. */
+long long orc_pm_sweep_views_taps(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
+                                  const orc_state* prev, orc_state* next, int v0, int v1, int nthreads);
 int orc_pm_sweep_views(const orc_frame* f, const orc_params* p, uint64_t seed, int iter, int phase,
                        const orc_state* prev, orc_state* next, int v0, int v1, int nthreads);
 

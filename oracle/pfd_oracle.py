@@ -97,6 +97,8 @@ def lib() -> ctypes.CDLL:
         L.orc_pm_init_views.argtypes = [FP, PP, ctypes.c_uint64, SP, _I, _I, _I]
         L.orc_pm_sweep.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I]
         L.orc_pm_sweep_views.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I, _I, _I]
+        L.orc_pm_sweep_views_taps.argtypes = [FP, PP, ctypes.c_uint64, _I, _I, SP, SP, _I, _I, _I]
+        L.orc_pm_sweep_views_taps.restype = ctypes.c_longlong
         L.orc_patchmatch.argtypes = [FP, PP, ctypes.c_uint64, SP, _I]
         L.orc_acmm_post_refine.argtypes = [FP, PP, SP, _I]
         L.orc_expf.argtypes = [_F]
@@ -236,13 +238,18 @@ class Oracle:
         assert rc == 0
         return arr
 
-    def sweep_taps(self, params, seed, it, phase, prev, nthreads=0):
-        """(next state, in-bounds NCC taps of the reference's algorithm in this sweep)."""
+    def sweep_taps(self, params, seed, it, phase, prev, nthreads=0, views=None):
+        """(next state, in-bounds NCC taps of the reference's algorithm in this
+        sweep, over the views [views[0], views[1]) when given)."""
         arr, st = self.new_state()
         ps = OrcState(_p(prev["plane"]), _p(prev["cost"]), _p(prev["disp"]), _p(prev["sel"]))
         p = self.params(params)
-        taps = lib().orc_pm_sweep_taps(ctypes.byref(self.f), ctypes.byref(p), seed, it, phase, ctypes.byref(ps),
-                                       ctypes.byref(st), nthreads)
+        if views is None:
+            taps = lib().orc_pm_sweep_taps(ctypes.byref(self.f), ctypes.byref(p), seed, it, phase, ctypes.byref(ps),
+                                           ctypes.byref(st), nthreads)
+        else:
+            taps = lib().orc_pm_sweep_views_taps(ctypes.byref(self.f), ctypes.byref(p), seed, it, phase,
+                                                 ctypes.byref(ps), ctypes.byref(st), views[0], views[1], nthreads)
         assert taps >= 0
         return arr, int(taps)
 

@@ -9,7 +9,7 @@
  * from the reference tree, so the frame kernels' static helpers are callable
  * here; MIStereo/AdaptMIPMUtil.cu is a separate object linked with
  * separable compilation, as CUDA_SEPARABLE_COMPILATION does in the
- * reference's build (CMakeLists.txt:27, :113-115).
+ * reference's build (CMakeLists.txt:27, :112-115).
  *   - pfdref_ncc_costs: ComputeMultiViewCostVector_Frame (AdaptMIPMFrame.cu:
  *     181-225) on given (view, pixel, plane) hypotheses, one thread each;
  *   - pfdref_patchmatch: the reference's RunPatchMatchCUDAForFrame_Impl
@@ -427,6 +427,65 @@ int pfdref_patchmatch(pfdref_frame* f, const pfdref_params* p, uint64_t seed, fl
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
+    f->seeded = true;
+    ok(cudaGetLastError(), "launch");
+    return g_first_error == cudaSuccess ? 0 : -3;
+}
+
+/* A bounded sample of the reference's whole run: RunPatchMatchCUDAForFrame_Impl
+ * launched with num_views = n, so its kernels update views [0, n) only (the
+ * caller puts the sampled block of views first).  Every view is initialised
+ * first, untimed, and both state buffers get that state, so the views past n
+ * that the sample's proposals read hold a valid (initial) plane throughout.
+ * ms[0] receives the device time of the sample's initialisation, ms[1] of its
+ * half-sweeps (CUDA events on the default stream). */
+int pfdref_patchmatch_sample(pfdref_frame* f, const pfdref_params* p, uint64_t seed, int n, float* ms)
+{
+    if (!f || n < 1 || n > f->V) return -1;
+    g_first_error = cudaSuccess;
+    g_error_text.clear();
+    PatchMatchParamsLF q = to_lf(p, f->mi, f->max_nb);
+    if (!set_seed(seed)) return -3;
+#ifdef PFD_REF_RNG_PHILOX
+    set_sweep(0);
+#endif
+    const dim3 block(16, 16, 1), grid = grid_of(f);
+    RandomInitializationForFrame<<<grid, block>>>(f->tex_dev, f->centers, f->tilekeys, f->nb_ids, f->nb_counts,
+                                                  f->max_nb, f->plane[0], f->cost[0], f->disp[0], f->sel[0],
+                                                  f->states, q, f->mi, f->mi, f->V);
+    CUDA_SAFE_CALL(cudaDeviceSynchronize());
+    const size_t px = (size_t)f->V * f->mi * f->mi;
+    ok(cudaMemcpy(f->plane[1], f->plane[0], sizeof(float4) * px, cudaMemcpyDeviceToDevice), "copy");
+    ok(cudaMemcpy(f->cost[1], f->cost[0], sizeof(float) * px, cudaMemcpyDeviceToDevice), "copy");
+    ok(cudaMemcpy(f->disp[1], f->disp[0], sizeof(float4) * px, cudaMemcpyDeviceToDevice), "copy");
+    ok(cudaMemcpy(f->sel[1], f->sel[0], sizeof(unsigned int) * px, cudaMemcpyDeviceToDevice), "copy");
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    const dim3 sgrid((f->mi + 15) / 16, (f->mi + 15) / 16, n);
+    cudaEventRecord(e0, 0);
+    RandomInitializationForFrame<<<sgrid, block>>>(f->tex_dev, f->centers, f->tilekeys, f->nb_ids, f->nb_counts,
+                                                   f->max_nb, f->plane[0], f->cost[0], f->disp[0], f->sel[0],
+                                                   f->states, q, f->mi, f->mi, n);
+    CUDA_SAFE_CALL(cudaDeviceSynchronize());
+    cudaEventRecord(e1, 0);
+    RunPatchMatchCUDAForFrame_Impl(f->tex_dev, f->centers, f->tilekeys, f->nb_ids, f->nb_counts, f->plane[0],
+                                   f->plane[1], f->cost[0], f->cost[1], f->disp[0], f->disp[1], f->sel[0], f->sel[1],
+                                   f->states, q, n, f->max_nb);
+    cudaEventRecord(e2, 0);
+    cudaEventSynchronize(e2);
+    float init = 0.0f, whole = 0.0f;
+    cudaEventElapsedTime(&init, e0, e1);
+    cudaEventElapsedTime(&whole, e1, e2);
+    if (ms) {
+        ms[0] = init;
+        ms[1] = whole - init;   /* the Impl initialises the sample again before its sweeps */
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    f->cur = 0;
     f->seeded = true;
     ok(cudaGetLastError(), "launch");
     return g_first_error == cudaSuccess ? 0 : -3;

@@ -8,6 +8,8 @@ never by the product.  Two builds of the same kernels:
   * libref_frame_philox.so the kernels drawing the engine's Philox streams, so
                            a run follows the same random numbers as the
                            engine and the CPU oracle
+  * libref_frame_ieee.so   the Philox build without --use_fast_math: the
+                           reference's own sensitivity to its arithmetic
 
     ref = RefFrame(workload, philox=True)
     costs = ref.ncc_costs(params, vids, pxy, planes)
@@ -26,6 +28,7 @@ ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(ORACLE_DIR, "_ref")
 LIB_XORWOW = os.path.join(REF_DIR, "libref_frame.so")
 LIB_PHILOX = os.path.join(REF_DIR, "libref_frame_philox.so")
+LIB_IEEE = os.path.join(REF_DIR, "libref_frame_ieee.so")
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -38,12 +41,12 @@ class RefParams(ctypes.Structure):
 
 
 def available() -> bool:
-    return os.path.exists(LIB_XORWOW) and os.path.exists(LIB_PHILOX)
+    return all(os.path.exists(p) for p in (LIB_XORWOW, LIB_PHILOX, LIB_IEEE))
 
 
 def build(reference_tree: str = "/root/reference") -> bool:
     """make -C oracle/ref when the reference tree is present (this container);
-    elsewhere the prebuilt libraries are used.  Returns whether both exist."""
+    elsewhere the prebuilt libraries are used.  Returns whether all exist."""
     if os.path.isdir(reference_tree):
         r = subprocess.run(["make", "-s", "-C", os.path.join(ORACLE_DIR, "ref"), "REF=" + reference_tree],
                            capture_output=True, text=True)
@@ -55,8 +58,8 @@ def build(reference_tree: str = "/root/reference") -> bool:
 _libs: dict = {}
 
 
-def lib(philox: bool) -> ctypes.CDLL:
-    path = LIB_PHILOX if philox else LIB_XORWOW
+def lib(philox: bool, ieee: bool = False) -> ctypes.CDLL:
+    path = LIB_IEEE if ieee else (LIB_PHILOX if philox else LIB_XORWOW)
     if path not in _libs:
         if not os.path.exists(path):
             raise ImportError(f"{path} is missing: build it with make -C oracle/ref (needs the reference tree)")
@@ -66,6 +69,7 @@ def lib(philox: bool) -> ctypes.CDLL:
         L.pfdref_frame_destroy.argtypes = [_P]
         L.pfdref_ncc_costs.argtypes = [_P, ctypes.POINTER(RefParams), _P, _P, _P, _I, _P]
         L.pfdref_patchmatch.argtypes = [_P, ctypes.POINTER(RefParams), ctypes.c_uint64, _P]
+        L.pfdref_patchmatch_sample.argtypes = [_P, ctypes.POINTER(RefParams), ctypes.c_uint64, _I, _P]
         L.pfdref_init.argtypes = [_P, ctypes.POINTER(RefParams), ctypes.c_uint64]
         L.pfdref_sweep.argtypes = [_P, ctypes.POINTER(RefParams), ctypes.c_uint64, _I, _I]
         L.pfdref_download.argtypes = [_P, _P, _P, _P, _P]
@@ -88,8 +92,8 @@ def to_params(p) -> RefParams:
 class RefFrame:
     """One frame bound to the reference's textures and state buffers."""
 
-    def __init__(self, w, philox: bool = True, blur: np.ndarray | None = None):
-        self.L = lib(philox)
+    def __init__(self, w, philox: bool = True, blur: np.ndarray | None = None, ieee: bool = False):
+        self.L = lib(philox, ieee)
         self.V = int(w.centers.shape[0])
         self.mi = int(w.mi)
         self.max_nb = int(w.nb_ids.shape[1])
@@ -133,6 +137,15 @@ class RefFrame:
         ms = np.zeros(2, np.float32)
         P = to_params(params)
         self._check(self.L.pfdref_patchmatch(self.h, ctypes.byref(P), seed, _ptr(ms)), "pfdref_patchmatch")
+        return float(ms[0]), float(ms[1])
+
+    def patchmatch_sample(self, params, seed: int, n: int):
+        """The reference's run on views [0, n) only (every view initialised
+        first, untimed); returns (init ms, sweeps ms) of the sample."""
+        ms = np.zeros(2, np.float32)
+        P = to_params(params)
+        self._check(self.L.pfdref_patchmatch_sample(self.h, ctypes.byref(P), seed, n, _ptr(ms)),
+                    "pfdref_patchmatch_sample")
         return float(ms[0]), float(ms[1])
 
     def init(self, params, seed: int):

@@ -172,7 +172,12 @@ extern "C" int orc_select_neighbors(int n_views, const float* centers, const int
     for (size_t i = 0; i < bin.size(); ++i) bin[i] = images[i] > 128 ? 255 : 0;   // threshold(128, BINARY)
     float delt = 0.15f;
     delt *= pitch;
+    // views in parallel, as the reference's loop (SelectNeighbors.cpp:123, omp
+    // parallel for, schedule(dynamic)); each thread has its own ring marks
+#pragma omp parallel
+    {
     RingSearch R{ G, L, pitch, delt, std::vector<char>(V, 0), {} };
+#pragma omp for schedule(dynamic, 16)
     for (int v = 0; v < V; ++v) {
         for (int t : R.touched) R.seen[t] = 0;
         R.touched.clear();
@@ -254,6 +259,7 @@ extern "C" int orc_select_neighbors(int n_views, const float* centers, const int
             nb_ids[(size_t)v * max_out + k] = k < n ? sv[k].first : -1;
             if (nb_sim) nb_sim[(size_t)v * max_out + k] = k < n ? scores[{ rows[sv[k].first], cols[sv[k].first] }].second.similarity : 0.0f;
         }
+    }
     }
     return 0;
 }

@@ -25,6 +25,8 @@ SYNTH_PATH = os.path.join(BUILD_DIR, "libpfd_synth.so")
 
 PFD_OK = 0
 PFD_ETIMEDOUT = -5
+SWEEP_SHAPES = 4
+SHAPE_AUTOTUNE = -1
 _ERRNAMES = {-1: "PFD_EINVAL", -2: "PFD_ENOMEM", -3: "PFD_ECUDA", -4: "PFD_ENOFRAME",
              -5: "PFD_ETIMEDOUT", -6: "PFD_ENODEV", -7: "PFD_ESTATE"}
 
@@ -213,7 +215,6 @@ def lib() -> ctypes.CDLL:
             "pfd_neighbors_by_baseline": [_P, _P, _I, _F, _I, _I, _P, _P],
             "pfd_set_tap_counting": [_P, _I],
             "pfd_read_tap_count": [_P, ctypes.POINTER(ctypes.c_ulonglong)],
-            "pfd_fp32_fma_rate": [_P, ctypes.POINTER(ctypes.c_double)],
             "pfd_filter": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P, _P],
             "pfd_reprojection_error": [_P, _I, ctypes.POINTER(FilterCfgC), _F, _P],
             "pfd_refocus": [_P, _I, _P, _I, _I, _I, _P],
@@ -236,6 +237,9 @@ def lib() -> ctypes.CDLL:
             "pfd_frame_bytes": [_I, _I, _I, _I, _I, _I, _I],
             "pfd_select_neighbors": [_P, _P, _P, _I, _I, _I, _F, _P, _I, _I, _I, _P, _P],
             "pfd_frame_select_neighbors": [_P, _I, _I, _I, _F, _I, _P, _P],
+            "pfd_set_sweep_shape": [_P, _I],
+            "pfd_sweep_shape_info": [_I, _P, _P],
+            "pfd_tuned_sweep_shape": [_P, _I, _P, _P],
             "pfd_mla_centers": [_P, _P, _I, _I, _I, _F, _I, _I, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
             "pfd_fuse_virtual_depth": [_P, _I, ctypes.POINTER(FuseParamsC), _P, _P, _I, _P, _P, _P, _P, _P, _P,
                                        ctypes.POINTER(ctypes.c_longlong)],
@@ -489,6 +493,19 @@ class Context:
         self._check(self._L.pfd_patchmatch_batch(self._h, _ptr(ids), len(ids), ctypes.cast(arr, _P), _ptr(sd)),
                     "pfd_patchmatch_batch")
 
+    def set_sweep_shape(self, shape: int) -> None:
+        """Launch shape of later half-sweeps: 0 .. SWEEP_SHAPES - 1, or
+        SHAPE_AUTOTUNE (-1) for the engine's autotuner."""
+        self._check(self._L.pfd_set_sweep_shape(self._h, int(shape)), "pfd_set_sweep_shape")
+
+    def tuned_sweep_shape(self, fid: int, params: "PmParams") -> int:
+        """The autotuner's shape for the frame's key, or -1 if not tuned yet."""
+        out = _I(-1)
+        p = params.c()
+        self._check(self._L.pfd_tuned_sweep_shape(self._h, fid, ctypes.byref(p), ctypes.byref(out)),
+                    "pfd_tuned_sweep_shape")
+        return out.value
+
     def set_matcher(self, acmm: bool) -> None:
         """PatchMatch rules of the context's later calls: the ACMM matcher at one
         pyramid level (PFD_MATCHER_ACMM) or the Frame matcher (the default)."""
@@ -504,11 +521,6 @@ class Context:
     def read_tap_count(self) -> int:
         v = ctypes.c_ulonglong()
         self._check(self._L.pfd_read_tap_count(self._h, ctypes.byref(v)), "pfd_read_tap_count")
-        return v.value
-
-    def fp32_fma_rate(self) -> float:
-        v = ctypes.c_double()
-        self._check(self._L.pfd_fp32_fma_rate(self._h, ctypes.byref(v)), "pfd_fp32_fma_rate")
         return v.value
 
     def filter(self, fid: int, cfg: FilterCfg, baseline_unit: float, download: bool = True):
@@ -798,6 +810,14 @@ class SynthConfigC(ctypes.Structure):
     _fields_ = [("width", _I), ("height", _I), ("pitch", _F), ("n_planes", _I), ("vd_min", _F), ("vd_max", _F),
                 ("noise_sigma", _F), ("n_lens_types", _I), ("blur_sigma", _F * 3), ("texture_cell", _F),
                 ("seed", ctypes.c_uint64)]
+
+
+def sweep_shape_info(shape: int) -> tuple:
+    """(warps per CTA, CTAs per SM) of a sweep launch shape."""
+    w, c = _I(), _I()
+    if lib().pfd_sweep_shape_info(int(shape), ctypes.byref(w), ctypes.byref(c)) != 0:
+        raise ValueError(f"no sweep shape {shape}")
+    return w.value, c.value
 
 
 def synth_lib() -> ctypes.CDLL:

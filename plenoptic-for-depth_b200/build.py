@@ -6,6 +6,7 @@ out as __fmaf_rn, so the arithmetic is exactly the one the CPU oracle states.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -23,7 +24,7 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "-ccbin", "/usr/bin/g++",
 ]
 
-CU_SOURCES = ["pm_kernels.cu", "pm_sweep.cu", "check_kernels.cu", "refocus_kernels.cu", "vdrd_kernels.cu", "fuse_kernels.cu", "mla_kernels.cu", "select_kernels.cu", "blur_kernels.cu", "pfd_abi.cu", "diag.cu"]
+CU_SOURCES = ["pm_kernels.cu", "pm_sweep.cu", "check_kernels.cu", "refocus_kernels.cu", "vdrd_kernels.cu", "fuse_kernels.cu", "mla_kernels.cu", "select_kernels.cu", "blur_kernels.cu", "pfd_abi.cu"]
 CPP_SOURCES = ["neighbors.cpp", "server.cpp", "calib_xml.cpp"]
 SYNTH_LIB = os.path.join(OUT, "libpfd_synth.so")
 HOST_DIR = os.path.join(PKG_DIR, "host")
@@ -63,19 +64,24 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     deps = _deps() + [__file__]
     if not force and not _stale(LIB, deps):
         return LIB
-    objs = []
+    objs, cmds = [], []
     for src in CU_SOURCES:
         obj = os.path.join(OUT, src.replace(".cu", ".o"))
         cmd = [NVCC, *ARCH, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        _run(cmd)
+        cmds.append(cmd)
         objs.append(obj)
     for src in CPP_SOURCES:
         obj = os.path.join(OUT, src.replace(".cpp", ".o"))
-        _run(["/usr/bin/g++", "-std=c++17", "-O2", "-fPIC", "-I", os.path.join(ROOT, "include"),
-              "-I", "/usr/local/cuda/include", "-c", os.path.join(CSRC, src), "-o", obj])
+        cmds.append(["/usr/bin/g++", "-std=c++17", "-O2", "-fPIC", "-I", os.path.join(ROOT, "include"),
+                     "-I", "/usr/local/cuda/include", "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+    # the translation units are independent: compile them side by side, the
+    # largest (the sweep's kernel variants) first
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, c) for c in sorted(cmds, key=lambda c: "pm_sweep" not in c[-3])]:
+            f.result()
     tmp = LIB + ".tmp"
     _run([NVCC, *ARCH, "-shared", "-Xlinker", "-soname=libpfd.so", "-o", tmp, *objs, "-ccbin", "/usr/bin/g++"])
     os.replace(tmp, LIB)
@@ -110,17 +116,20 @@ def build_synth(force: bool = False) -> str:
 
 TEST_OUT = os.path.join(ROOT, "tests", "_build")
 TEX_PROBE = os.path.join(TEST_OUT, "libtexprobe.so")
+FMA_PROBE = os.path.join(TEST_OUT, "libfmaprobe.so")
 SHIM_PROBE = os.path.join(TEST_OUT, "libshimprobe.so")
 
 
 def build_test_helpers(force: bool = False) -> str:
-    """Compile the texture-probe helper the device tests use."""
+    """Compile the device probes the tests and bench.py use (the texture
+    probe, the FP32 throughput probe) and the C++ drop-in probe."""
     os.makedirs(TEST_OUT, exist_ok=True)
-    src = os.path.join(ROOT, "tests", "csrc", "tex_probe.cu")
-    if force or _stale(TEX_PROBE, [src, __file__]):
-        tmp = TEX_PROBE + ".tmp"
-        _run([NVCC, *ARCH, "-O2", "-shared", "-Xcompiler", "-fPIC", "-ccbin", "/usr/bin/g++", src, "-o", tmp])
-        os.replace(tmp, TEX_PROBE)
+    for name, lib_path in (("tex_probe.cu", TEX_PROBE), ("fma_probe.cu", FMA_PROBE)):
+        src = os.path.join(ROOT, "tests", "csrc", name)
+        if force or _stale(lib_path, [src, __file__]):
+            tmp = lib_path + ".tmp"
+            _run([NVCC, *ARCH, "-O2", "-shared", "-Xcompiler", "-fPIC", "-ccbin", "/usr/bin/g++", src, "-o", tmp])
+            os.replace(tmp, lib_path)
     host = build_host()
     src = os.path.join(ROOT, "tests", "csrc", "shim_probe.cpp")
     if force or _stale(SHIM_PROBE, [src, host, __file__] + _deps()):

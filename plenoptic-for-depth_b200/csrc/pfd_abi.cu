@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <new>
 #include <string>
 #include <vector>
@@ -91,6 +92,7 @@ struct pfd_ctx {
     unsigned long long launches = 0;        // kernels this context has launched
     float* d_scratch = nullptr;             // sweep candidate costs, per resident CTA
     size_t scratch_bytes = 0;
+    int sweep_shape = 0;                    // launch shape of the half-sweeps, or PFD_SHAPE_AUTOTUNE
     std::string last_error;
 };
 
@@ -375,18 +377,6 @@ pfd_status pfd_read_tap_count(pfd_ctx* ctx, unsigned long long* taps)
     CU(cudaMemcpyAsync(taps, ctx->d_taps, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaMemsetAsync(ctx->d_taps, 0, sizeof(unsigned long long), ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
-    return PFD_OK;
-}
-
-pfd_status pfd_fp32_fma_rate(pfd_ctx* ctx, double* tflops)
-{
-    if (!ctx || !tflops) return PFD_EINVAL;
-    DeviceGuard g(ctx->device);
-    float ms = 0.0f;
-    double flops = 0.0;
-    CU(pfd::measure_fma_rate(ctx->stream, &ms, &flops));
-    ctx->launches += 4;                      // warm-up + three timed launches
-    *tflops = flops / (ms * 1e-3) / 1e12;
     return PFD_OK;
 }
 
@@ -730,6 +720,149 @@ static pfd_status ensure_scratch(pfd_ctx* ctx, size_t need)
     return PFD_OK;
 }
 
+// ---- launch shapes of the half-sweep and their autotuner -------------------------
+//
+// Every shape (warps per CTA, CTAs per SM the registers are sized for) computes
+// the same state bit for bit; which is fastest depends on the frame's window,
+// neighbour count, patch and channels, through the shared-memory plan (CTAs
+// that fit an SM), the registers (spills) and the pixels per micro-image
+// (warps per staged view).  The autotuner times each shape once per such key
+// and device on the frame's own half-sweep and keeps the fastest for the
+// process.
+
+namespace {
+
+struct ShapeKey {
+    int dev, W, H, K, ntap, inc, blur, shift, acmm;
+    bool operator<(const ShapeKey& o) const
+    {
+        return std::tie(dev, W, H, K, ntap, inc, blur, shift, acmm) <
+               std::tie(o.dev, o.W, o.H, o.K, o.ntap, o.inc, o.blur, o.shift, o.acmm);
+    }
+};
+
+std::mutex g_shape_mu;
+std::map<ShapeKey, int> g_shape_cache;
+
+ShapeKey shape_key(const pfd_ctx* ctx, const Frame& f, const pfd::PmParams& P)
+{
+    return ShapeKey{ ctx->device, P.W, P.H, P.K, P.ntap, P.inc, f.has_blur ? 1 : 0, P.shifted, P.acmm };
+}
+
+int cached_shape(const ShapeKey& k)
+{
+    std::lock_guard<std::mutex> lock(g_shape_mu);
+    auto it = g_shape_cache.find(k);
+    return it == g_shape_cache.end() ? -1 : it->second;
+}
+
+}  // namespace
+
+// Runs the frame's half-sweep (iter, phase) once in every shape, from its
+// current state into the other buffer, with the stored cost vectors neither
+// read nor written (so every trial computes the same state), timing each on
+// the context's stream; records the fastest for the frame's key.
+static pfd_status tune_shape(pfd_ctx* ctx, Frame& f, pfd::PmParams P, int iter, int phase, int* out)
+{
+    P.cvec_ok = 0;
+    P.cvec = nullptr;
+    P.tap_counter = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    CU(cudaEventCreate(&a));
+    if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return fail(ctx, PFD_ECUDA, "event"); }
+    int best = 0;
+    float best_ms = 0.0f;
+    pfd_status st = PFD_OK;
+    for (int shape = 0; shape < pfd::kSweepShapes && st == PFD_OK; ++shape) {
+        if (pfd::sweep_warp_smem_bytes(P, f.has_blur, shape) > 227 * 1024) continue;
+        int n_ctas = 0;
+        if (pfd::sweep_warp_grid(P, f.has_blur, &n_ctas, shape) != cudaSuccess) {
+            cudaGetLastError();                      // this shape does not fit the plan: not a candidate
+            continue;
+        }
+        st = ensure_scratch(ctx, pfd::sweep_warp_scratch_bytes(P, n_ctas, shape));
+        if (st != PFD_OK) break;
+        pfd::PmParams Q = P;
+        Q.cost_scratch = ctx->d_scratch;
+        Q.scratch_floats = ctx->scratch_bytes / sizeof(float);
+        cudaError_t e = cudaEventRecord(a, ctx->stream);
+        if (e == cudaSuccess)
+            e = pfd::launch_sweep_warp(frame_dev(f), Q, f.s[f.cur], f.s[f.cur ^ 1], iter, phase, n_ctas, ctx->d_err,
+                                       ctx->stream, shape);
+        if (e == cudaSuccess) e = cudaEventRecord(b, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            st = fail(ctx, PFD_ECUDA, "sweep autotune, shape %d: %s", shape, cudaGetErrorString(e));
+            break;
+        }
+        ctx->launches += 1;
+        if (shape == 0 || ms < best_ms) { best = shape; best_ms = ms; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (st != PFD_OK) return st;
+    st = check_device_error(ctx);
+    if (st != PFD_OK) return st;
+    {
+        std::lock_guard<std::mutex> lock(g_shape_mu);
+        g_shape_cache[shape_key(ctx, f, P)] = best;
+    }
+    *out = best;
+    return PFD_OK;
+}
+
+// The shape the context's next half-sweep of frame f runs: the fixed one, or
+// under PFD_SHAPE_AUTOTUNE the tuned one (tuning on this half-sweep when the
+// key is new).  Tap counting runs shape 0.
+static pfd_status sweep_shape_for(pfd_ctx* ctx, Frame& f, const pfd::PmParams& P, int iter, int phase, int* shape)
+{
+    *shape = 0;
+    if (ctx->counting) return PFD_OK;
+    if (ctx->sweep_shape != PFD_SHAPE_AUTOTUNE) {
+        *shape = ctx->sweep_shape;
+        return PFD_OK;
+    }
+    const int c = cached_shape(shape_key(ctx, f, P));
+    if (c >= 0) {
+        *shape = c;
+        return PFD_OK;
+    }
+    return tune_shape(ctx, f, P, iter, phase, shape);
+}
+
+pfd_status pfd_set_sweep_shape(pfd_ctx* ctx, int shape)
+{
+    if (!ctx) return PFD_EINVAL;
+    if (shape != PFD_SHAPE_AUTOTUNE && (shape < 0 || shape >= PFD_SWEEP_SHAPES))
+        return fail(ctx, PFD_EINVAL, "sweep shape %d: give 0-%d or PFD_SHAPE_AUTOTUNE", shape, PFD_SWEEP_SHAPES - 1);
+    ctx->sweep_shape = shape;
+    return PFD_OK;
+}
+
+pfd_status pfd_sweep_shape_info(int shape, int* warps_per_cta, int* ctas_per_sm)
+{
+    static const int kMin[PFD_SWEEP_SHAPES] = { 4, 3, 6, 2 };
+    static_assert(PFD_SWEEP_SHAPES == pfd::kSweepShapes, "shape tables");
+    if (shape < 0 || shape >= PFD_SWEEP_SHAPES) return PFD_EINVAL;
+    if (warps_per_cta) *warps_per_cta = pfd::sweep_shape_warps(shape);
+    if (ctas_per_sm) *ctas_per_sm = kMin[shape];
+    return PFD_OK;
+}
+
+pfd_status pfd_tuned_sweep_shape(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, int* shape)
+{
+    if (!ctx || !shape) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    const pfd_status st = check_params(ctx, *f, params);
+    if (st != PFD_OK) return st;
+    *shape = cached_shape(shape_key(ctx, *f, make_params(ctx, *f, params, 0)));
+    return PFD_OK;
+}
+
 pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed, int iter, int phase)
 {
     if (!ctx) return PFD_EINVAL;
@@ -745,15 +878,18 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
     if (ctx->counting) P.tap_counter = ctx->d_taps;
     if (pfd::sweep_warp_smem_bytes(P, f->has_blur) > 227 * 1024)
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
+    int shape = 0;
+    st = sweep_shape_for(ctx, *f, P, iter, phase, &shape);
+    if (st != PFD_OK) return st;
     int n_ctas = 0;
-    CU(pfd::sweep_warp_grid(P, f->has_blur, &n_ctas));
-    st = ensure_scratch(ctx, pfd::sweep_warp_scratch_bytes(P, n_ctas));
+    CU(pfd::sweep_warp_grid(P, f->has_blur, &n_ctas, shape));
+    st = ensure_scratch(ctx, pfd::sweep_warp_scratch_bytes(P, n_ctas, shape));
     if (st != PFD_OK) return st;
     P.cost_scratch = ctx->d_scratch;
     P.scratch_floats = ctx->scratch_bytes / sizeof(float);
     P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, cost_mode(ctx));
     CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
-                              ctx->stream));
+                              ctx->stream, shape));
     ctx->launches += 1;
     f->cur ^= 1;
     if (ctx->counting) f->cvec_valid = 0;        // tap counting evaluates everything and stores nothing
@@ -818,12 +954,39 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
     int k_max = 0;
     for (int b = 0; b < n; ++b) k_max = std::max(k_max, fr[b]->K);
     const int stride = pfd::sweep_warp_stride(k_max);
+    // launch shape per group: the fixed one, or the one tuned for the group's
+    // largest frame (tuned on that frame's first half-sweep when its key is new)
+    int shape[2] = { 0, 0 };
     for (int grp = 0; grp < 2; ++grp) {
         if (!used[grp]) continue;
-        CU(pfd::sweep_batch_grid(smem[grp], grp == 1, shift, &n_ctas[grp]));
+        int big = -1;
+        for (int b = 0; b < n; ++b)
+            if ((fr[b]->has_blur ? 1 : 0) == grp && params[b].max_iterations > 0 &&
+                (big < 0 || (size_t)fr[b]->V * fr[b]->mi_w * fr[b]->mi_h > (size_t)fr[big]->V * fr[big]->mi_w * fr[big]->mi_h))
+                big = b;
+        if (big >= 0) {
+            const pfd::PmParams Pb = make_params(ctx, *fr[big], &params[big], seeds[big]);
+            const pfd_status st = sweep_shape_for(ctx, *fr[big], Pb, 0, 0, &shape[grp]);
+            if (st != PFD_OK) return st;
+        }
+        // every frame's plan in the chosen shape (the warps' area grows with the warps)
+        smem[grp] = 0;
+        for (int b = 0; b < n; ++b)
+            if ((fr[b]->has_blur ? 1 : 0) == grp)
+                smem[grp] = std::max(smem[grp], pfd::sweep_warp_smem_bytes(make_params(ctx, *fr[b], &params[b], seeds[b]),
+                                                                        grp == 1, shape[grp]));
+        if (smem[grp] > 227 * 1024) shape[grp] = 0;
+        if (shape[grp] == 0) {
+            smem[grp] = 0;
+            for (int b = 0; b < n; ++b)
+                if ((fr[b]->has_blur ? 1 : 0) == grp)
+                    smem[grp] = std::max(smem[grp], pfd::sweep_warp_smem_bytes(make_params(ctx, *fr[b], &params[b],
+                                                                                        seeds[b]), grp == 1, 0));
+        }
+        CU(pfd::sweep_batch_grid(smem[grp], grp == 1, shift, &n_ctas[grp], shape[grp]));
         pfd::PmParams Pk = {};
         Pk.K = k_max;                                  // the scratch of n_ctas CTAs at that stride
-        scratch = std::max(scratch, pfd::sweep_warp_scratch_bytes(Pk, n_ctas[grp]));
+        scratch = std::max(scratch, pfd::sweep_warp_scratch_bytes(Pk, n_ctas[grp], shape[grp]));
     }
     pfd_status st = ensure_scratch(ctx, scratch);
     if (st != PFD_OK) return st;
@@ -875,7 +1038,7 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
         for (int grp = 0, off = 0; grp < 2; off += count[grp], ++grp) {
             if (!count[grp]) continue;
             const cudaError_t e = pfd::launch_sweep_batch(row + off, count[grp], grp == 1, shift, smem[grp],
-                                                          n_ctas[grp], ctx->d_err, ctx->stream);
+                                                          n_ctas[grp], ctx->d_err, ctx->stream, shape[grp]);
             if (e != cudaSuccess) {
                 st = fail(ctx, PFD_ECUDA, "launch_sweep_batch: %s", cudaGetErrorString(e));
                 break;

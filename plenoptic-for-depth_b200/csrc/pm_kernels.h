@@ -21,13 +21,18 @@ cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, 
                        const int* hyp_out, float* costs, int* err, cudaStream_t st);
 // The warp-per-pixel sweep (pm_sweep.cu): grid, shared memory, and the global
 // scratch it needs (P.cost_scratch: per warp, the cost vectors of one pixel).
-cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas);
-int sweep_warp_smem_bytes(const PmParams& P, bool blur);
-size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas);
+// shape selects one of kSweepShapes launch shapes (warps per CTA and CTAs per
+// SM the registers are sized for); every shape computes the same result bit
+// for bit.  Shape 0 is the default; tap counting always runs shape 0.
+constexpr int kSweepShapes = 4;
+int sweep_shape_warps(int shape);
+cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas, int shape = 0);
+int sweep_warp_smem_bytes(const PmParams& P, bool blur, int shape = 0);
+size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas, int shape = 0);
 // Floats of global scratch one warp uses for K neighbours (PmParams::scratch_stride).
 int sweep_warp_stride(int K);
 cudaError_t launch_sweep_warp(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
-                              int iter, int phase, int n_ctas, int* err, cudaStream_t st);
+                              int iter, int phase, int n_ctas, int* err, cudaStream_t st, int shape = 0);
 // One frame's half-sweep in a launch over several frames (pm_sweep_batch_kernel).
 struct SweepItem {
     FrameDev F;
@@ -36,11 +41,9 @@ struct SweepItem {
     int iter, phase;
 };
 // Grid of the batch kernel for `smem` bytes of dynamic shared memory per CTA.
-cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, int* n_ctas);
+cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, int* n_ctas, int shape = 0);
 // items: device array of n frames, all with or all without a blur channel.
 cudaError_t launch_sweep_batch(const SweepItem* items, int n, bool blur, bool shift, int smem, int n_ctas, int* err,
-                               cudaStream_t st);
-// FP32 FFMA throughput probe (diag.cu): best of three timed launches.
-cudaError_t measure_fma_rate(cudaStream_t st, float* ms, double* flops);
+                               cudaStream_t st, int shape = 0);
 
 }  // namespace pfd

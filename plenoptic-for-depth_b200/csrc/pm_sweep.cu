@@ -36,8 +36,16 @@ namespace pfd {
 
 namespace {
 
-constexpr int kWarps = 7;
-constexpr int kThreads = 32 * kWarps;
+// Launch shapes: (warps per CTA, CTAs per SM the registers are sized for).
+// Shape 0 is the default; the others are the autotuner's alternatives
+// (pfd_set_autotune), which trade resident CTAs for warps per CTA and
+// registers per thread as the frame's shared-memory plan allows.
+template <int S> struct ShapeOf;
+template <> struct ShapeOf<0> { static constexpr int warps = 7, min_ctas = 4; };
+template <> struct ShapeOf<1> { static constexpr int warps = 8, min_ctas = 3; };
+template <> struct ShapeOf<2> { static constexpr int warps = 4, min_ctas = 6; };
+template <> struct ShapeOf<3> { static constexpr int warps = 10, min_ctas = 2; };
+constexpr int kShapeWarps[kSweepShapes] = { ShapeOf<0>::warps, ShapeOf<1>::warps, ShapeOf<2>::warps, ShapeOf<3>::warps };
 
 struct Quad {
     const float* R;          // [H][W] reference texels
@@ -83,7 +91,7 @@ struct Plan {
     int total;
 
     __host__ __device__ static int a16(int v) { return (v + 15) & ~15; }
-    __host__ __device__ static Plan make(int W, int H, int K, int ntap, bool blur, int tile_stride)
+    __host__ __device__ static Plan make(int W, int H, int K, int ntap, bool blur, int tile_stride, int warps)
     {
         Plan p;
         int o = 0;
@@ -110,20 +118,20 @@ struct Plan {
         p.off_warp = o;
         p.off_stage = o;
         const int stage_bytes = a16((1 + K) * tile_stride * (blur ? 2 : 1));
-        o += (kWarps * p.warp_bytes > stage_bytes) ? kWarps * p.warp_bytes : stage_bytes;
+        o += (warps * p.warp_bytes > stage_bytes) ? warps * p.warp_bytes : stage_bytes;
         p.total = o;
         return p;
     }
     // stride: floats of global scratch per warp; a launch over several frames uses
     // the largest frame's, so CTAs on different frames never share a region
-    __device__ WarpBlock warp_block(unsigned char* smem, float* gscratch, int w, int K, int stride) const
+    __device__ WarpBlock warp_block(unsigned char* smem, float* gscratch, int w, int warps, int K, int stride) const
     {
         unsigned char* b = smem + off_warp + w * warp_bytes;
         WarpBlock S;
         S.tab = (float4*)b;                  b += a16(tab_n * 16);
         S.plane = (float4*)b;
         S.dp = S.plane + maxh;
-        float* g = gscratch + ((size_t)blockIdx.x * kWarps + w) * (size_t)stride;
+        float* g = gscratch + ((size_t)blockIdx.x * warps + w) * (size_t)stride;
         S.cost = g;
         S.pair = (uint16_t*)(g + maxh * K);
         S.wres = g + maxh * K + (maxh * K + 1) / 2;
@@ -592,13 +600,13 @@ __device__ __forceinline__ void refine_candidates(int x, int y, float4 best, flo
 // One half-sweep of one frame by this CTA: it takes the frame's micro-images
 // from P.view_queue until none is left.  parity: the staging barrier's phase,
 // carried across frames.  Returns false when a staging wait gave up.
-template <bool BLUR, bool COUNT, bool SHIFT>
+template <bool BLUR, bool COUNT, bool SHIFT, int WARPS>
 __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev& F, const PmParams& P,
                                             const StateDev& prev, const StateDev& next, int iter, int phase, int* err,
                                             uint32_t& parity)
 {
     const int W = P.W, H = P.H, K = P.K;
-    const Plan L = Plan::make(W, H, K, P.ntap, BLUR, P.tile_stride);
+    const Plan L = Plan::make(W, H, K, P.ntap, BLUR, P.tile_stride, WARPS);
     {
         // the frame's shared-memory plan and its warps' scratch must fit what the
         // launch has (checked once per frame; the decision is the same in every thread)
@@ -606,14 +614,14 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
         asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
         const bool fits = L.total <= (int)dyn && P.view_queue != nullptr && P.cost_scratch != nullptr &&
                           P.scratch_stride >= sweep_warp_words(K) &&
-                          (size_t)gridDim.x * kWarps * (size_t)P.scratch_stride <= P.scratch_floats;
+                          (size_t)gridDim.x * WARPS * (size_t)P.scratch_stride <= P.scratch_floats;
         if (!fits) {
             if (threadIdx.x == 0) atomicOr(err, PFD_DEVERR_SWEEP_CHECK);
             return false;
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const WarpBlock S = L.warp_block(smem, P.cost_scratch, warp, K, P.scratch_stride);
+    const WarpBlock S = L.warp_block(smem, P.cost_scratch, warp, WARPS, K, P.scratch_stride);
     float* pc = (float*)(smem + L.off_pc);
     uint32_t* ps = (uint32_t*)(smem + L.off_ps);
     int* ctl = (int*)(smem + L.off_ctl);
@@ -990,43 +998,47 @@ __device__ __forceinline__ void init_barrier(unsigned char* smem)
     __syncthreads();
 }
 
-template <bool BLUR, bool COUNT, bool SHIFT>
-__global__ void __launch_bounds__(kThreads, 4) pm_sweep_warp_kernel(FrameDev F, PmParams P, StateDev prev,
-                                                                     StateDev next, int iter, int phase, int* err)
+template <bool BLUR, bool COUNT, bool SHIFT, int SHAPE>
+__global__ void __launch_bounds__(32 * ShapeOf<SHAPE>::warps, ShapeOf<SHAPE>::min_ctas)
+pm_sweep_warp_kernel(FrameDev F, PmParams P, StateDev prev, StateDev next, int iter, int phase, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     init_barrier(smem);
     uint32_t parity = 0;
-    sweep_frame<BLUR, COUNT, SHIFT>(smem, F, P, prev, next, iter, phase, err, parity);
+    sweep_frame<BLUR, COUNT, SHIFT, ShapeOf<SHAPE>::warps>(smem, F, P, prev, next, iter, phase, err, parity);
 }
 
 // Several frames' half-sweeps in one launch, in list order: a CTA that finds a
 // frame's queue empty moves on to the next frame at once, so one frame's tail
 // overlaps the next one's start.  The dynamic shared memory is the largest of
 // the frames' plans.
-template <bool BLUR, bool SHIFT>
-__global__ void __launch_bounds__(kThreads, 4) pm_sweep_batch_kernel(const SweepItem* items, int n, int* err)
+template <bool BLUR, bool SHIFT, int SHAPE>
+__global__ void __launch_bounds__(32 * ShapeOf<SHAPE>::warps, ShapeOf<SHAPE>::min_ctas)
+pm_sweep_batch_kernel(const SweepItem* items, int n, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     init_barrier(smem);
     uint32_t parity = 0;
     for (int b = 0; b < n; ++b) {
         const SweepItem it = items[b];
-        if (!sweep_frame<BLUR, false, SHIFT>(smem, it.F, it.P, it.prev, it.next, it.iter, it.phase, err, parity))
+        if (!sweep_frame<BLUR, false, SHIFT, ShapeOf<SHAPE>::warps>(smem, it.F, it.P, it.prev, it.next, it.iter,
+                                                                    it.phase, err, parity))
             return;
     }
 }
 
-int sweep_warp_smem_bytes(const PmParams& P, bool blur)
+int sweep_shape_warps(int shape) { return kShapeWarps[(shape >= 0 && shape < kSweepShapes) ? shape : 0]; }
+
+int sweep_warp_smem_bytes(const PmParams& P, bool blur, int shape)
 {
-    return Plan::make(P.W, P.H, P.K, P.ntap, blur, P.tile_stride).total;
+    return Plan::make(P.W, P.H, P.K, P.ntap, blur, P.tile_stride, sweep_shape_warps(shape)).total;
 }
 
 int sweep_warp_stride(int K) { return sweep_warp_words(K); }
 
-size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas)
+size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas, int shape)
 {
-    return (size_t)n_ctas * kWarps * (size_t)sweep_warp_words(P.K) * 4u;
+    return (size_t)n_ctas * sweep_shape_warps(shape) * (size_t)sweep_warp_words(P.K) * 4u;
 }
 
 template <class Kern>
@@ -1037,77 +1049,103 @@ static cudaError_t launch_k(Kern k, dim3 grid, dim3 block, int smem, cudaStream_
     return cudaLaunchKernel((const void*)k, grid, block, args, (size_t)smem, st);
 }
 
-cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas)
+// The half-sweep kernel of one variant; tap counting exists in shape 0 only.
+template <int SHAPE>
+static const void* warp_kernel_of(bool blur, bool count, bool shift)
+{
+    if (count) {
+        if (shift) return blur ? (const void*)pm_sweep_warp_kernel<true, true, true, 0>
+                               : (const void*)pm_sweep_warp_kernel<false, true, true, 0>;
+        return blur ? (const void*)pm_sweep_warp_kernel<true, true, false, 0>
+                    : (const void*)pm_sweep_warp_kernel<false, true, false, 0>;
+    }
+    if (shift) return blur ? (const void*)pm_sweep_warp_kernel<true, false, true, SHAPE>
+                           : (const void*)pm_sweep_warp_kernel<false, false, true, SHAPE>;
+    return blur ? (const void*)pm_sweep_warp_kernel<true, false, false, SHAPE>
+                : (const void*)pm_sweep_warp_kernel<false, false, false, SHAPE>;
+}
+
+static const void* warp_kernel(int shape, bool blur, bool count, bool shift)
+{
+    if (count) shape = 0;
+    switch (shape) {
+    case 1: return warp_kernel_of<1>(blur, count, shift);
+    case 2: return warp_kernel_of<2>(blur, count, shift);
+    case 3: return warp_kernel_of<3>(blur, count, shift);
+    default: return warp_kernel_of<0>(blur, count, shift);
+    }
+}
+
+template <int SHAPE>
+static const void* batch_kernel_of(bool blur, bool shift)
+{
+    if (blur) return shift ? (const void*)pm_sweep_batch_kernel<true, true, SHAPE>
+                           : (const void*)pm_sweep_batch_kernel<true, false, SHAPE>;
+    return shift ? (const void*)pm_sweep_batch_kernel<false, true, SHAPE>
+                 : (const void*)pm_sweep_batch_kernel<false, false, SHAPE>;
+}
+
+static const void* batch_kernel(int shape, bool blur, bool shift)
+{
+    switch (shape) {
+    case 1: return batch_kernel_of<1>(blur, shift);
+    case 2: return batch_kernel_of<2>(blur, shift);
+    case 3: return batch_kernel_of<3>(blur, shift);
+    default: return batch_kernel_of<0>(blur, shift);
+    }
+}
+
+static cudaError_t grid_for(const void* k, int threads, int smem, int* n_ctas)
 {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int smem = sweep_warp_smem_bytes(P, blur);
-    const void* k = blur ? (const void*)pm_sweep_warp_kernel<true, false, false>
-                         : (const void*)pm_sweep_warp_kernel<false, false, false>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     *n_ctas = sms * per_sm;
     return cudaSuccess;
 }
 
+cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas, int shape)
+{
+    if (P.tap_counter) shape = 0;
+    return grid_for(warp_kernel(shape, blur, P.tap_counter != nullptr, P.shifted != 0), 32 * sweep_shape_warps(shape),
+                    sweep_warp_smem_bytes(P, blur, shape), n_ctas);
+}
+
 cudaError_t launch_sweep_warp(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
-                              int iter, int phase, int n_ctas, int* err, cudaStream_t st)
+                              int iter, int phase, int n_ctas, int* err, cudaStream_t st, int shape)
 {
     const bool blur = F.blur != nullptr;
-    const int smem = sweep_warp_smem_bytes(P, blur);
+    if (P.tap_counter) shape = 0;
+    const int smem = sweep_warp_smem_bytes(P, blur, shape);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     const int grid = std::max(1, std::min(n_ctas, F.V));
     cudaError_t qe = cudaMemsetAsync(P.view_queue, 0, sizeof(int), st);
     if (qe != cudaSuccess) return qe;
     FrameDev f = F; PmParams p = P; StateDev a = prev, b = next; int it = iter, ph = phase; int* e = err;
     void* args[] = { &f, &p, &a, &b, &it, &ph, &e };
-    if (P.tap_counter) {
-        if (P.shifted)
-            return blur ? launch_k(pm_sweep_warp_kernel<true, true, true>, grid, kThreads, smem, st, args)
-                        : launch_k(pm_sweep_warp_kernel<false, true, true>, grid, kThreads, smem, st, args);
-        return blur ? launch_k(pm_sweep_warp_kernel<true, true, false>, grid, kThreads, smem, st, args)
-                    : launch_k(pm_sweep_warp_kernel<false, true, false>, grid, kThreads, smem, st, args);
-    }
-    if (P.shifted)
-        return blur ? launch_k(pm_sweep_warp_kernel<true, false, true>, grid, kThreads, smem, st, args)
-                    : launch_k(pm_sweep_warp_kernel<false, false, true>, grid, kThreads, smem, st, args);
-    return blur ? launch_k(pm_sweep_warp_kernel<true, false, false>, grid, kThreads, smem, st, args)
-                : launch_k(pm_sweep_warp_kernel<false, false, false>, grid, kThreads, smem, st, args);
+    return launch_k(warp_kernel(shape, blur, P.tap_counter != nullptr, P.shifted != 0), grid,
+                    32 * sweep_shape_warps(shape), smem, st, args);
 }
 
-static const void* batch_kernel(bool blur, bool shift)
+cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, int* n_ctas, int shape)
 {
-    if (blur) return shift ? (const void*)pm_sweep_batch_kernel<true, true> : (const void*)pm_sweep_batch_kernel<true, false>;
-    return shift ? (const void*)pm_sweep_batch_kernel<false, true> : (const void*)pm_sweep_batch_kernel<false, false>;
-}
-
-cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, int* n_ctas)
-{
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const void* k = batch_kernel(blur, shift);
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    *n_ctas = sms * per_sm;
-    return cudaSuccess;
+    return grid_for(batch_kernel(shape, blur, shift), 32 * sweep_shape_warps(shape), smem, n_ctas);
 }
 
 cudaError_t launch_sweep_batch(const SweepItem* items, int n, bool blur, bool shift, int smem, int n_ctas, int* err,
-                               cudaStream_t st)
+                               cudaStream_t st, int shape)
 {
     if (n <= 0) return cudaSuccess;
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     const SweepItem* it = items; int nn = n; int* e = err;
     void* args[] = { &it, &nn, &e };
-    return launch_k(batch_kernel(blur, shift), dim3(std::max(1, n_ctas)), kThreads, smem, st, args);
+    return launch_k(batch_kernel(shape, blur, shift), dim3(std::max(1, n_ctas)), 32 * sweep_shape_warps(shape), smem,
+                    st, args);
 }
 
 }  // namespace pfd

@@ -1,8 +1,9 @@
-// diag.cu -- device throughput probe used for roofline denominators.
+// fma_probe.cu -- FP32 throughput probe for the roofline denominator (not
+// part of the engine): independent FFMA chains on every SM, best of three
+// timed launches after a warm-up.  bench.py loads it from tests/_build.
 #include <cuda_runtime.h>
-#include "pm_kernels.h"
 
-namespace pfd {
+namespace {
 
 // 8 independent FFMA chains per thread; the values converge to a fixed point
 // (x = 0.999 x + 0.001), so nothing overflows or goes subnormal.
@@ -22,24 +23,29 @@ __global__ void __launch_bounds__(256) fma_rate_kernel(float* out, int iters)
     if (s == 12345.0f) out[blockIdx.x] = s;   // keeps the chains alive
 }
 
-cudaError_t measure_fma_rate(cudaStream_t st, float* ms, double* flops)
+}  // namespace
+
+// Measured FFMA throughput of `device` in TFLOP/s (2 flops per FFMA).
+// Returns 0, or the CUDA error code.
+extern "C" int pfd_probe_fp32_fma_rate(int device, double* tflops)
 {
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return (int)e;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const int blocks = sms * 8, threads = 256, iters = 512;
     float* out = nullptr;
-    cudaError_t e = cudaMallocAsync((void**)&out, sizeof(float) * blocks, st);
-    if (e != cudaSuccess) return e;
+    e = cudaMalloc((void**)&out, sizeof(float) * blocks);
+    if (e != cudaSuccess) return (int)e;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     float best = 1e30f;
-    fma_rate_kernel<<<blocks, threads, 0, st>>>(out, iters);    // warm-up
+    fma_rate_kernel<<<blocks, threads>>>(out, iters);    // warm-up
     for (int r = 0; r < 3; ++r) {
-        cudaEventRecord(a, st);
-        fma_rate_kernel<<<blocks, threads, 0, st>>>(out, iters);
-        cudaEventRecord(b, st);
+        cudaEventRecord(a);
+        fma_rate_kernel<<<blocks, threads>>>(out, iters);
+        cudaEventRecord(b);
         cudaEventSynchronize(b);
         float t = 0.0f;
         cudaEventElapsedTime(&t, a, b);
@@ -48,10 +54,8 @@ cudaError_t measure_fma_rate(cudaStream_t st, float* ms, double* flops)
     e = cudaGetLastError();
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    cudaFreeAsync(out, st);
-    *ms = best;
-    *flops = 2.0 * 8.0 * 16.0 * (double)iters * (double)blocks * (double)threads;
-    return e;
+    cudaFree(out);
+    const double flops = 2.0 * 8.0 * 16.0 * (double)iters * (double)blocks * (double)threads;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return (int)e;
 }
-
-}  // namespace pfd
