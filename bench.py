@@ -478,9 +478,9 @@ def run_engine(args, rank, world, local_rank):
         result["acmm"] = acmm_leg(pfd, ctx, fid, raw_dev, stream, seed)
     ctx.frame_free(fid)
     ctx.close()
-    if result is not None and world == 1 and not args.no_serving:
-        result["batching"] = batching_leg(pfd)
-        result["serving"] = serving_leg(pfd)
+    if result is not None:
+        result["forms"] = ("batching (64 mixed frames) and serving (Poisson streams) are measured by "
+                           "python bench.py --forms; profiles/forms_mixed_frames.md")
     return result
 
 
@@ -512,140 +512,200 @@ def acmm_leg(pfd, ctx, fid, raw_dev, stream, seed, reps=3):
             "covers": "init + 10 half-sweeps + post-refine (matching only, no checks or focal stack)"}
 
 
-def mixed_requests(pfd, n_req, seed):
-    """n_req frames drawn from the mixed distribution (sizes 1024x768 /
-    2048x1536 / 4080x3068, pitches 15-30 px, 6-18 neighbours, 3-20 planes,
-    patch 11-15, 4-12 PatchMatch iterations): (workload, params, seed) each."""
+# --------------------------------------------------------------------------
+# batching and serving forms (python bench.py --forms)
+# --------------------------------------------------------------------------
+MIX = dict(sizes=((1024, 768), (2048, 1536), (4080, 3068)), pitch=(15.0, 30.0), K=(6, 18), planes=(3, 20),
+           iters=(4, 12), patches=(11, 13, 15), seed=4242)
+
+
+def mixed_frames(pfd, n, seed):
+    """n distinct seeded frames of the mixed distribution: size uniform over
+    1024x768 / 2048x1536 / 4080x3068, pitch U(15, 30) px, 6-18 neighbours, 3-20
+    planes, patch 11/13/15, 4-12 PatchMatch iterations.  (workload, params, seed) each."""
     rs = np.random.RandomState(seed)
-    shapes = [(1024, 768), (1024, 768), (2048, 1536), (2048, 1536), (4080, 3068)]
-    pool = []
-    for i, (W, H) in enumerate(shapes):
-        pitch = float(np.float32(rs.uniform(15.0, 30.0)))
-        K = int(rs.randint(6, 19))
-        planes = int(rs.randint(3, 21))
-        w = pfd.make_workload(W, H, pitch, planes, seed=100 + i, max_nb=K)
-        pool.append((w, pitch, int(rs.choice([11, 13, 15]))))
     out = []
-    for r in range(n_req):
-        idx = int(rs.choice(len(pool), p=[0.3, 0.3, 0.15, 0.15, 0.1]))
-        w, pitch, patch = pool[idx]
-        out.append((w, pfd.PmParams(base=pitch, patch_size=patch, max_iterations=int(rs.randint(4, 13))), 1000 + r))
+    for i in range(n):
+        W, H = MIX["sizes"][rs.randint(len(MIX["sizes"]))]
+        pitch = float(np.float32(rs.uniform(*MIX["pitch"])))
+        K = int(rs.randint(MIX["K"][0], MIX["K"][1] + 1))
+        planes = int(rs.randint(MIX["planes"][0], MIX["planes"][1] + 1))
+        iters = int(rs.randint(MIX["iters"][0], MIX["iters"][1] + 1))
+        patch = int(rs.choice(MIX["patches"]))
+        w = pfd.make_workload(W, H, pitch, planes, seed=seed * 1000 + i, max_nb=K)
+        out.append((w, pfd.PmParams(base=pitch, patch_size=patch, max_iterations=iters), 5000 + i))
     return out
 
 
-def batching_leg(pfd, n_frames=16, seed=7, reps=1):
-    """The batching form on resident frames of the mixed distribution: every
-    frame's PatchMatch one after another (pfd_patchmatch per frame, the plain
-    method) against pfd_patchmatch_batch (one persistent launch per
-    half-sweep over all the frames), device-timed on the context's stream;
-    the states of the two are compared bit for bit."""
+def _state_hash(st):
+    import hashlib
+    h = hashlib.sha1()
+    for a in st:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def _depth_tally(pfd, items, states):
+    """Depth error of each frame's state against its scene: pooled matched
+    fraction and fraction within 0.5 virtual depth, median of the frames'
+    median errors."""
+    meds, n_ok, w05, tot = [], 0.0, 0.0, 0
+    for (w, _, _), st in zip(items, states):
+        de = pfd.depth_error(w, st[0], cost=st[1])
+        npx = st[0].shape[0]
+        tot += npx
+        n_ok += de["matched"] * npx
+        w05 += de.get("within_0.5", 0.0) * de["matched"] * npx
+        if "median_abs" in de:
+            meds.append(de["median_abs"])
+    return {"matched": round(n_ok / tot, 4), "within_0.5": round(w05 / max(n_ok, 1.0), 4),
+            "median_abs_of_frames": round(float(np.median(meds)), 4) if meds else None}
+
+
+def batching_leg(pfd, items):
+    """The batching form on n resident frames (sizes, pitches, neighbour
+    counts, patches and iteration counts all mixed), device-timed on one
+    context's stream, every variant bit-identical per frame:
+      plain     pfd_patchmatch frame after frame, default launch shape;
+      graphs    the same from CUDA graphs (third repetition: captured, replayed);
+      batched   pfd_patchmatch_batch, one persistent launch per half-sweep over
+                all frames, autotuned launch shape (tuning in its first call);
+    and the plain GPU method, the reference's own kernels (oracle/_ref) frame
+    after frame, each frame timed on a block of 1024 of its views and scaled."""
     import torch
-    reqs = mixed_requests(pfd, n_frames, seed)
+    ref_frame = load_ref_frame()
+    out = {}
     with pfd.Context(0) as ctx:
         stream = torch.cuda.ExternalStream(ctx.stream, device="cuda:0")
         fids = [ctx.frame_upload(w.frame.raw, w.centers, w.tilekeys, w.mi, w.mi, w.nb_ids, w.nb_counts)
-                for w, _, _ in reqs]
-        params = [P for _, P, _ in reqs]
-        seeds = [sd for _, _, sd in reqs]
+                for w, _, _ in items]
+        params = [P for _, P, _ in items]
+        seeds = [sd for _, _, sd in items]
 
         def timed(fn):
-            fn()                                   # warm-up
             ctx.sync()
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            for _ in range(reps):
-                fn()
+            fn()
             b.record(stream)
             b.synchronize()
-            return a.elapsed_time(b) / reps
+            return a.elapsed_time(b)
 
         def plain():
             for fid, P, sd in zip(fids, params, seeds):
                 ctx.patchmatch(fid, P, sd)
 
-        ms_plain = timed(plain)
-        ref = [ctx.download(f) for f in fids]
-        ms_batch = timed(lambda: ctx.patchmatch_batch(fids, params, seeds))
-        same = True
-        for f, r in zip(fids, ref):
-            for x, y in zip(ctx.download(f), r):
-                same = same and bool(np.all((x == y) | (np.isnan(x) & np.isnan(y))) if x.dtype.kind == "f"
-                                     else np.array_equal(x, y))
+        out["plain_ms"] = timed(plain)
+        states = [ctx.download(f) for f in fids]
+        want = [_state_hash(st) for st in states]
+        out["depth_error"] = _depth_tally(pfd, items, states)
+        del states
+        ctx.set_graphs(True)
+        timed(plain)                                  # uncaptured
+        timed(plain)                                  # captured
+        out["graphs_ms"] = timed(plain)
+        same_g = all(_state_hash(ctx.download(f)) == h for f, h in zip(fids, want))
+        ctx.set_graphs(False)
+        ctx.set_sweep_shape(pfd.SHAPE_AUTOTUNE)
+        out["batched_first_call_ms"] = timed(lambda: ctx.patchmatch_batch(fids, params, seeds))
+        out["batched_ms"] = timed(lambda: ctx.patchmatch_batch(fids, params, seeds))
+        same_b = all(_state_hash(ctx.download(f)) == h for f, h in zip(fids, want))
+        out["tuned_shapes"] = sorted({int(ctx.tuned_sweep_shape(f, P)) for f, P in zip(fids, params)})
         for f in fids:
             ctx.frame_free(f)
-    sizes = [w.frame.raw.shape for w, _, _ in reqs]
-    return {"frames": n_frames,
-            "mix": "%d x 1024x768, %d x 2048x1536, %d x 4080x3068; 4-12 iterations" %
-                   (sum(1 for s in sizes if s[1] == 1024), sum(1 for s in sizes if s[1] == 2048),
-                    sum(1 for s in sizes if s[1] == 4080)),
-            "plain": {"ms": round(ms_plain, 1), "frames_per_s": round(1000.0 * n_frames / ms_plain, 3)},
-            "batched": {"ms": round(ms_batch, 1), "frames_per_s": round(1000.0 * n_frames / ms_batch, 3)},
-            "speedup": round(ms_plain / ms_batch, 3),
-            "covers": "PatchMatch only (init + half-sweeps), frames resident in HBM",
-            "depth_error": "identical (bit-exact per frame)" if same else "DIFFERS"}
+    # the plain GPU method: the reference's kernels, one frame at a time
+    ref_s, ref_err = 0.0, []
+    for w, P, sd in items:
+        V = w.centers.shape[0]
+        n = min(V, 1024)
+        wb = block_first(pfd, w, n)
+        with ref_frame.RefFrame(wb, philox=False) as ref:
+            ms = ref.patchmatch_sample(P, sd, n)
+            plane, cost, _, _ = ref.download()
+        ref_s += (ms[0] + ms[1]) / 1e3 * V / n
+        rows = slice(0, n * w.mi * w.mi)
+        wsub = pfd.Workload(w.frame, w.mi, wb.centers[:n], wb.tilekeys[:n], wb.nb_ids[:n], wb.nb_counts[:n],
+                            wb.gray[:n])
+        ref_err.append(pfd.depth_error(wsub, plane[rows], cost=cost[rows]).get("median_abs", np.nan))
+    n_fr = len(items)
+    counts = "/".join(str(sum(1 for w, _, _ in items if w.frame.raw.shape[1] == sz[0])) for sz in MIX["sizes"])
+    best_ms = min(out["batched_ms"], out["plain_ms"], out["graphs_ms"])
+    return {"config": "%d seeded frames, sizes uniform in 1024x768 / 2048x1536 / 4080x3068 (%s), pitch U(15, 30) px, "
+                      "6-18 neighbours, 3-20 planes, patch 11-15, 4-12 iterations; u8 pixels (exact in FP16/BF16), "
+                      "FP32 accumulation" % (n_fr, counts),
+            "plain": {"ms": round(out["plain_ms"], 1), "frames_per_s": round(1e3 * n_fr / out["plain_ms"], 3)},
+            "graphs": {"ms": round(out["graphs_ms"], 1), "frames_per_s": round(1e3 * n_fr / out["graphs_ms"], 3),
+                       "bit_identical": same_g},
+            "batched_autotuned": {"ms": round(out["batched_ms"], 1),
+                                  "frames_per_s": round(1e3 * n_fr / out["batched_ms"], 3),
+                                  "first_call_ms": round(out["batched_first_call_ms"], 1),
+                                  "shapes_chosen": out["tuned_shapes"], "bit_identical": same_b},
+            "plain_reference_gpu": {"s": round(ref_s, 1), "frames_per_s": round(n_fr / ref_s, 4),
+                                    "median_depth_error_of_frames": round(float(np.nanmedian(ref_err)), 4),
+                                    "how": "reference kernels (oracle/_ref, cuRAND, sync per launch) on 1024 views "
+                                           "of each frame, scaled by views"},
+            "depth_error": out["depth_error"],
+            "speedup_vs_plain_reference_gpu": round(ref_s * 1e3 / best_ms, 2)}
 
 
-def serving_leg(pfd, n_req=16, slots=4, seed=7):
-    """The serving form on a mixed stream (sizes 1024x768 / 2048x1536 /
-    4080x3068, pitches 15-30 px, 6-18 neighbours, 3-20 planes, 4-12 PatchMatch
-    iterations, each followed by the disparity filter): all requests arrive at
-    once, once to a server with `slots` concurrent slots and once to a
-    one-slot server (the plain method: one frame at a time, in arrival order).
-    Returns frames/s over the makespan and p50/p99 latency (submission to
-    result) for both; results are bit-identical between the two (each request
-    computes exactly what it computes alone).  The same requests are then sent
-    as a Poisson stream at 90% of the plain method's throughput, to both
-    servers, for latency under a steady arrival rate."""
+def serving_leg(pfd, items, plain_fps, window_s=60.0, slots=4, seed=7):
+    """The serving form: Poisson request streams of window_s seconds at rates
+    below and above the plain method's throughput on the mix (plain_fps), each
+    request a frame of the pool with its own 4-12 iterations and the filter,
+    sent to a server with `slots` slots and a 150 GB budget and to a one-slot
+    server (the plain method: one frame at a time).  frames/s over the makespan
+    and p50/p99 latency (submission to result) for each; every result is the
+    same bit for bit in both servers."""
     import time
-    rs = np.random.RandomState(seed)
-    shapes = [(1024, 768), (1024, 768), (2048, 1536), (2048, 1536), (4080, 3068)]
-    pool = []
-    for i, (W, H) in enumerate(shapes):
-        pitch = float(np.float32(rs.uniform(15.0, 30.0)))
-        K = int(rs.randint(6, 19))
-        planes = int(rs.randint(3, 21))
-        w = pfd.make_workload(W, H, pitch, planes, seed=100 + i, max_nb=K)
-        pool.append((w, pitch, int(rs.choice([11, 13, 15]))))
-    reqs = []
-    for r in range(n_req):
-        idx = int(rs.choice(len(pool), p=[0.3, 0.3, 0.15, 0.15, 0.1]))
-        reqs.append((idx, int(rs.randint(4, 13)), 1000 + r))
+    out = []
+    for mult in (0.5, 1.0, 2.0):
+        rate = mult * plain_fps
+        rs = np.random.RandomState(seed + int(mult * 10))
+        arrivals = []
+        t = rs.exponential(1.0 / rate)
+        while t < window_s:
+            arrivals.append(t)
+            t += rs.exponential(1.0 / rate)
+        reqs = [(int(rs.randint(len(items))), int(rs.randint(4, 13)), 9000 + i) for i in range(len(arrivals))]
 
-    def run(n_slots, arrivals=None):
-        with pfd.Server(0, hbm_budget=150 << 30, slots=n_slots) as srv:
-            t0 = time.perf_counter()
-            tickets = []
-            for r, (idx, iters, sd) in enumerate(reqs):
-                if arrivals is not None:
-                    delay = t0 + arrivals[r] - time.perf_counter()
+        def run(n_slots):
+            with pfd.Server(0, hbm_budget=150 << 30, slots=n_slots) as srv:
+                t0 = time.perf_counter()
+                tickets = []
+                for a, (idx, iters, sd) in zip(arrivals, reqs):
+                    delay = t0 + a - time.perf_counter()
                     if delay > 0:
                         time.sleep(delay)
-                w, pitch, patch = pool[idx]
-                P = pfd.PmParams(base=pitch, patch_size=patch, max_iterations=iters)
-                tickets.append(srv.submit(w, P, sd, filter_cfg=pfd.FilterCfg(), baseline_unit=pitch))
-            lat = [srv.wait(t)[4] for t in tickets]
-            span = time.perf_counter() - t0
-        return {"frames_per_s": round(len(reqs) / span, 3), "p50_ms": round(float(np.percentile(lat, 50)), 1),
-                "p99_ms": round(float(np.percentile(lat, 99)), 1), "makespan_s": round(span, 2)}
+                    w, P, _ = items[idx]
+                    Q = pfd.PmParams(base=P.base, patch_size=P.patch_size, max_iterations=iters)
+                    tickets.append(srv.submit(w, Q, sd, filter_cfg=pfd.FilterCfg(), baseline_unit=P.base))
+                res = [srv.wait(tk) for tk in tickets]
+                span = time.perf_counter() - t0
+            lat = [r[4] for r in res]
+            return ({"frames_per_s": round(len(res) / span, 3), "p50_ms": round(float(np.percentile(lat, 50)), 1),
+                     "p99_ms": round(float(np.percentile(lat, 99)), 1), "makespan_s": round(span, 1)},
+                    [_state_hash(r[:4]) for r in res])
 
-    run(slots)                                    # warm-up: contexts, pinned pool, memory pool
-    served = run(slots)
-    plain = run(1)
-    # the same requests arriving as a Poisson stream at 90% of the plain method's rate
-    rate = 0.9 * plain["frames_per_s"]
-    arrivals = np.cumsum(np.random.RandomState(seed + 1).exponential(1.0 / rate, len(reqs)))
-    served_p = run(slots, arrivals)
-    plain_p = run(1, arrivals)
-    sizes = [pool[i][0].frame.raw.shape for i, _, _ in reqs]
-    return {"requests": len(reqs), "arrival": "all at once",
-            "mix": "%d x 1024x768, %d x 2048x1536, %d x 4080x3068; 4-12 iterations, filter" %
-                   (sum(1 for s in sizes if s[1] == 1024), sum(1 for s in sizes if s[1] == 2048),
-                    sum(1 for s in sizes if s[1] == 4080)),
-            "served": dict(served, slots=slots), "plain": plain,
-            "speedup": round(served["frames_per_s"] / plain["frames_per_s"], 3),
-            "poisson": {"rate_per_s": round(rate, 3), "served": dict(served_p, slots=slots), "plain": plain_p},
-            "depth_error": "identical (bit-exact per request)"}
+        served, hs = run(slots)
+        plain, hp = run(1)
+        out.append({"rate_per_s": round(rate, 3), "requests": len(reqs), "served": dict(served, slots=slots),
+                    "plain": plain, "bit_identical": hs == hp})
+    return {"config": "Poisson streams of %.0f s from the %d-frame pool of the batching form, 4-12 iterations and the "
+                      "filter per request, 150 GB budget; rates 0.5x / 1x / 2x the plain method's throughput on the mix "
+                      "(%.3f frames/s)" % (window_s, len(items), plain_fps),
+            "streams": out}
+
+
+def run_forms(args):
+    import torch
+    torch.cuda.set_device(0)
+    pfd = load_pfd()
+    load_oracle()
+    items = mixed_frames(pfd, args.forms_frames, MIX["seed"])
+    bat = batching_leg(pfd, items)
+    srv = serving_leg(pfd, items, bat["plain"]["frames_per_s"], window_s=args.forms_window)
+    return {"forms": "batching and serving", "batching": bat, "serving": srv}
 
 
 def load_ref_frame():
@@ -790,7 +850,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-serving", action="store_true", help="skip the serving-form measurement")
+    ap.add_argument("--forms", action="store_true", help="measure the batching and serving forms instead")
+    ap.add_argument("--forms-frames", type=int, default=64)
+    ap.add_argument("--forms-window", type=float, default=60.0)
     ap.add_argument("--frame", default=None, help="WxH override (profiling captures of a smaller frame)")
     ap.add_argument("--iterations", type=int, default=None, help="PatchMatch iterations override (profiling)")
     args = ap.parse_args()
@@ -802,6 +864,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.forms:
+        print(json.dumps(run_forms(args)), flush=True)
+        return
     if args.impl == "reference":
         res = run_reference(args, rank, world)
         if res is not None:

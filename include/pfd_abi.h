@@ -176,6 +176,17 @@ pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* param
  * alone.  Tap counting (pfd_set_tap_counting) runs the frames one by one. */
 pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const pfd_pm_params* params,
                                 const uint64_t* seeds);
+/* CUDA graphs for the context's later pfd_patchmatch calls and enqueue-only
+ * pfd_filter calls (reason and stats NULL); no counterpart in the reference,
+ * which launches and synchronises kernel by kernel.  Per frame, the first call
+ * with a given key (the call's arguments and the context's matcher, moment
+ * mode and sweep shape) runs as usual, which sizes the scratch and tunes the
+ * launch shape; the second is captured into a graph; later calls replay it.
+ * A graph reads and writes the frame's buffers in place, so new raw data and
+ * new neighbour lists are picked up; a new key, new neighbour lists (for the
+ * filter) or moved sweep scratch make the next call run uncaptured again.
+ * Results are the same bit for bit with graphs on or off. */
+pfd_status pfd_set_graphs(pfd_ctx* ctx, int on);
 /* The steps of pfd_patchmatch, separately: RandomInitializationForFrame
  * (AdaptMIPMFrame.cu:474-518) and one CheckerboardUpdateFrame launch (:520-947). */
 pfd_status pfd_pm_init(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed);

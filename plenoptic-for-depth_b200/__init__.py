@@ -238,6 +238,7 @@ def lib() -> ctypes.CDLL:
             "pfd_select_neighbors": [_P, _P, _P, _I, _I, _I, _F, _P, _I, _I, _I, _P, _P],
             "pfd_frame_select_neighbors": [_P, _I, _I, _I, _F, _I, _P, _P],
             "pfd_set_sweep_shape": [_P, _I],
+            "pfd_set_graphs": [_P, _I],
             "pfd_sweep_shape_info": [_I, _P, _P],
             "pfd_tuned_sweep_shape": [_P, _I, _P, _P],
             "pfd_mla_centers": [_P, _P, _I, _I, _I, _F, _I, _I, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
@@ -492,6 +493,11 @@ class Context:
         sd = np.ascontiguousarray(seeds, np.uint64)
         self._check(self._L.pfd_patchmatch_batch(self._h, _ptr(ids), len(ids), ctypes.cast(arr, _P), _ptr(sd)),
                     "pfd_patchmatch_batch")
+
+    def set_graphs(self, on: bool) -> None:
+        """Replay pfd_patchmatch and enqueue-only filter calls from CUDA graphs
+        (captured on the second call with the same arguments)."""
+        self._check(self._L.pfd_set_graphs(self._h, 1 if on else 0), "pfd_set_graphs")
 
     def set_sweep_shape(self, shape: int) -> None:
         """Launch shape of later half-sweeps: 0 .. SWEEP_SHAPES - 1, or

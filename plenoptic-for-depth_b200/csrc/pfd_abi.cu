@@ -28,6 +28,28 @@
 
 namespace {
 
+// A launch sequence of one frame replayed from a CUDA graph: the key of the
+// call it was captured from, and the frame's host-side bookkeeping as the
+// sequence leaves it (restored after each replay).
+struct FrameGraph {
+    std::vector<unsigned char> key;   // the call's arguments and the context modes; empty = none
+    bool warm = false;                // one call with this key ran uncaptured (allocations, tuning done)
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches = 0;  // kernels in the graph
+    unsigned scratch_gen = 0;         // the context's scratch generation at capture
+    int cur = 0;
+    unsigned cvec_valid = 0;
+    pfd_pm_params cvec_key = {};
+    int cvec_mode = 0;
+    void reset()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+        warm = false;
+    }
+};
+
 struct Frame {
     int W = 0, H = 0;                 // raw frame
     int V = 0, mi_w = 0, mi_h = 0, K = 0, tile_stride = 0;
@@ -73,6 +95,9 @@ struct Frame {
     float* d_slice_vd = nullptr;               // refocus: slice virtual depths [kMaxSlices]
     float* d_stack = nullptr;                  // refocus: focal stack
     size_t stack_bytes = 0;
+    unsigned long long* d_fstats = nullptr;    // filter counters, allocated on first use
+    // CUDA graphs of the enqueue-only PatchMatch and filter (pfd_set_graphs)
+    FrameGraph pm_graph, filter_graph;
 };
 
 }  // namespace
@@ -93,6 +118,8 @@ struct pfd_ctx {
     float* d_scratch = nullptr;             // sweep candidate costs, per resident CTA
     size_t scratch_bytes = 0;
     int sweep_shape = 0;                    // launch shape of the half-sweeps, or PFD_SHAPE_AUTOTUNE
+    bool graphs = false;                    // replay pfd_patchmatch / pfd_filter from CUDA graphs
+    unsigned scratch_gen = 0;               // bumped whenever d_scratch moves (graphs hold its address)
     std::string last_error;
 };
 
@@ -162,6 +189,8 @@ void frame_free_one(pfd_ctx* ctx, Frame& f, void* p, size_t bytes)
 
 void frame_release(Frame& f, cudaStream_t s)
 {
+    f.pm_graph.reset();
+    f.filter_graph.reset();
     for (void* p : f.allocs) cudaFreeAsync(p, s);
     f.allocs.clear();
     f.bytes = 0;
@@ -711,6 +740,7 @@ static pfd_status ensure_scratch(pfd_ctx* ctx, size_t need)
     ctx->used -= ctx->scratch_bytes;
     ctx->d_scratch = nullptr;
     ctx->scratch_bytes = 0;
+    ++ctx->scratch_gen;
     if (cudaMallocAsync((void**)&ctx->d_scratch, need, ctx->stream) != cudaSuccess) {
         cudaGetLastError();
         return fail(ctx, PFD_ENOMEM, "cudaMallocAsync(%zu) for sweep scratch failed", need);
@@ -897,13 +927,79 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
     return PFD_OK;
 }
 
-pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed)
+static pfd_status patchmatch_enqueue(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed)
 {
     pfd_status st = pfd_pm_init(ctx, frame_id, params, seed);
     for (int it = 0; st == PFD_OK && it < params->max_iterations; ++it)
         for (int ph = 0; ph < 2 && st == PFD_OK; ++ph) st = pfd_pm_sweep(ctx, frame_id, params, seed, it, ph);
     if (st == PFD_OK && ctx->matcher == PFD_MATCHER_ACMM) st = pfd_acmm_post_refine(ctx, frame_id, params);
     return st;
+}
+
+pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, uint64_t seed)
+{
+    if (!ctx) return PFD_EINVAL;
+    Frame* f = find_frame(ctx, frame_id);
+    if (!f) return fail(ctx, PFD_ENOFRAME, "no frame %d", frame_id);
+    if (!ctx->graphs || ctx->counting) return patchmatch_enqueue(ctx, frame_id, params, seed);
+    pfd_status st = check_params(ctx, *f, params);
+    if (st != PFD_OK) return st;
+    // the key: the call's arguments and every context mode the launches depend on
+    std::vector<unsigned char> key(sizeof(pfd_pm_params) + sizeof(uint64_t) + 4 * sizeof(int));
+    const int modes[4] = { ctx->matcher, ctx->ncc_moments, ctx->sweep_shape, 0 };
+    std::memcpy(key.data(), params, sizeof(pfd_pm_params));
+    std::memcpy(key.data() + sizeof(pfd_pm_params), &seed, sizeof(uint64_t));
+    std::memcpy(key.data() + sizeof(pfd_pm_params) + sizeof(uint64_t), modes, sizeof(modes));
+    FrameGraph& G = f->pm_graph;
+    DeviceGuard g(ctx->device);
+    if (G.exec && G.scratch_gen != ctx->scratch_gen) G.reset();   // the scratch moved since the capture
+    if (G.exec && G.key == key) {
+        CU(cudaGraphLaunch(G.exec, ctx->stream));
+        ctx->launches += G.launches;
+    } else if (G.warm && G.key == key) {
+        // the first call ran uncaptured (scratch sized, launch shape tuned): capture
+        // this one's enqueue sequence, then replay it
+        const unsigned long long launches0 = ctx->launches;
+        CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        st = patchmatch_enqueue(ctx, frame_id, params, seed);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if (st == PFD_OK && (ce != cudaSuccess || cudaGraphInstantiate(&G.exec, graph, 0) != cudaSuccess)) {
+            cudaGetLastError();
+            st = fail(ctx, PFD_ECUDA, "patchmatch: graph capture failed");
+        }
+        if (graph) cudaGraphDestroy(graph);
+        if (st != PFD_OK) { G.reset(); return st; }
+        G.launches = ctx->launches - launches0;
+        ctx->launches = launches0;
+        G.scratch_gen = ctx->scratch_gen;
+        G.cur = f->cur;
+        G.cvec_valid = f->cvec_valid;
+        G.cvec_key = f->cvec_key;
+        G.cvec_mode = f->cvec_mode;
+        CU(cudaGraphLaunch(G.exec, ctx->stream));
+        ctx->launches += G.launches;
+    } else {
+        G.reset();
+        st = patchmatch_enqueue(ctx, frame_id, params, seed);
+        if (st != PFD_OK) return st;
+        G.key = key;
+        G.warm = true;
+        return PFD_OK;
+    }
+    f->has_state = true;
+    f->cur = G.cur;
+    f->cvec_valid = G.cvec_valid;
+    f->cvec_key = G.cvec_key;
+    f->cvec_mode = G.cvec_mode;
+    return PFD_OK;
+}
+
+pfd_status pfd_set_graphs(pfd_ctx* ctx, int on)
+{
+    if (!ctx) return PFD_EINVAL;
+    ctx->graphs = on != 0;
+    return PFD_OK;
 }
 
 pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const pfd_pm_params* params,
@@ -1238,21 +1334,66 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
     std::memcpy(&fc, cfg, sizeof(fc));
     const pfd::CheckFrame F = check_frame(*f, baseline_unit);
     if (pfd::filter_smem_bytes(F) > 227 * 1024) return fail(ctx, PFD_EINVAL, "filter tile does not fit shared memory");
-    unsigned long long* d_stats = nullptr;
-    CU(cudaMallocAsync((void**)&d_stats, 8 * sizeof(unsigned long long), ctx->stream));
-    CU(cudaMemsetAsync(d_stats, 0, 8 * sizeof(unsigned long long), ctx->stream));
+    if (!f->d_fstats) {
+        void* p = nullptr;
+        if ((st = frame_alloc(ctx, *f, &p, 8 * sizeof(unsigned long long))) != PFD_OK) return st;
+        f->d_fstats = (unsigned long long*)p;
+    }
+    unsigned long long* d_stats = f->d_fstats;
+    // enqueue-only calls under pfd_set_graphs: the first call with a key runs as
+    // usual, the second is captured, later ones replay the graph (it reads the
+    // state buffer the frame's current state was in at capture)
+    FrameGraph& G = f->filter_graph;
+    const bool graph_mode = !stats && !reason && ctx->graphs;
+    bool capture = false;
+    if (graph_mode) {
+        std::vector<unsigned char> key(sizeof(pfd_filter_cfg) + sizeof(float));
+        std::memcpy(key.data(), cfg, sizeof(pfd_filter_cfg));
+        std::memcpy(key.data() + sizeof(pfd_filter_cfg), &baseline_unit, sizeof(float));
+        if (G.exec && G.key == key && G.cur == f->cur) {
+            CU(cudaGraphLaunch(G.exec, ctx->stream));
+            ctx->launches += G.launches;
+            f->cvec_valid = 0;
+            return PFD_OK;
+        }
+        capture = G.warm && !G.exec && G.key == key && G.cur == f->cur;
+        if (!capture) {
+            G.reset();
+            G.key = key;
+            G.warm = true;
+            G.cur = f->cur;
+        }
+    }
+    if (capture) CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const unsigned long long launches0 = ctx->launches;
+    pfd_status fst = PFD_OK;
+    if (cudaMemsetAsync(d_stats, 0, 8 * sizeof(unsigned long long), ctx->stream) != cudaSuccess)
+        fst = fail(ctx, PFD_ECUDA, "filter: counter reset");
     const pfd::StateDev& S = f->s[f->cur];
     f->cvec_valid = 0;                             // rejected pixels get new planes
-    for (size_t s = 0; s + 1 < f->step_start.size(); ++s) {
+    for (size_t s = 0; fst == PFD_OK && s + 1 < f->step_start.size(); ++s) {
         const int a = f->step_start[s], b = f->step_start[s + 1];
         cudaError_t e = pfd::launch_filter_step(F, fc, S, f->d_steps + a, b - a, f->d_reason, d_stats, ctx->stream);
-        if (e != cudaSuccess) { cudaFreeAsync(d_stats, ctx->stream); return fail(ctx, PFD_ECUDA, "filter step: %s", cudaGetErrorString(e)); }
-        ctx->launches += 1;
+        if (e != cudaSuccess) fst = fail(ctx, PFD_ECUDA, "filter step: %s", cudaGetErrorString(e));
+        else ctx->launches += 1;
     }
+    if (capture) {
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if (fst == PFD_OK && (ce != cudaSuccess || cudaGraphInstantiate(&G.exec, graph, 0) != cudaSuccess)) {
+            cudaGetLastError();
+            fst = fail(ctx, PFD_ECUDA, "filter: graph capture failed");
+        }
+        if (graph) cudaGraphDestroy(graph);
+        if (fst != PFD_OK) { G.reset(); return fst; }
+        G.launches = ctx->launches - launches0;
+        CU(cudaGraphLaunch(G.exec, ctx->stream));
+        return PFD_OK;
+    }
+    if (fst != PFD_OK) return fst;
     unsigned long long h[8] = {};
     if (stats) CU(cudaMemcpyAsync(h, d_stats, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
     if (reason) CU(cudaMemcpyAsync(reason, f->d_reason, px, cudaMemcpyDeviceToHost, ctx->stream));
-    cudaFreeAsync(d_stats, ctx->stream);
     if (stats || reason) {
         CU(cudaStreamSynchronize(ctx->stream));
         if (stats) for (int i = 0; i < 8; ++i) stats[i] = (long long)h[i];
@@ -1913,6 +2054,7 @@ pfd_status pfd_frame_select_neighbors(pfd_ctx* ctx, int frame_id, int mla_u_size
     f->has_state = false;
     f->cvec_valid = 0;
     f->step_start.clear();
+    f->filter_graph.reset();          // its launches follow the old lists' schedule
     return PFD_OK;
 }
 
