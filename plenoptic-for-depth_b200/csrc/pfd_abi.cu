@@ -81,8 +81,9 @@ struct Frame {
     std::vector<int> h_keys, h_nb_ids, h_nb_counts;
     uint8_t* d_reason = nullptr;      // filter reject reasons, allocated on first use
     float* d_err = nullptr;           // reprojection-error map, allocated on first use
-    int* d_steps = nullptr;           // views grouped by wavefront step
-    std::vector<int> step_start;      // [n_steps + 1] offsets into d_steps
+    int* d_order = nullptr;           // filter: views in key order (row, column), then each view's rank
+    int* d_rank = nullptr;
+    int* d_done = nullptr;            // filter: a done flag per view
     pfd::CycleTileRec* d_cyc_recs = nullptr;   // cycle check: per-view sums, allocated on first use
     unsigned int* d_cyc_hist = nullptr;        // cycle check: masked geometric-error histogram
     float* d_cyc_maps = nullptr;               // cycle check: geo and photo error maps
@@ -300,6 +301,8 @@ pfd_status check_device_error(pfd_ctx* ctx)
         if (h == PFD_DEVERR_REFOCUS_LENSES)
             return fail(ctx, PFD_EINVAL, "refocus: more than %d lenses reach one output tile (slice virtual depth "
                         "too large for this lens density)", pfd::kMaxRefocusCand);
+        if (h & PFD_DEVERR_FILTER_TIMEOUT)
+            return fail(ctx, PFD_ETIMEDOUT, "filter: a wait for an earlier micro-image ran out (flags 0x%x)", h);
         if (h & PFD_DEVERR_SWEEP_CHECK)
             return fail(ctx, PFD_ECUDA, "sweep launch refused its work: shared-memory plan, scratch or neighbour "
                         "ids out of range (flags 0x%x)", h);
@@ -1261,54 +1264,32 @@ static pfd_status check_filter_cfg(pfd_ctx* ctx, const pfd_filter_cfg* cfg, floa
     return PFD_OK;
 }
 
-// Groups the views into wavefront steps col + c * row such that every
-// neighbour that precedes a view in key order (row, col) lands in an earlier
-// step and every one that follows it in a later step.
-static pfd_status build_steps(pfd_ctx* ctx, Frame& f)
+// The filter's order (FilterGlobal walks the views in key order, row then
+// column, MIDisparityFilter.cpp:962-986): the views sorted by key, each view's
+// position, and the per-view done flags; made once per frame (keys do not change).
+static pfd_status build_order(pfd_ctx* ctx, Frame& f)
 {
-    if (!f.step_start.empty()) return PFD_OK;
+    if (f.d_order) return PFD_OK;
     const int V = f.V;
-    long long c = 1;
-    for (int v = 0; v < V; ++v) {
-        const int cv = f.h_keys[2 * v], rv = f.h_keys[2 * v + 1];
-        for (int k = 0; k < f.h_nb_counts[v]; ++k) {
-            const int u = f.h_nb_ids[(size_t)v * f.K + k];
-            if (u < 0) continue;
-            const int cu = f.h_keys[2 * u], ru = f.h_keys[2 * u + 1];
-            if (ru == rv) continue;
-            // earlier row: c (rv - ru) > cu - cv; later row: c (ru - rv) > cv - cu
-            const long long num = (ru < rv) ? (long long)cu - cv : (long long)cv - cu;
-            const long long den = (ru < rv) ? (long long)rv - ru : (long long)ru - rv;
-            long long need = (num >= 0) ? num / den + 1 : 1;
-            if (need > c) c = need;
-        }
-    }
-    std::vector<long long> step(V);
-    long long smin = LLONG_MAX, smax = LLONG_MIN;
-    for (int v = 0; v < V; ++v) {
-        step[v] = (long long)f.h_keys[2 * v] + c * (long long)f.h_keys[2 * v + 1];
-        smin = std::min(smin, step[v]);
-        smax = std::max(smax, step[v]);
-    }
-    const long long ns = smax - smin + 1;
-    if (ns > 100000000LL) return fail(ctx, PFD_EINVAL, "tile keys too sparse for the filter schedule");
-    std::vector<int> counts((size_t)ns + 1, 0), order(V);
-    for (int v = 0; v < V; ++v) counts[(size_t)(step[v] - smin) + 1]++;
-    for (size_t i = 1; i < counts.size(); ++i) counts[i] += counts[i - 1];
-    std::vector<int> fill(counts.begin(), counts.end() - 1);
-    for (int v = 0; v < V; ++v) order[fill[(size_t)(step[v] - smin)]++] = v;
-    // compact away empty steps
-    f.step_start.clear();
-    for (size_t s = 0; s + 1 < counts.size(); ++s)
-        if (counts[s + 1] > counts[s]) f.step_start.push_back(counts[s]);
-    f.step_start.push_back(V);
-    if (!f.d_steps) {                 // kept when new neighbour lists rebuild the schedule
-        void* p = nullptr;
-        pfd_status st = frame_alloc(ctx, f, &p, sizeof(int) * (size_t)V);
-        if (st != PFD_OK) { f.step_start.clear(); return st; }
-        f.d_steps = (int*)p;
-    }
-    CU(cudaMemcpyAsync(f.d_steps, order.data(), sizeof(int) * (size_t)V, cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<int> order(V), rank(V);
+    for (int v = 0; v < V; ++v) order[v] = v;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const int ra = f.h_keys[2 * a + 1], rb = f.h_keys[2 * b + 1];
+        return ra != rb ? ra < rb : f.h_keys[2 * a] < f.h_keys[2 * b];
+    });
+    for (int i = 0; i < V; ++i) rank[order[i]] = i;
+    void* p = nullptr;
+    pfd_status st = frame_alloc(ctx, f, &p, sizeof(int) * 3 * (size_t)V);
+    if (st != PFD_OK) return st;
+    int* d = (int*)p;
+    std::vector<int> both(2 * (size_t)V);
+    std::copy(order.begin(), order.end(), both.begin());
+    std::copy(rank.begin(), rank.end(), both.begin() + V);
+    CU(cudaMemcpyAsync(d, both.data(), sizeof(int) * 2 * (size_t)V, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));      // the staging vector dies on return
+    f.d_order = d;
+    f.d_rank = d + V;
+    f.d_done = d + 2 * V;
     return PFD_OK;
 }
 
@@ -1322,7 +1303,7 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
     if (st != PFD_OK) return st;
     if (!f->has_state) return fail(ctx, PFD_ESTATE, "filter before PatchMatch");
     DeviceGuard g(ctx->device);
-    if ((st = build_steps(ctx, *f)) != PFD_OK) return st;
+    if ((st = build_order(ctx, *f)) != PFD_OK) return st;
     const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
     if (!f->d_reason) {
         void* p = nullptr;
@@ -1354,6 +1335,7 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
             CU(cudaGraphLaunch(G.exec, ctx->stream));
             ctx->launches += G.launches;
             f->cvec_valid = 0;
+            f->cur ^= 1;                               // the filtered state is in the other buffer
             return PFD_OK;
         }
         capture = G.warm && !G.exec && G.key == key && G.cur == f->cur;
@@ -1369,14 +1351,15 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
     pfd_status fst = PFD_OK;
     if (cudaMemsetAsync(d_stats, 0, 8 * sizeof(unsigned long long), ctx->stream) != cudaSuccess)
         fst = fail(ctx, PFD_ECUDA, "filter: counter reset");
-    const pfd::StateDev& S = f->s[f->cur];
     f->cvec_valid = 0;                             // rejected pixels get new planes
-    for (size_t s = 0; fst == PFD_OK && s + 1 < f->step_start.size(); ++s) {
-        const int a = f->step_start[s], b = f->step_start[s + 1];
-        cudaError_t e = pfd::launch_filter_step(F, fc, S, f->d_steps + a, b - a, f->d_reason, d_stats, ctx->stream);
-        if (e != cudaSuccess) fst = fail(ctx, PFD_ECUDA, "filter step: %s", cudaGetErrorString(e));
+    if (fst == PFD_OK) {
+        const pfd::FilterFlow fl{ f->d_order, f->d_rank, f->d_done, ctx->d_vq, ctx->d_err };
+        const cudaError_t e = pfd::launch_filter(F, fc, f->s[f->cur], f->s[f->cur ^ 1], fl, f->d_reason, d_stats,
+                                                 ctx->stream);
+        if (e != cudaSuccess) fst = fail(ctx, PFD_ECUDA, "filter: %s", cudaGetErrorString(e));
         else ctx->launches += 1;
     }
+    if (fst == PFD_OK) f->cur ^= 1;               // the filtered state is in the other buffer
     if (capture) {
         cudaGraph_t graph = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
@@ -2053,8 +2036,7 @@ pfd_status pfd_frame_select_neighbors(pfd_ctx* ctx, int frame_id, int mla_u_size
     // old lists
     f->has_state = false;
     f->cvec_valid = 0;
-    f->step_start.clear();
-    f->filter_graph.reset();          // its launches follow the old lists' schedule
+    f->filter_graph.reset();
     return PFD_OK;
 }
 

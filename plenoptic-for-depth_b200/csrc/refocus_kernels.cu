@@ -104,6 +104,9 @@ __global__ void __launch_bounds__(kThreads) pm_refocus_kernel(RefocusFrame F, co
         for (int t = 0; t < nc; ++t) {
             const float2 c = cc[t];
             const uint8_t* T = tiles + (size_t)t * F.tile_stride;
+            // the column coordinates do not depend on the row: one division per column
+            float ua[2];
+            for (int a = 0; a < 2; ++a) ua[a] = __fadd_rn(__fdiv_rn(__fsub_rn(Xa[a], c.x), v), cmx);
             for (int b = 0; b < 2; ++b) {
                 const float w = __fadd_rn(__fdiv_rn(__fsub_rn(Yb[b], c.y), v), cmy);   // warp-uniform
                 if (!(w >= 0.0f && w <= wmax)) continue;
@@ -111,7 +114,7 @@ __global__ void __launch_bounds__(kThreads) pm_refocus_kernel(RefocusFrame F, co
                 const int y1 = min(y0 + 1, mh - 1);
                 const float ay = __fsub_rn(w, (float)y0);
                 for (int a = 0; a < 2; ++a) {
-                    const float u = __fadd_rn(__fdiv_rn(__fsub_rn(Xa[a], c.x), v), cmx);
+                    const float u = ua[a];
                     if (!(u >= 0.0f && u <= umax)) continue;
                     const int x0 = (int)floorf(u);
                     const int x1 = min(x0 + 1, m - 1);
