@@ -1,7 +1,8 @@
 /*
  * oracle/patchmatch.c -- CPU restatement of the reference's whole-frame
  * plane-hypothesis PatchMatch (AdaptMIPMFrame).  TEST INFRASTRUCTURE ONLY;
- * see pfd_oracle.h for who may call it and why parity is unpinned.
+ * see pfd_oracle.h for who may call it and how it is pinned to the
+ * reference's own kernels.
  *
  * Structure and order of operations follow the reference line by line:
  *   MIStereo/AdaptMIPMFrame.cu:24-947, MIStereo/CudaUtil.cu:13-170,341-361,491-507,

@@ -5,13 +5,19 @@
  * baseline legs of bench.py load this library, and only to check or time the
  * reference algorithm; the product library never links it.
  *
- * PARITY UNPINNED: the reference (fengyunxuan6/plenoptic-for-depth) ships no
- * tests, fixtures or golden vectors, and it cannot be built here (it needs the
- * OpenCV C++ SDK, Eigen, Boost, libpleno, yaml-cpp and libv, none of which is
- * installed), so nothing the reference itself computed pins this restatement.
- * What pins it instead: known-answer tests (fronto-parallel scenes, shifted
- * copies), an FP64 cross-check, and a device test comparing the texture
- * emulation with tex2D on a B200.
+ * Pins.  The reference (fengyunxuan6/plenoptic-for-depth) ships no tests,
+ * fixtures or golden vectors.  The PatchMatch restatement (patchmatch.c) is
+ * pinned to the reference's own frame kernels, compiled from its sources in
+ * oracle/ref and run beside the engine on the same hypotheses and the same
+ * random streams (tests/test_gpu_refpin.py): the two differ only by the
+ * reference's fast-math arithmetic, by as much as the reference's own IEEE
+ * build differs from it.  The host-side stages (checks.c, fuse.c, vdrd.c,
+ * select.cpp, mla.cpp, blur.c) restate reference code that needs the OpenCV
+ * C++ SDK, Eigen, Boost, libpleno, yaml-cpp and libv, none of which is
+ * installed, so it cannot run here: their parity with the reference is
+ * unpinned, and they are pinned to OpenCV (cv2) on the OpenCV arithmetic they
+ * call, to known answers and to an FP64 cross-check; refocus.c has no
+ * reference counterpart.  The texture emulation is pinned to tex2D on a B200.
  *
  * Every function cites the reference lines it restates.  Arithmetic follows
  * oracle/canon.h.

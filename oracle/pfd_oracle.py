@@ -1,8 +1,9 @@
 """ctypes binding of the CPU oracle (oracle/_build/liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline legs of bench.py, never by the product.  PARITY UNPINNED: see
-oracle/pfd_oracle.h.
+baseline legs of bench.py, never by the product.  What pins it (the
+reference's own kernels for the PatchMatch, OpenCV and known answers for the
+host-side stages): see oracle/pfd_oracle.h.
 """
 from __future__ import annotations
 
