@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <tuple>
 #include <new>
@@ -27,6 +28,35 @@
 #include "blur_kernels.h"
 
 namespace {
+
+// SelectNeighbors' candidate rings of every view, which depend on the lens
+// geometry only (ComputeNearestCircleKeys, SelectNeighbors.cpp:195-365), and
+// the (view, candidate) pairs whose similarities the device computes.
+struct RingPlan {
+    int u = 0, v = 0;
+    float pitch = 0.0f;
+    pfd::LensGrid G;
+    std::vector<std::vector<std::vector<int>>> R;
+    std::vector<int2> pairs;
+    std::vector<size_t> first;       // [view * 5 + ring] offset into pairs
+    bool build(const float* centers, const int* keys, int n, int u_size, int v_size, float p)
+    {
+        if (!G.build(centers, keys, n, u_size, v_size)) return false;
+        u = u_size;
+        v = v_size;
+        pitch = p;
+        pfd::collect_rings(G, pitch, 5, R);
+        pairs.clear();
+        first.assign((size_t)n * 5 + 1, 0);
+        for (int i = 0; i < n; ++i)
+            for (int k = 0; k < 5; ++k) {
+                first[(size_t)i * 5 + k] = pairs.size();
+                for (int m : R[i][k]) pairs.push_back(make_int2(i, m));
+            }
+        first[(size_t)n * 5] = pairs.size();
+        return true;
+    }
+};
 
 // A launch sequence of one frame replayed from a CUDA graph: the key of the
 // call it was captured from, and the frame's host-side bookkeeping as the
@@ -97,6 +127,11 @@ struct Frame {
     float* d_stack = nullptr;                  // refocus: focal stack
     size_t stack_bytes = 0;
     unsigned long long* d_fstats = nullptr;    // filter counters, allocated on first use
+    // neighbour selection: the rings of the frame's lens grid, kept for the next call
+    std::shared_ptr<RingPlan> rings;
+    int2* d_pairs = nullptr;                   // rings->pairs on the device
+    int* d_sims = nullptr;                     // their similarities
+    size_t n_pairs_alloc = 0;                  // entries d_pairs and d_sims hold
     // CUDA graphs of the enqueue-only PatchMatch and filter (pfd_set_graphs)
     FrameGraph pm_graph, filter_graph;
 };
@@ -1912,35 +1947,34 @@ pfd_status pfd_fuse_virtual_depth(pfd_ctx* ctx, int frame_id, const pfd_fuse_par
 // apart) and the centres on the host and the device: every ring candidate's
 // similarity on the device, then the per-view ring walk, RANSAC, stop rule and
 // sort on the host threads.  out_ids [n][max_nb], out_counts [n].
-static pfd_status select_lists(pfd_ctx* ctx, const pfd::LensGrid& G, float pitch, const uint8_t* d_img,
-                               int tile_stride, int mi_w, int mi_h, const float2* d_c, int max_nb, int* out_ids,
-                               int* out_counts)
+// The selection given the rings and the micro-images on the device (tiles
+// tile_stride bytes apart): every ring candidate's similarity on the device,
+// then the per-view RANSAC, stop rule and sort on the host threads.  d_pairs /
+// d_out: the plan's pairs already on the device and room for their
+// similarities, or NULL to use temporary buffers.  out_ids [n][max_nb],
+// out_counts [n].
+static pfd_status select_lists(pfd_ctx* ctx, const RingPlan& rp, const int2* d_pairs, int* d_out,
+                               const uint8_t* d_img, int tile_stride, int mi_w, int mi_h, const float2* d_c,
+                               int max_nb, int* out_ids, int* out_counts)
 {
-    const int n_views = G.V;
-    std::vector<std::vector<std::vector<int>>> R;
-    pfd::collect_rings(G, pitch, 5, R);
-    // every candidate of every ring: the search may stop early, the similarities are cheap
-    std::vector<int2> pairs;
-    std::vector<size_t> first((size_t)n_views * 5 + 1, 0);
-    for (int v = 0; v < n_views; ++v)
-        for (int k = 0; k < 5; ++k) {
-            first[(size_t)v * 5 + k] = pairs.size();
-            for (int n : R[v][k]) pairs.push_back(make_int2(v, n));
-        }
-    first[(size_t)n_views * 5] = pairs.size();
+    const int n_views = rp.G.V;
     cudaStream_t s = ctx->stream;
-    std::vector<int> sims(pairs.size());
-    int2* d_pairs = nullptr;
-    int* d_out = nullptr;
-    cudaError_t e = cudaMallocAsync((void**)&d_pairs, sizeof(int2) * std::max<size_t>(pairs.size(), 1), s);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_out, sizeof(int) * std::max<size_t>(pairs.size(), 1), s);
-    if (e == cudaSuccess && !pairs.empty())
-        e = cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = pfd::launch_similarity(d_img, tile_stride, mi_w, mi_h, d_c, d_pairs, (int)pairs.size(), d_out, s);
-    if (e == cudaSuccess && !pairs.empty())
-        e = cudaMemcpyAsync(sims.data(), d_out, sizeof(int) * pairs.size(), cudaMemcpyDeviceToHost, s);
-    for (void* q : { (void*)d_pairs, (void*)d_out })
+    const size_t np = rp.pairs.size();
+    std::vector<int> sims(np);
+    int2* tp = nullptr;
+    int* to = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (!d_pairs) {
+        e = cudaMallocAsync((void**)&tp, sizeof(int2) * std::max<size_t>(np, 1), s);
+        if (e == cudaSuccess) e = cudaMallocAsync((void**)&to, sizeof(int) * std::max<size_t>(np, 1), s);
+        if (e == cudaSuccess && np)
+            e = cudaMemcpyAsync(tp, rp.pairs.data(), sizeof(int2) * np, cudaMemcpyHostToDevice, s);
+        d_pairs = tp;
+        d_out = to;
+    }
+    if (e == cudaSuccess) e = pfd::launch_similarity(d_img, tile_stride, mi_w, mi_h, d_c, d_pairs, (int)np, d_out, s);
+    if (e == cudaSuccess && np) e = cudaMemcpyAsync(sims.data(), d_out, sizeof(int) * np, cudaMemcpyDeviceToHost, s);
+    for (void* q : { (void*)tp, (void*)to })
         if (q) cudaFreeAsync(q, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
@@ -1951,8 +1985,8 @@ static pfd_status select_lists(pfd_ctx* ctx, const pfd::LensGrid& G, float pitch
     pfd::parallel_views(n_views, [&](int a, int b) {
         std::vector<int> list;
         for (int v = a; v < b; ++v) {
-            auto sim = [&](int ring, int i) { return (float)(double)sims[first[(size_t)v * 5 + ring] + i]; };
-            pfd::select_for_view(G, pitch, v, R[v], sim, list);
+            auto sim = [&](int ring, int i) { return (float)(double)sims[rp.first[(size_t)v * 5 + ring] + i]; };
+            pfd::select_for_view(rp.G, rp.pitch, v, rp.R[v], sim, list);
             const int n = std::min((int)list.size(), max_nb);
             for (int k = 0; k < max_nb; ++k) out_ids[(size_t)v * max_nb + k] = k < n ? list[k] : -1;
             out_counts[v] = n;
@@ -1972,8 +2006,8 @@ pfd_status pfd_select_neighbors(pfd_ctx* ctx, const float* centers, const int* t
         return fail(ctx, PFD_EINVAL, "select_neighbors: bad pitch, window or max_nb");
     if (mla_u_size < 1 || mla_v_size < 1 || (long long)mla_u_size * mla_v_size > (1LL << 28))
         return fail(ctx, PFD_EINVAL, "select_neighbors: bad lens grid %d x %d", mla_u_size, mla_v_size);
-    pfd::LensGrid G;
-    if (!G.build(centers, tilekeys, n_views, mla_u_size, mla_v_size))
+    RingPlan rp;
+    if (!rp.build(centers, tilekeys, n_views, mla_u_size, mla_v_size, pitch))
         return fail(ctx, PFD_EINVAL, "select_neighbors: a tile key lies outside the grid or is repeated");
     DeviceGuard g(ctx->device);
     cudaStream_t s = ctx->stream;
@@ -1989,7 +2023,7 @@ pfd_status pfd_select_neighbors(pfd_ctx* ctx, const float* centers, const int* t
         cudaGetLastError();
         st = fail(ctx, PFD_ECUDA, "select_neighbors: %s", cudaGetErrorString(e));
     } else {
-        st = select_lists(ctx, G, pitch, d_img, (int)ppv, mi_w, mi_h, d_c, max_nb, nb_ids, nb_counts);
+        st = select_lists(ctx, rp, nullptr, nullptr, d_img, (int)ppv, mi_w, mi_h, d_c, max_nb, nb_ids, nb_counts);
     }
     for (void* q : { (void*)d_img, (void*)d_c })
         if (q) cudaFreeAsync(q, s);
@@ -2008,14 +2042,31 @@ pfd_status pfd_frame_select_neighbors(pfd_ctx* ctx, int frame_id, int mla_u_size
         return fail(ctx, PFD_EINVAL, "frame_select_neighbors: give both lists (max_list 1-128) or neither");
     if (mla_u_size < 1 || mla_v_size < 1 || (long long)mla_u_size * mla_v_size > (1LL << 28))
         return fail(ctx, PFD_EINVAL, "frame_select_neighbors: bad lens grid %d x %d", mla_u_size, mla_v_size);
-    pfd::LensGrid G;
-    if (!G.build(f->h_centers.data(), f->h_keys.data(), f->V, mla_u_size, mla_v_size))
-        return fail(ctx, PFD_EINVAL, "frame_select_neighbors: a tile key lies outside the grid or is repeated");
     DeviceGuard g(ctx->device);
+    // the rings depend on the lens grid and the pitch only: made once per frame
+    if (!f->rings || f->rings->u != mla_u_size || f->rings->v != mla_v_size || f->rings->pitch != pitch) {
+        auto rp = std::make_shared<RingPlan>();
+        if (!rp->build(f->h_centers.data(), f->h_keys.data(), f->V, mla_u_size, mla_v_size, pitch))
+            return fail(ctx, PFD_EINVAL, "frame_select_neighbors: a tile key lies outside the grid or is repeated");
+        if (f->d_pairs) { frame_free_one(ctx, *f, f->d_pairs, sizeof(int2) * f->n_pairs_alloc); f->d_pairs = nullptr; }
+        if (f->d_sims) { frame_free_one(ctx, *f, f->d_sims, sizeof(int) * f->n_pairs_alloc); f->d_sims = nullptr; }
+        const size_t np = std::max<size_t>(rp->pairs.size(), 1);
+        f->n_pairs_alloc = np;
+        void* p = nullptr;
+        pfd_status st = frame_alloc(ctx, *f, &p, sizeof(int2) * np);
+        if (st != PFD_OK) return st;
+        f->d_pairs = (int2*)p;
+        if ((st = frame_alloc(ctx, *f, &p, sizeof(int) * np)) != PFD_OK) return st;
+        f->d_sims = (int*)p;
+        if (!rp->pairs.empty())
+            CU(cudaMemcpyAsync(f->d_pairs, rp->pairs.data(), sizeof(int2) * rp->pairs.size(), cudaMemcpyHostToDevice,
+                               ctx->stream));
+        f->rings = rp;
+    }
     const int L = std::max(f->K, nb_ids ? max_list : 0);
     std::vector<int> ids((size_t)f->V * L), cnt(f->V);
-    pfd_status st = select_lists(ctx, G, pitch, f->d_gray, f->tile_stride, f->mi_w, f->mi_h, f->d_centers, L,
-                                 ids.data(), cnt.data());
+    pfd_status st = select_lists(ctx, *f->rings, f->d_pairs, f->d_sims, f->d_gray, f->tile_stride, f->mi_w, f->mi_h,
+                                 f->d_centers, L, ids.data(), cnt.data());
     if (st != PFD_OK) return st;
     // the matcher's lists: the first K of each (AdaptMIPMFrame::BuildViewIndexMap keeps the first 16 views)
     for (int v = 0; v < f->V; ++v) {
