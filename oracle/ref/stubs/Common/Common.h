@@ -7,9 +7,10 @@
  * MIStereo/AdaptMIPMFrame.h name.  Test infrastructure: nothing in the engine
  * includes it.
  *
- * MAX_IMAGES is raised from the reference's 4096 (Common/Common.h:28) so that
- * a 4080x3068 frame (26 600 micro-images) fits cudaTextureObjects; nothing
- * else reads it in these files.
+ * MAX_IMAGES is raised from the reference's 4096 (Common/Common.h:28) to the
+ * launch grid's z limit, so that a 4080x3068 frame fits cudaTextureObjects
+ * down to pitch 15 (about 64 000 micro-images); nothing else reads it in these
+ * files.
  */
 #ifndef PFD_REF_STUB_COMMON_H
 #define PFD_REF_STUB_COMMON_H
@@ -27,7 +28,7 @@ class Mat {};
 }
 
 namespace LFMVS {
-#define MAX_IMAGES 32768
+#define MAX_IMAGES 65535
 }
 
 #endif

@@ -175,15 +175,20 @@ __device__ __forceinline__ bool cost_ok(float c, const FilterCfg& cfg)
 
 }  // namespace
 
-// Bounded wait (about a second) for a micro-image's done flag; flags an error
-// and gives up when it runs out.
-__device__ __forceinline__ void wait_done(const int* flag, int* err)
+// Bounded wait for a micro-image's done flag, polled by one thread with a
+// backoff that grows to about a microsecond (so the waiting CTAs do not crowd
+// the L2 the running ones read from); after about a second it flags an error
+// and gives up.  budget: the polls left for this micro-image's waits.
+__device__ __forceinline__ void wait_done(const int* flag, int* err, uint32_t& budget)
 {
-    for (uint32_t it = 0; it < (1u << 24); ++it) {
+    uint32_t ns = 32;
+    while (budget) {
         int f;
         asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(f) : "l"(flag) : "memory");
         if (f != 0) return;
-        if (it > 32) __nanosleep(64);
+        --budget;
+        __nanosleep(ns);
+        if (ns < 1024) ns *= 2;
     }
     atomicOr(err, PFD_DEVERR_FILTER_TIMEOUT);
 }
@@ -211,9 +216,12 @@ __global__ void pm_filter_kernel(CheckFrame F, FilterCfg cfg, StateDev in, State
         const int rv = fl.rank[v];
         const size_t base = (size_t)v * N;
         // the neighbours earlier in key order must be filtered before they are read
-        if (threadIdx.x < nc) {
-            const int u = F.nb_ids[v * F.K + threadIdx.x];
-            if (u >= 0 && u < F.V && fl.rank[u] < rv) wait_done(fl.done + u, fl.err);
+        if (threadIdx.x == 0) {
+            uint32_t budget = 1u << 20;
+            for (int k = 0; k < nc; ++k) {
+                const int u = F.nb_ids[v * F.K + k];
+                if (u >= 0 && u < F.V && fl.rank[u] < rv) wait_done(fl.done + u, fl.err, budget);
+            }
         }
         if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
         for (int e = threadIdx.x; e < N; e += blockDim.x) ref[e] = (float)F.gray[(size_t)v * F.tile_stride + e];
@@ -667,7 +675,6 @@ cudaError_t filter_grid(const CheckFrame& F, int* n_ctas, int* threads)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int smem = filter_smem_bytes(F);
     *threads = F.W * F.H < 256 ? ((F.W * F.H + 31) / 32) * 32 : 256;
-    if (*threads < F.K) *threads = ((F.K + 31) / 32) * 32;       // one thread per neighbour for the waits
     cudaError_t e = cudaFuncSetAttribute(pm_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pm_filter_kernel, *threads, smem);
