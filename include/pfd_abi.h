@@ -167,8 +167,9 @@ pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* param
 /* pfd_patchmatch of n frames of the context at once (no counterpart in the
  * reference, which matches one frame at a time): every frame is initialised,
  * then each half-sweep is ONE persistent launch over all the frames that still
- * have iterations left (frames with a blur channel and frames without take one
- * launch each), in which a CTA that finds one frame's micro-images all taken
+ * have iterations left (one launch per group of frames that share a blur
+ * channel and whose own shared-memory plans allow the same CTAs per SM, so no
+ * frame runs at a larger frame's occupancy), in which a CTA that finds one frame's micro-images all taken
  * moves straight on to the next frame, so small frames and the tails of large
  * ones do not leave the GPU idle between launches.  params[b] and seeds[b] are
  * frame b's own (sizes, neighbour counts, patch sizes and iteration counts may

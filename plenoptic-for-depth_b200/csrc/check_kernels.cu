@@ -5,21 +5,15 @@
 //
 // The filter invalidates rejected pixels in place and walks the micro-images
 // in key order, so a later micro-image reads the already filtered state of
-// earlier neighbours and the unfiltered state of later ones (FilterGlobal,
-// :962-986).  The device keeps exactly that dependency in one launch: CTAs
-// take the micro-images in key order from a counter and write the filtered
-// state to the other state buffer; a micro-image first waits until each of its
-// neighbours that comes earlier in key order is done (a flag per micro-image,
-// released after its writes), then reads those from the output buffer and the
-// later ones from the input buffer, which the launch never writes.  The wait
-// cannot deadlock: every micro-image it waits for was taken earlier by a CTA
-// that is already running, and the earliest unfinished one waits for nothing
-// unfinished.  Waits are bounded (about a second) and flag an error.
+// earlier neighbours (FilterGlobal, :962-986).  The device keeps exactly that
+// dependency: micro-image (col, row) runs in wavefront step col + c * row, with
+// c chosen on the host so that every neighbour earlier in key order falls in
+// an earlier step and every later one in a later step.  Micro-images of one
+// step are never neighbours of each other and run in parallel.
 //
 // Arithmetic is the reference's expressions evaluated as written, one
 // rounding per operation (the library is built with -fmad=false), matching the
 // CPU oracle (oracle/checks.c).
-#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -94,25 +88,15 @@ __device__ __forceinline__ float photo_residual(const float* ref, const float* n
     return fabsf(In - Ir);
 }
 
-// Loads of state another CTA of the same launch wrote go to L2 (the SM's L1
-// is not coherent with other SMs' writes).
-template <bool L2>
-__device__ __forceinline__ float ld_f(const float* p)
-{
-    return L2 ? __ldcg(p) : *p;
-}
-
 // BilinearDisparity (MIDisparityFilter.cpp:80-118) over a neighbour's state.
-template <bool L2 = false>
 __device__ __forceinline__ float bilinear_disp(const float4* plane, int W, int H, float x, float y, float min_valid)
 {
     if (x < 0 || y < 0 || x > W - 1 || y > H - 1) return CUDART_NAN_F;
     const int x0 = (int)floorf(x), y0 = (int)floorf(y);
     const int x1 = min(x0 + 1, W - 1), y1 = min(y0 + 1, H - 1);
     const float ax = x - (float)x0, ay = y - (float)y0;
-    const float* pw = &plane[0].w;
-    const float d00 = ld_f<L2>(pw + 4 * (y0 * W + x0)), d01 = ld_f<L2>(pw + 4 * (y1 * W + x0));
-    const float d10 = ld_f<L2>(pw + 4 * (y0 * W + x1)), d11 = ld_f<L2>(pw + 4 * (y1 * W + x1));
+    const float d00 = plane[y0 * W + x0].w, d01 = plane[y1 * W + x0].w;
+    const float d10 = plane[y0 * W + x1].w, d11 = plane[y1 * W + x1].w;
     if (!isfinite(d00) || d00 <= min_valid || !isfinite(d01) || d01 <= min_valid ||
         !isfinite(d10) || d10 <= min_valid || !isfinite(d11) || d11 <= min_valid)
         return CUDART_NAN_F;
@@ -123,15 +107,13 @@ __device__ __forceinline__ float bilinear_disp(const float4* plane, int W, int H
     return r;
 }
 
-template <bool L2 = false>
 __device__ __forceinline__ float bilinear_cost(const float* cost, int W, int H, float x, float y)
 {
     if (x < 0 || y < 0 || x > W - 1 || y > H - 1) return CUDART_NAN_F;
     const int x0 = (int)floorf(x), y0 = (int)floorf(y);
     const int x1 = min(x0 + 1, W - 1), y1 = min(y0 + 1, H - 1);
     const float ax = x - (float)x0, ay = y - (float)y0;
-    const float c00 = ld_f<L2>(cost + y0 * W + x0), c01 = ld_f<L2>(cost + y1 * W + x0);
-    const float c10 = ld_f<L2>(cost + y0 * W + x1), c11 = ld_f<L2>(cost + y1 * W + x1);
+    const float c00 = cost[y0 * W + x0], c01 = cost[y1 * W + x0], c10 = cost[y0 * W + x1], c11 = cost[y1 * W + x1];
     if (!isfinite(c00) || !isfinite(c01) || !isfinite(c10) || !isfinite(c11)) return CUDART_NAN_F;
     float r = ((1.0f - ax) * (1.0f - ay)) * c00;
     r = r + ((1.0f - ax) * ay) * c01;
@@ -175,26 +157,8 @@ __device__ __forceinline__ bool cost_ok(float c, const FilterCfg& cfg)
 
 }  // namespace
 
-// Bounded wait for a micro-image's done flag, polled by one thread with a
-// backoff that grows to about a microsecond (so the waiting CTAs do not crowd
-// the L2 the running ones read from); after about a second it flags an error
-// and gives up.  budget: the polls left for this micro-image's waits.
-__device__ __forceinline__ void wait_done(const int* flag, int* err, uint32_t& budget)
-{
-    uint32_t ns = 32;
-    while (budget) {
-        int f;
-        asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(f) : "l"(flag) : "memory");
-        if (f != 0) return;
-        --budget;
-        __nanosleep(ns);
-        if (ns < 1024) ns *= 2;
-    }
-    atomicOr(err, PFD_DEVERR_FILTER_TIMEOUT);
-}
-
 // Gray micro-images are read as floats from the 8-bit tiles.
-__global__ void pm_filter_kernel(CheckFrame F, FilterCfg cfg, StateDev in, StateDev out, FilterFlow fl,
+__global__ void pm_filter_kernel(CheckFrame F, FilterCfg cfg, StateDev st, const int* step_views, int n_step,
                                  uint8_t* reason, unsigned long long* stats)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -204,25 +168,10 @@ __global__ void pm_filter_kernel(CheckFrame F, FilterCfg cfg, StateDev in, State
     unsigned char* keep1 = (unsigned char*)(nei + (size_t)F.K * N);
     unsigned char* keepf = keep1 + N;
     __shared__ unsigned long long cnt[8];
-    __shared__ int s_item;
-    for (;;) {
-        __syncthreads();                               // the previous item is finished
-        if (threadIdx.x == 0) s_item = atomicAdd(fl.queue, 1);
-        __syncthreads();
-        const int item = s_item;
-        if (item >= F.V) break;
-        const int v = fl.order[item];
+    for (int item = blockIdx.x; item < n_step; item += gridDim.x) {
+        const int v = step_views[item];
         const int nc = min(F.nb_counts[v], F.K);
-        const int rv = fl.rank[v];
         const size_t base = (size_t)v * N;
-        // the neighbours earlier in key order must be filtered before they are read
-        if (threadIdx.x == 0) {
-            uint32_t budget = 1u << 20;
-            for (int k = 0; k < nc; ++k) {
-                const int u = F.nb_ids[v * F.K + k];
-                if (u >= 0 && u < F.V && fl.rank[u] < rv) wait_done(fl.done + u, fl.err, budget);
-            }
-        }
         if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
         for (int e = threadIdx.x; e < N; e += blockDim.x) ref[e] = (float)F.gray[(size_t)v * F.tile_stride + e];
         for (int e = threadIdx.x; e < nc * N; e += blockDim.x) {
@@ -237,16 +186,16 @@ __global__ void pm_filter_kernel(CheckFrame F, FilterCfg cfg, StateDev in, State
             keep1[idx] = 0;
             uint8_t why = kPrKeep;
             atomicAdd(&cnt[kFsTotal], 1ull);
-            const float d = in.plane[base + idx].w;
+            const float d = st.plane[base + idx].w;
             if (isfinite(d) && d > cfg.min_valid_disp) {
                 atomicAdd(&cnt[kFsValidIn], 1ull);
-                const float cost = in.cost[base + idx];
+                const float cost = st.cost[base + idx];
                 if (!cost_ok(cost, cfg)) {
                     why = kPrCost;
                 } else {
                     int vids[32];
                     int nv;
-                    if (cfg.use_selected_views_only) nv = set_bits(in.sel[base + idx], vids, cfg.max_triplet);
+                    if (cfg.use_selected_views_only) nv = set_bits(st.sel[base + idx], vids, cfg.max_triplet);
                     else { nv = min(nc, cfg.max_triplet); for (int i = 0; i < nv; ++i) vids[i] = i; }
                     if (nv == 0) {
                         why = kPrNoSupport;
@@ -264,16 +213,9 @@ __global__ void pm_filter_kernel(CheckFrame F, FilterCfg cfg, StateDev in, State
                             const float qy = py + (g.dy * d) * g.scale;
                             if (qx < 0 || qy < 0 || qx > W - 1 || qy > H - 1) continue;
                             const size_t nbase = (size_t)nvid * N;
-                            // an earlier neighbour is read filtered (output), a later one as it came in
-                            const bool done = fl.rank[nvid] < rv;
-                            const float d_nei = done ? bilinear_disp<true>(out.plane + nbase, W, H, qx, qy, cfg.min_valid_disp)
-                                                     : bilinear_disp<false>(in.plane + nbase, W, H, qx, qy, cfg.min_valid_disp);
+                            const float d_nei = bilinear_disp(st.plane + nbase, W, H, qx, qy, cfg.min_valid_disp);
                             if (!isfinite(d_nei)) continue;
-                            if (cfg.enable_cost_filter) {
-                                const float cn = done ? bilinear_cost<true>(out.cost + nbase, W, H, qx, qy)
-                                                      : bilinear_cost<false>(in.cost + nbase, W, H, qx, qy);
-                                if (!cost_ok(cn, cfg)) continue;
-                            }
+                            if (cfg.enable_cost_filter && !cost_ok(bilinear_cost(st.cost + nbase, W, H, qx, qy), cfg)) continue;
                             ++support;
                             bool pass_geo = true, pass_photo = true;
                             if (cfg.enable_cycle_geo_filter) {
@@ -314,7 +256,7 @@ __global__ void pm_filter_kernel(CheckFrame F, FilterCfg cfg, StateDev in, State
                     if (xn < 0 || yn < 0 || xn >= W || yn >= H) continue;
                     const int ni = yn * W + xn;
                     if (!keep1[ni]) continue;
-                    const float dv = in.plane[base + ni].w;
+                    const float dv = st.plane[base + ni].w;
                     if (!isfinite(dv) || dv <= cfg.min_valid_disp) continue;
                     nvals[n++] = dv;
                 }
@@ -326,7 +268,7 @@ __global__ void pm_filter_kernel(CheckFrame F, FilterCfg cfg, StateDev in, State
                 nvals[b + 1] = t;
             }
             const float med = nvals[n / 2];
-            const float cur = in.plane[base + idx].w;
+            const float cur = st.plane[base + idx].w;
             if (!isfinite(cur)) continue;
             if (fabsf(cur - med) > cfg.spike_abs_diff) {
                 keepf[idx] = 0;
@@ -335,36 +277,20 @@ __global__ void pm_filter_kernel(CheckFrame F, FilterCfg cfg, StateDev in, State
             }
         }
         __syncthreads();
-        // the view's filtered state: InvalidatePixel (MIDisparityFilter.cpp:158-174) for
-        // every rejected valid pixel, the input for every other
+        // InvalidatePixel (MIDisparityFilter.cpp:158-174) for every rejected valid pixel
         for (int idx = threadIdx.x; idx < N; idx += blockDim.x) {
-            const size_t t = base + idx;
-            float4 pl = in.plane[t];
-            float c = in.cost[t];
-            float4 dq = in.disp[t];
-            uint32_t sv = in.sel[t];
-            const float d = pl.w;
-            if (isfinite(d) && d > cfg.min_valid_disp) {
-                if (keepf[idx]) {
-                    atomicAdd(&cnt[kFsKept], 1ull);
-                } else {
-                    atomicAdd(&cnt[kFsRemoved], 1ull);
-                    pl = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-                    c = 2.0f;
-                    dq = make_float4(-1.0f, -1.0f, 0.0f, 0.0f);
-                    if (cfg.clear_selected_views_when_invalid) sv = 0u;
-                }
-            }
-            out.plane[t] = pl;
-            out.cost[t] = c;
-            out.disp[t] = dq;
-            out.sel[t] = sv;
+            const float d = st.plane[base + idx].w;
+            if (!isfinite(d) || d <= cfg.min_valid_disp) continue;
+            if (keepf[idx]) { atomicAdd(&cnt[kFsKept], 1ull); continue; }
+            atomicAdd(&cnt[kFsRemoved], 1ull);
+            st.plane[base + idx] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+            st.cost[base + idx] = 2.0f;
+            st.disp[base + idx] = make_float4(-1.0f, -1.0f, 0.0f, 0.0f);
+            if (cfg.clear_selected_views_when_invalid) st.sel[base + idx] = 0u;
         }
-        __threadfence();                               // this thread's writes, visible device-wide
         __syncthreads();
-        if (threadIdx.x == 0)
-            asm volatile("st.release.gpu.global.s32 [%0], %1;" :: "l"(fl.done + v), "r"(1) : "memory");
         if (threadIdx.x < 8 && stats) atomicAdd(&stats[threadIdx.x], cnt[threadIdx.x]);
+        __syncthreads();
     }
 }
 
@@ -668,31 +594,15 @@ int filter_smem_bytes(const CheckFrame& F)
     return (1 + F.K) * N * 4 + 2 * N;
 }
 
-cudaError_t filter_grid(const CheckFrame& F, int* n_ctas, int* threads)
+cudaError_t launch_filter_step(const CheckFrame& F, const FilterCfg& cfg, const StateDev& st, const int* step_views,
+                               int n_step, uint8_t* reason, unsigned long long* stats, cudaStream_t s)
 {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (n_step <= 0) return cudaSuccess;
     const int smem = filter_smem_bytes(F);
-    *threads = F.W * F.H < 256 ? ((F.W * F.H + 31) / 32) * 32 : 256;
+    const int threads = F.W * F.H < 256 ? ((F.W * F.H + 31) / 32) * 32 : 256;
     cudaError_t e = cudaFuncSetAttribute(pm_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pm_filter_kernel, *threads, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    *n_ctas = sms * per_sm;
-    return cudaSuccess;
-}
-
-cudaError_t launch_filter(const CheckFrame& F, const FilterCfg& cfg, const StateDev& in, const StateDev& out,
-                          const FilterFlow& fl, uint8_t* reason, unsigned long long* stats, cudaStream_t s)
-{
-    int n_ctas = 0, threads = 0;
-    cudaError_t e = filter_grid(F, &n_ctas, &threads);
-    if (e != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(fl.queue, 0, sizeof(int), s)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(fl.done, 0, sizeof(int) * (size_t)F.V, s)) != cudaSuccess) return e;
-    pm_filter_kernel<<<std::min(n_ctas, F.V), threads, filter_smem_bytes(F), s>>>(F, cfg, in, out, fl, reason, stats);
+    pm_filter_kernel<<<n_step, threads, smem, s>>>(F, cfg, st, step_views, n_step, reason, stats);
     return cudaGetLastError();
 }
 

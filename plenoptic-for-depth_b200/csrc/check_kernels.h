@@ -71,23 +71,10 @@ int cycle_smem_bytes(const CheckFrame& F);
 cudaError_t launch_cycle(const CheckFrame& F, const CycleCfg& cfg, const StateDev& st, float* geo_err, float* pho_err,
                          uint8_t* texmask, CycleTileRec* recs, unsigned int* hist, cudaStream_t s);
 
-// The filter's order: views in key order (row, column), each view's position
-// in it, a done flag per view (zeroed by the launcher), the launch's view
-// counter (zeroed by the launcher) and the device error word.
-struct FilterFlow {
-    const int* order;
-    const int* rank;
-    int* done;
-    int* queue;
-    int* err;
-};
-#define PFD_DEVERR_FILTER_TIMEOUT 0x20   // a filter dependency wait ran out
-
 int filter_smem_bytes(const CheckFrame& F);
-// MIDisparityFilterCPU::FilterGlobal of the whole frame in one launch: reads
-// `in`, writes the filtered state of every view to `out`.
-cudaError_t launch_filter(const CheckFrame& F, const FilterCfg& cfg, const StateDev& in, const StateDev& out,
-                          const FilterFlow& fl, uint8_t* reason, unsigned long long* stats, cudaStream_t s);
+// One wavefront step: the views step_views[0..n_step) filtered in parallel.
+cudaError_t launch_filter_step(const CheckFrame& F, const FilterCfg& cfg, const StateDev& st, const int* step_views,
+                               int n_step, uint8_t* reason, unsigned long long* stats, cudaStream_t s);
 cudaError_t launch_reproj(const CheckFrame& F, const FilterCfg& cfg, const StateDev& st, float* err, cudaStream_t s);
 
 }  // namespace pfd

@@ -111,9 +111,8 @@ struct Frame {
     std::vector<int> h_keys, h_nb_ids, h_nb_counts;
     uint8_t* d_reason = nullptr;      // filter reject reasons, allocated on first use
     float* d_err = nullptr;           // reprojection-error map, allocated on first use
-    int* d_order = nullptr;           // filter: views in key order (row, column), then each view's rank
-    int* d_rank = nullptr;
-    int* d_done = nullptr;            // filter: a done flag per view
+    int* d_steps = nullptr;           // views grouped by wavefront step
+    std::vector<int> step_start;      // [n_steps + 1] offsets into d_steps
     pfd::CycleTileRec* d_cyc_recs = nullptr;   // cycle check: per-view sums, allocated on first use
     unsigned int* d_cyc_hist = nullptr;        // cycle check: masked geometric-error histogram
     float* d_cyc_maps = nullptr;               // cycle check: geo and photo error maps
@@ -336,8 +335,6 @@ pfd_status check_device_error(pfd_ctx* ctx)
         if (h == PFD_DEVERR_REFOCUS_LENSES)
             return fail(ctx, PFD_EINVAL, "refocus: more than %d lenses reach one output tile (slice virtual depth "
                         "too large for this lens density)", pfd::kMaxRefocusCand);
-        if (h & PFD_DEVERR_FILTER_TIMEOUT)
-            return fail(ctx, PFD_ETIMEDOUT, "filter: a wait for an earlier micro-image ran out (flags 0x%x)", h);
         if (h & PFD_DEVERR_SWEEP_CHECK)
             return fail(ctx, PFD_ECUDA, "sweep launch refused its work: shared-memory plan, scratch or neighbour "
                         "ids out of range (flags 0x%x)", h);
@@ -1067,60 +1064,64 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
         const pfd_status st = pfd_pm_init(ctx, frame_ids[b], &params[b], seeds[b]);
         if (st != PFD_OK) return st;
     }
-    // per blur group: the largest shared-memory plan and the grid it allows
+    // launch shape per blur group: the fixed one, or the one tuned for the group's
+    // largest frame (tuned on that frame's first half-sweep when its key is new)
     const bool shift = ctx->ncc_moments == PFD_NCC_SHIFTED;
-    int smem[2] = { 0, 0 }, n_ctas[2] = { 0, 0 }, half_sweeps = 0;
-    bool used[2] = { false, false };
-    size_t scratch = 0;
+    int half_sweeps = 0;
     for (int b = 0; b < n; ++b) {
-        const int grp = fr[b]->has_blur ? 1 : 0;
         const pfd::PmParams P = make_params(ctx, *fr[b], &params[b], seeds[b]);
-        const int sm = pfd::sweep_warp_smem_bytes(P, fr[b]->has_blur);
-        if (sm > 227 * 1024)
+        if (pfd::sweep_warp_smem_bytes(P, fr[b]->has_blur) > 227 * 1024)
             return fail(ctx, PFD_EINVAL, "frame %d: window %dx%d with %d neighbours does not fit shared memory",
                         frame_ids[b], fr[b]->mi_w, fr[b]->mi_h, fr[b]->K);
-        smem[grp] = std::max(smem[grp], sm);
-        used[grp] = true;
         half_sweeps = std::max(half_sweeps, 2 * params[b].max_iterations);
+    }
+    int shape_of_blur[2] = { 0, 0 };
+    for (int grp = 0; grp < 2; ++grp) {
+        int big = -1;
+        for (int b = 0; b < n; ++b)
+            if ((fr[b]->has_blur ? 1 : 0) == grp && params[b].max_iterations > 0 &&
+                (big < 0 || (size_t)fr[b]->V * fr[b]->mi_w * fr[b]->mi_h > (size_t)fr[big]->V * fr[big]->mi_w * fr[big]->mi_h))
+                big = b;
+        if (big < 0) continue;
+        const pfd::PmParams Pb = make_params(ctx, *fr[big], &params[big], seeds[big]);
+        const pfd_status st = sweep_shape_for(ctx, *fr[big], Pb, 0, 0, &shape_of_blur[grp]);
+        if (st != PFD_OK) return st;
+        for (int b = 0; b < n; ++b)          // a shape every frame of the group fits, or the default
+            if ((fr[b]->has_blur ? 1 : 0) == grp &&
+                pfd::sweep_warp_smem_bytes(make_params(ctx, *fr[b], &params[b], seeds[b]), grp == 1,
+                                           shape_of_blur[grp]) > 227 * 1024)
+                shape_of_blur[grp] = 0;
+    }
+    // launch groups: frames with the same blur channel whose own shared-memory plans
+    // allow the same CTAs per SM share a launch, so no frame runs at the occupancy of
+    // a larger frame's plan; a group's plan is its largest member's (same occupancy)
+    struct Group { int blur, ctas, smem, shape; std::vector<int> members; };
+    std::vector<Group> groups;
+    for (int b = 0; b < n; ++b) {
+        const int blur = fr[b]->has_blur ? 1 : 0, shape = shape_of_blur[blur];
+        const int sm = pfd::sweep_warp_smem_bytes(make_params(ctx, *fr[b], &params[b], seeds[b]), blur == 1, shape);
+        int ctas = 0;
+        CU(pfd::sweep_batch_grid(sm, blur == 1, shift, &ctas, shape));
+        int g = -1;
+        for (size_t k = 0; k < groups.size(); ++k)
+            if (groups[k].blur == blur && groups[k].ctas == ctas) g = (int)k;
+        if (g < 0) {
+            groups.push_back(Group{ blur, ctas, 0, shape, {} });
+            g = (int)groups.size() - 1;
+        }
+        groups[g].smem = std::max(groups[g].smem, sm);
+        groups[g].members.push_back(b);
     }
     // one warp-scratch stride for every frame (the largest neighbour count's): CTAs of a
     // launch work on different frames at once, and their regions must not overlap
     int k_max = 0;
     for (int b = 0; b < n; ++b) k_max = std::max(k_max, fr[b]->K);
     const int stride = pfd::sweep_warp_stride(k_max);
-    // launch shape per group: the fixed one, or the one tuned for the group's
-    // largest frame (tuned on that frame's first half-sweep when its key is new)
-    int shape[2] = { 0, 0 };
-    for (int grp = 0; grp < 2; ++grp) {
-        if (!used[grp]) continue;
-        int big = -1;
-        for (int b = 0; b < n; ++b)
-            if ((fr[b]->has_blur ? 1 : 0) == grp && params[b].max_iterations > 0 &&
-                (big < 0 || (size_t)fr[b]->V * fr[b]->mi_w * fr[b]->mi_h > (size_t)fr[big]->V * fr[big]->mi_w * fr[big]->mi_h))
-                big = b;
-        if (big >= 0) {
-            const pfd::PmParams Pb = make_params(ctx, *fr[big], &params[big], seeds[big]);
-            const pfd_status st = sweep_shape_for(ctx, *fr[big], Pb, 0, 0, &shape[grp]);
-            if (st != PFD_OK) return st;
-        }
-        // every frame's plan in the chosen shape (the warps' area grows with the warps)
-        smem[grp] = 0;
-        for (int b = 0; b < n; ++b)
-            if ((fr[b]->has_blur ? 1 : 0) == grp)
-                smem[grp] = std::max(smem[grp], pfd::sweep_warp_smem_bytes(make_params(ctx, *fr[b], &params[b], seeds[b]),
-                                                                        grp == 1, shape[grp]));
-        if (smem[grp] > 227 * 1024) shape[grp] = 0;
-        if (shape[grp] == 0) {
-            smem[grp] = 0;
-            for (int b = 0; b < n; ++b)
-                if ((fr[b]->has_blur ? 1 : 0) == grp)
-                    smem[grp] = std::max(smem[grp], pfd::sweep_warp_smem_bytes(make_params(ctx, *fr[b], &params[b],
-                                                                                        seeds[b]), grp == 1, 0));
-        }
-        CU(pfd::sweep_batch_grid(smem[grp], grp == 1, shift, &n_ctas[grp], shape[grp]));
+    size_t scratch = 0;
+    for (const Group& g : groups) {
         pfd::PmParams Pk = {};
-        Pk.K = k_max;                                  // the scratch of n_ctas CTAs at that stride
-        scratch = std::max(scratch, pfd::sweep_warp_scratch_bytes(Pk, n_ctas[grp], shape[grp]));
+        Pk.K = k_max;                                  // the scratch of the group's CTAs at that stride
+        scratch = std::max(scratch, pfd::sweep_warp_scratch_bytes(Pk, g.ctas, g.shape));
     }
     pfd_status st = ensure_scratch(ctx, scratch);
     if (st != PFD_OK) return st;
@@ -1138,14 +1139,15 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
     CU(cudaMemsetAsync(d_queues, 0, sizeof(int) * n_items, ctx->stream));
     std::vector<pfd::SweepItem> items;
     const int mode = cost_mode(ctx);
+    std::vector<int> count(groups.size());
     for (int s = 0; s < half_sweeps && st == PFD_OK; ++s) {
         const int iter = s / 2, phase = s % 2;
-        int count[2] = { 0, 0 };
+        std::fill(count.begin(), count.end(), 0);
         items.clear();
-        for (int grp = 0; grp < 2; ++grp)
-            for (int b = 0; b < n; ++b) {
+        for (size_t grp = 0; grp < groups.size(); ++grp)
+            for (int b : groups[grp].members) {
                 Frame& f = *fr[b];
-                if ((f.has_blur ? 1 : 0) != grp || s >= 2 * params[b].max_iterations) continue;
+                if (s >= 2 * params[b].max_iterations) continue;
                 pfd::SweepItem it;
                 it.F = frame_dev(f);
                 it.P = make_params(ctx, f, &params[b], seeds[b]);
@@ -1169,10 +1171,12 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
             st = fail(ctx, PFD_ECUDA, "patchmatch_batch: item upload");
             break;
         }
-        for (int grp = 0, off = 0; grp < 2; off += count[grp], ++grp) {
+        int off = 0;
+        for (size_t grp = 0; grp < groups.size(); off += count[grp], ++grp) {
             if (!count[grp]) continue;
-            const cudaError_t e = pfd::launch_sweep_batch(row + off, count[grp], grp == 1, shift, smem[grp],
-                                                          n_ctas[grp], ctx->d_err, ctx->stream, shape[grp]);
+            const Group& G = groups[grp];
+            const cudaError_t e = pfd::launch_sweep_batch(row + off, count[grp], G.blur == 1, shift, G.smem, G.ctas,
+                                                          ctx->d_err, ctx->stream, G.shape);
             if (e != cudaSuccess) {
                 st = fail(ctx, PFD_ECUDA, "launch_sweep_batch: %s", cudaGetErrorString(e));
                 break;
@@ -1299,32 +1303,54 @@ static pfd_status check_filter_cfg(pfd_ctx* ctx, const pfd_filter_cfg* cfg, floa
     return PFD_OK;
 }
 
-// The filter's order (FilterGlobal walks the views in key order, row then
-// column, MIDisparityFilter.cpp:962-986): the views sorted by key, each view's
-// position, and the per-view done flags; made once per frame (keys do not change).
-static pfd_status build_order(pfd_ctx* ctx, Frame& f)
+// Groups the views into wavefront steps col + c * row such that every
+// neighbour that precedes a view in key order (row, col) lands in an earlier
+// step and every one that follows it in a later step.
+static pfd_status build_steps(pfd_ctx* ctx, Frame& f)
 {
-    if (f.d_order) return PFD_OK;
+    if (!f.step_start.empty()) return PFD_OK;
     const int V = f.V;
-    std::vector<int> order(V), rank(V);
-    for (int v = 0; v < V; ++v) order[v] = v;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        const int ra = f.h_keys[2 * a + 1], rb = f.h_keys[2 * b + 1];
-        return ra != rb ? ra < rb : f.h_keys[2 * a] < f.h_keys[2 * b];
-    });
-    for (int i = 0; i < V; ++i) rank[order[i]] = i;
-    void* p = nullptr;
-    pfd_status st = frame_alloc(ctx, f, &p, sizeof(int) * 3 * (size_t)V);
-    if (st != PFD_OK) return st;
-    int* d = (int*)p;
-    std::vector<int> both(2 * (size_t)V);
-    std::copy(order.begin(), order.end(), both.begin());
-    std::copy(rank.begin(), rank.end(), both.begin() + V);
-    CU(cudaMemcpyAsync(d, both.data(), sizeof(int) * 2 * (size_t)V, cudaMemcpyHostToDevice, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));      // the staging vector dies on return
-    f.d_order = d;
-    f.d_rank = d + V;
-    f.d_done = d + 2 * V;
+    long long c = 1;
+    for (int v = 0; v < V; ++v) {
+        const int cv = f.h_keys[2 * v], rv = f.h_keys[2 * v + 1];
+        for (int k = 0; k < f.h_nb_counts[v]; ++k) {
+            const int u = f.h_nb_ids[(size_t)v * f.K + k];
+            if (u < 0) continue;
+            const int cu = f.h_keys[2 * u], ru = f.h_keys[2 * u + 1];
+            if (ru == rv) continue;
+            // earlier row: c (rv - ru) > cu - cv; later row: c (ru - rv) > cv - cu
+            const long long num = (ru < rv) ? (long long)cu - cv : (long long)cv - cu;
+            const long long den = (ru < rv) ? (long long)rv - ru : (long long)ru - rv;
+            long long need = (num >= 0) ? num / den + 1 : 1;
+            if (need > c) c = need;
+        }
+    }
+    std::vector<long long> step(V);
+    long long smin = LLONG_MAX, smax = LLONG_MIN;
+    for (int v = 0; v < V; ++v) {
+        step[v] = (long long)f.h_keys[2 * v] + c * (long long)f.h_keys[2 * v + 1];
+        smin = std::min(smin, step[v]);
+        smax = std::max(smax, step[v]);
+    }
+    const long long ns = smax - smin + 1;
+    if (ns > 100000000LL) return fail(ctx, PFD_EINVAL, "tile keys too sparse for the filter schedule");
+    std::vector<int> counts((size_t)ns + 1, 0), order(V);
+    for (int v = 0; v < V; ++v) counts[(size_t)(step[v] - smin) + 1]++;
+    for (size_t i = 1; i < counts.size(); ++i) counts[i] += counts[i - 1];
+    std::vector<int> fill(counts.begin(), counts.end() - 1);
+    for (int v = 0; v < V; ++v) order[fill[(size_t)(step[v] - smin)]++] = v;
+    // compact away empty steps
+    f.step_start.clear();
+    for (size_t s = 0; s + 1 < counts.size(); ++s)
+        if (counts[s + 1] > counts[s]) f.step_start.push_back(counts[s]);
+    f.step_start.push_back(V);
+    if (!f.d_steps) {                 // kept when new neighbour lists rebuild the schedule
+        void* p = nullptr;
+        pfd_status st = frame_alloc(ctx, f, &p, sizeof(int) * (size_t)V);
+        if (st != PFD_OK) { f.step_start.clear(); return st; }
+        f.d_steps = (int*)p;
+    }
+    CU(cudaMemcpyAsync(f.d_steps, order.data(), sizeof(int) * (size_t)V, cudaMemcpyHostToDevice, ctx->stream));
     return PFD_OK;
 }
 
@@ -1338,7 +1364,7 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
     if (st != PFD_OK) return st;
     if (!f->has_state) return fail(ctx, PFD_ESTATE, "filter before PatchMatch");
     DeviceGuard g(ctx->device);
-    if ((st = build_order(ctx, *f)) != PFD_OK) return st;
+    if ((st = build_steps(ctx, *f)) != PFD_OK) return st;
     const size_t px = (size_t)f->V * f->mi_w * f->mi_h;
     if (!f->d_reason) {
         void* p = nullptr;
@@ -1370,7 +1396,6 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
             CU(cudaGraphLaunch(G.exec, ctx->stream));
             ctx->launches += G.launches;
             f->cvec_valid = 0;
-            f->cur ^= 1;                               // the filtered state is in the other buffer
             return PFD_OK;
         }
         capture = G.warm && !G.exec && G.key == key && G.cur == f->cur;
@@ -1386,15 +1411,14 @@ pfd_status pfd_filter(pfd_ctx* ctx, int frame_id, const pfd_filter_cfg* cfg, flo
     pfd_status fst = PFD_OK;
     if (cudaMemsetAsync(d_stats, 0, 8 * sizeof(unsigned long long), ctx->stream) != cudaSuccess)
         fst = fail(ctx, PFD_ECUDA, "filter: counter reset");
+    const pfd::StateDev& S = f->s[f->cur];
     f->cvec_valid = 0;                             // rejected pixels get new planes
-    if (fst == PFD_OK) {
-        const pfd::FilterFlow fl{ f->d_order, f->d_rank, f->d_done, ctx->d_vq, ctx->d_err };
-        const cudaError_t e = pfd::launch_filter(F, fc, f->s[f->cur], f->s[f->cur ^ 1], fl, f->d_reason, d_stats,
-                                                 ctx->stream);
-        if (e != cudaSuccess) fst = fail(ctx, PFD_ECUDA, "filter: %s", cudaGetErrorString(e));
+    for (size_t s = 0; fst == PFD_OK && s + 1 < f->step_start.size(); ++s) {
+        const int a = f->step_start[s], b = f->step_start[s + 1];
+        cudaError_t e = pfd::launch_filter_step(F, fc, S, f->d_steps + a, b - a, f->d_reason, d_stats, ctx->stream);
+        if (e != cudaSuccess) fst = fail(ctx, PFD_ECUDA, "filter step: %s", cudaGetErrorString(e));
         else ctx->launches += 1;
     }
-    if (fst == PFD_OK) f->cur ^= 1;               // the filtered state is in the other buffer
     if (capture) {
         cudaGraph_t graph = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
@@ -2087,7 +2111,8 @@ pfd_status pfd_frame_select_neighbors(pfd_ctx* ctx, int frame_id, int mla_u_size
     // old lists
     f->has_state = false;
     f->cvec_valid = 0;
-    f->filter_graph.reset();
+    f->step_start.clear();
+    f->filter_graph.reset();          // its launches follow the old lists' schedule
     return PFD_OK;
 }
 
