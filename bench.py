@@ -388,6 +388,33 @@ def run_engine(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
 
+    # the same step with the PatchMatch and the filter replayed from CUDA graphs
+    graphs = None
+    if world == 1:
+        def step_graph():
+            ctx.frame_set_raw_device(fid, raw_dev.data_ptr(), raw_dev.shape[1])
+            ctx.frame_select_neighbors(fid, n_cols, n_rows, WORKLOAD["pitch"])
+            ctx.patchmatch(fid, params, seed)
+            ctx.cycle_check(fid, ccfg, unit, maps=False, stats=False)
+            ctx.filter(fid, fcfg, unit, download=False)
+            ctx.reprojection_error(fid, fcfg, unit, download=False)
+            ctx.refocus(fid, vds, ow, oh, download=False)
+            ctx.cycle_check_stats(fid)
+        ctx.set_graphs(True)
+        for _ in range(2):                       # uncaptured, then captured
+            step_graph()
+        ctx.sync()
+        ga = torch.cuda.Event(enable_timing=True)
+        gb = torch.cuda.Event(enable_timing=True)
+        ga.record(stream)
+        for _ in range(3):
+            step_graph()
+        gb.record(stream)
+        ctx.sync()
+        ctx.set_graphs(False)
+        graphs = {"ms_per_step": round(ga.elapsed_time(gb) / 3, 2),
+                  "covers": "the same step with pfd_patchmatch and the filter replayed from CUDA graphs"}
+
     # e2e through the public API with host buffers: pinned raw frame in; the
     # filtered per-pixel state (plane, cost, selected views) and the focal
     # stack out, every step
@@ -463,6 +490,8 @@ def run_engine(args, rank, world, local_rank):
             "clocks": clk,
             "gpu_launches": launches,
         }
+        if graphs is not None:
+            result["graphs"] = graphs
         result["depth_error"] = dict({k: round(v, 4) for k, v in depth.items()},
                                      against="the scene's true virtual depth at each raw pixel (synthetic frame)")
         if world == 1 and not args.no_cpu_baseline:

@@ -2093,6 +2093,7 @@ pfd_status pfd_frame_select_neighbors(pfd_ctx* ctx, int frame_id, int mla_u_size
                                  f->d_centers, L, ids.data(), cnt.data());
     if (st != PFD_OK) return st;
     // the matcher's lists: the first K of each (AdaptMIPMFrame::BuildViewIndexMap keeps the first 16 views)
+    const std::vector<int> old_ids = f->h_nb_ids, old_counts = f->h_nb_counts;
     for (int v = 0; v < f->V; ++v) {
         const int n = std::min(cnt[v], f->K);
         for (int k = 0; k < f->K; ++k) f->h_nb_ids[(size_t)v * f->K + k] = k < n ? ids[(size_t)v * L + k] : -1;
@@ -2111,8 +2112,10 @@ pfd_status pfd_frame_select_neighbors(pfd_ctx* ctx, int frame_id, int mla_u_size
     // old lists
     f->has_state = false;
     f->cvec_valid = 0;
-    f->step_start.clear();
-    f->filter_graph.reset();          // its launches follow the old lists' schedule
+    if (f->h_nb_ids != old_ids || f->h_nb_counts != old_counts) {
+        f->step_start.clear();        // the filter's schedule and its graph follow the old lists
+        f->filter_graph.reset();
+    }
     return PFD_OK;
 }
 
