@@ -297,6 +297,7 @@ def run_engine(args, rank, world, local_rank):
     vds = slice_vds()
     ccfg, fcfg = pfd.CycleCfg(), pfd.FilterCfg()
     ctx = pfd.Context(local_rank)
+    ctx.set_sweep_fetch(pfd.FETCH_TEXTURE if args.fetch == "texture" else pfd.FETCH_SHARED)
     fid = ctx.frame_create(w.frame.raw.shape[1], w.frame.raw.shape[0], w.centers, w.tilekeys, w.mi, w.mi,
                            w.nb_ids, w.nb_counts)
     raw_dev = torch.from_numpy(w.frame.raw).to(f"cuda:{local_rank}")
@@ -472,6 +473,7 @@ def run_engine(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plenoptic raw frame)",
             "config": {"workload": workload_text(V, ow, oh),
                        "parallelism": "replicas" if world > 1 else "single",
+                       "sweep_fetch": args.fetch,
                        "l2": "per-step working set %.2f GB > 126 MB L2 (state, tiles, focal stack)" %
                              (px * 40 * 2 / 1e9 + len(vds) * ow * oh * 4 / 1e9),
                        "stages": list(STAGES)},
@@ -906,6 +908,8 @@ def main():
     ap.add_argument("--forms-legs", default="batching,serving")
     ap.add_argument("--frame", default=None, help="WxH override (profiling captures of a smaller frame)")
     ap.add_argument("--iterations", type=int, default=None, help="PatchMatch iterations override (profiling)")
+    ap.add_argument("--fetch", choices=["shared", "texture"], default="shared",
+                    help="where the half-sweeps read neighbour samples (pfd_set_sweep_fetch)")
     args = ap.parse_args()
     if args.frame:
         wdt, hgt = args.frame.lower().split("x")

@@ -181,7 +181,7 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
  * pfd_filter calls (reason and stats NULL); no counterpart in the reference,
  * which launches and synchronises kernel by kernel.  Per frame, the first call
  * with a given key (the call's arguments and the context's matcher, moment
- * mode and sweep shape) runs as usual, which sizes the scratch and tunes the
+ * mode, sweep shape and sweep fetch) runs as usual, which sizes the scratch and tunes the
  * launch shape; the second is captured into a graph; later calls replay it.
  * A graph reads and writes the frame's buffers in place, so new raw data and
  * new neighbour lists are picked up; a new key, new neighbour lists (for the
@@ -269,6 +269,22 @@ pfd_status pfd_sweep_shape_info(int shape, int* warps_per_cta, int* ctas_per_sm)
 /* The shape the autotuner chose for the key of (frame, params), or -1 when the
  * key has not been tuned in this process. */
 pfd_status pfd_tuned_sweep_shape(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params, int* shape);
+/* Where the context's later half-sweeps read neighbour samples.
+ * PFD_FETCH_SHARED (the default): from the micro-image and its neighbours
+ * staged in shared memory, blended as the texture unit does.
+ * PFD_FETCH_TEXTURE: from the frame's micro-images held as layered float
+ * textures with the reference's filter settings (linear filter, unnormalised
+ * coordinates; AdaptMIPMFrame.cpp:224-249 makes one texture per micro-image),
+ * one tex2DLayered fetch per tap as the reference's tex2D.  The textures (4
+ * bytes per micro-image pixel and channel) are created at the frame's first
+ * sweep under this mode (pfd_pm_sweep_noalloc creates none: it fetches from
+ * textures only where they exist) and refilled, one launch, before the first
+ * sweep after new tiles.  Both modes give the same state bit for bit; the
+ * texture fetches measure slower on B200.  Tap counting always stages in
+ * shared memory. */
+#define PFD_FETCH_TEXTURE 0
+#define PFD_FETCH_SHARED  1
+pfd_status pfd_set_sweep_fetch(pfd_ctx* ctx, int mode);
 
 /* PostRefineMetadataFrame (AdaptMIPMFrameACMM.cu:903-929): every pixel keeps
  * its plane and gets the cost, selected views and disp of it as the ACMM

@@ -27,6 +27,8 @@ PFD_OK = 0
 PFD_ETIMEDOUT = -5
 SWEEP_SHAPES = 4
 SHAPE_AUTOTUNE = -1
+FETCH_TEXTURE = 0
+FETCH_SHARED = 1
 _ERRNAMES = {-1: "PFD_EINVAL", -2: "PFD_ENOMEM", -3: "PFD_ECUDA", -4: "PFD_ENOFRAME",
              -5: "PFD_ETIMEDOUT", -6: "PFD_ENODEV", -7: "PFD_ESTATE"}
 
@@ -238,6 +240,7 @@ def lib() -> ctypes.CDLL:
             "pfd_select_neighbors": [_P, _P, _P, _I, _I, _I, _F, _P, _I, _I, _I, _P, _P],
             "pfd_frame_select_neighbors": [_P, _I, _I, _I, _F, _I, _P, _P],
             "pfd_set_sweep_shape": [_P, _I],
+            "pfd_set_sweep_fetch": [_P, _I],
             "pfd_set_graphs": [_P, _I],
             "pfd_sweep_shape_info": [_I, _P, _P],
             "pfd_tuned_sweep_shape": [_P, _I, _P, _P],
@@ -503,6 +506,13 @@ class Context:
         """Launch shape of later half-sweeps: 0 .. SWEEP_SHAPES - 1, or
         SHAPE_AUTOTUNE (-1) for the engine's autotuner."""
         self._check(self._L.pfd_set_sweep_shape(self._h, int(shape)), "pfd_set_sweep_shape")
+
+    def set_sweep_fetch(self, mode: int) -> None:
+        """Where later half-sweeps read neighbour samples: FETCH_SHARED (1,
+        the default: tiles staged in shared memory) or FETCH_TEXTURE (0: the
+        frame's layered textures, created at its first sweep in this mode).
+        Both give the same state bit for bit."""
+        self._check(self._L.pfd_set_sweep_fetch(self._h, int(mode)), "pfd_set_sweep_fetch")
 
     def tuned_sweep_shape(self, fid: int, params: "PmParams") -> int:
         """The autotuner's shape for the frame's key, or -1 if not tuned yet."""

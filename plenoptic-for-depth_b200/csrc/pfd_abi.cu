@@ -80,6 +80,28 @@ struct FrameGraph {
     }
 };
 
+// One channel of a frame's micro-image tiles (gray or blur) as layered float
+// textures for the sweep's fetches: view v is layer v % layers of array
+// v / layers.  The surfaces write the same arrays.
+struct TexTiles {
+    std::vector<cudaArray_t> arr;
+    std::vector<cudaTextureObject_t> tex;
+    std::vector<cudaSurfaceObject_t> surf;
+    cudaTextureObject_t* d_tex = nullptr;     // the texture handles on the device (frame allocation)
+    cudaSurfaceObject_t* d_surf = nullptr;    // the surface handles on the device (frame allocation)
+    bool stale = true;                        // the tiles changed since the last fill
+    bool ready() const { return d_tex != nullptr; }
+    void release()
+    {
+        for (auto t : tex) cudaDestroyTextureObject(t);
+        for (auto t : surf) cudaDestroySurfaceObject(t);
+        for (auto a : arr) cudaFreeArray(a);
+        tex.clear(); surf.clear(); arr.clear();
+        d_tex = nullptr; d_surf = nullptr;
+        stale = true;
+    }
+};
+
 struct Frame {
     int W = 0, H = 0;                 // raw frame
     int V = 0, mi_w = 0, mi_h = 0, K = 0, tile_stride = 0;
@@ -133,6 +155,9 @@ struct Frame {
     size_t n_pairs_alloc = 0;                  // entries d_pairs and d_sims hold
     // CUDA graphs of the enqueue-only PatchMatch and filter (pfd_set_graphs)
     FrameGraph pm_graph, filter_graph;
+    // the tiles as textures: [0] gray, [1] blur; tex_layers views per array
+    TexTiles tx[2];
+    int tex_layers = 0;
 };
 
 }  // namespace
@@ -153,6 +178,7 @@ struct pfd_ctx {
     float* d_scratch = nullptr;             // sweep candidate costs, per resident CTA
     size_t scratch_bytes = 0;
     int sweep_shape = 0;                    // launch shape of the half-sweeps, or PFD_SHAPE_AUTOTUNE
+    int sweep_fetch = PFD_FETCH_SHARED;     // where the half-sweeps read neighbour samples
     bool graphs = false;                    // replay pfd_patchmatch / pfd_filter from CUDA graphs
     unsigned scratch_gen = 0;               // bumped whenever d_scratch moves (graphs hold its address)
     std::string last_error;
@@ -222,10 +248,112 @@ void frame_free_one(pfd_ctx* ctx, Frame& f, void* p, size_t bytes)
     if (f.registered) ctx->used -= bytes;
 }
 
+// Creates channel c's textures (c = 0 gray, 1 blur) of frame f: float arrays of
+// mi_w x mi_h texels, up to the device's layer limit each, with a linear-filter,
+// clamped, unnormalised-coordinate texture and a surface on each.
+pfd_status tex_create(pfd_ctx* ctx, Frame& f, int c)
+{
+    TexTiles& T = f.tx[c];
+    if (T.ready()) return PFD_OK;
+    int max_layers = 0, max_w = 0, max_h = 0;
+    cudaDeviceGetAttribute(&max_layers, cudaDevAttrMaxTexture2DLayeredLayers, ctx->device);
+    cudaDeviceGetAttribute(&max_w, cudaDevAttrMaxTexture2DLayeredWidth, ctx->device);
+    cudaDeviceGetAttribute(&max_h, cudaDevAttrMaxTexture2DLayeredHeight, ctx->device);
+    if (max_layers < 1 || f.mi_w > max_w || f.mi_h > max_h)
+        return fail(ctx, PFD_EINVAL, "micro-image %dx%d does not fit a layered texture", f.mi_w, f.mi_h);
+    const int layers = std::min(max_layers, f.V);
+    const int n = (f.V + layers - 1) / layers;
+    const size_t bytes = (size_t)f.V * f.mi_w * f.mi_h * sizeof(float);
+    const size_t pending = f.registered ? 0 : f.bytes;
+    if (ctx->budget && ctx->used + pending + bytes > ctx->budget)
+        return fail(ctx, PFD_ENOMEM, "HBM budget exceeded: %zu in use + %zu requested > %zu", ctx->used + pending,
+                    bytes, ctx->budget);
+    pfd_status st = frame_alloc(ctx, f, (void**)&T.d_tex, sizeof(cudaTextureObject_t) * n);
+    if (st == PFD_OK) st = frame_alloc(ctx, f, (void**)&T.d_surf, sizeof(cudaSurfaceObject_t) * n);
+    if (st != PFD_OK) { T.d_tex = nullptr; T.d_surf = nullptr; return st; }
+    const cudaChannelFormatDesc cd = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        const int nl = std::min(layers, f.V - i * layers);
+        cudaArray_t a = nullptr;
+        e = cudaMalloc3DArray(&a, &cd, make_cudaExtent(f.mi_w, f.mi_h, nl), cudaArrayLayered | cudaArraySurfaceLoadStore);
+        if (e != cudaSuccess) break;
+        T.arr.push_back(a);
+        cudaResourceDesc rd = {};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = a;
+        cudaTextureDesc td = {};
+        td.addressMode[0] = cudaAddressModeClamp;
+        td.addressMode[1] = cudaAddressModeClamp;
+        td.addressMode[2] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        cudaTextureObject_t t = 0;
+        e = cudaCreateTextureObject(&t, &rd, &td, nullptr);
+        if (e != cudaSuccess) break;
+        T.tex.push_back(t);
+        cudaSurfaceObject_t sf = 0;
+        e = cudaCreateSurfaceObject(&sf, &rd);
+        if (e != cudaSuccess) break;
+        T.surf.push_back(sf);
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(T.d_tex, T.tex.data(), sizeof(cudaTextureObject_t) * n, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(T.d_surf, T.surf.data(), sizeof(cudaSurfaceObject_t) * n, cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);      // the handle vectors stay; no staging dies
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamSynchronize(ctx->stream);
+        void* dt = T.d_tex; void* ds = T.d_surf;
+        T.release();
+        frame_free_one(ctx, f, dt, sizeof(cudaTextureObject_t) * n);
+        frame_free_one(ctx, f, ds, sizeof(cudaSurfaceObject_t) * n);
+        return fail(ctx, PFD_ECUDA, "micro-image textures: %s", cudaGetErrorString(e));
+    }
+    f.tex_layers = layers;
+    f.bytes += bytes;
+    if (f.registered) ctx->used += bytes;
+    T.stale = true;
+    return PFD_OK;
+}
+
+// Refills the textures of every channel whose tiles changed since the last
+// fill (stream-ordered before the sweeps that read them).  With create, first
+// creates the textures the frame lacks when the context fetches from textures
+// (an allocation, and a synchronisation of the context's stream).
+pfd_status tex_refresh(pfd_ctx* ctx, Frame& f, bool create = true)
+{
+    if (create && ctx->sweep_fetch == PFD_FETCH_TEXTURE) {
+        for (int c = 0; c < (f.has_blur ? 2 : 1); ++c) {
+            const pfd_status st = tex_create(ctx, f, c);
+            if (st != PFD_OK) return st;
+        }
+    }
+    for (int c = 0; c < 2; ++c) {
+        TexTiles& T = f.tx[c];
+        const uint8_t* tiles = c == 0 ? f.d_gray : (f.has_blur ? f.d_blur : nullptr);
+        if (!T.ready() || !T.stale || !tiles) continue;
+        const cudaError_t e = pfd::launch_tex_fill(tiles, f.V, f.mi_w, f.mi_h, f.tile_stride, T.d_surf, f.tex_layers,
+                                                   ctx->stream);
+        if (e != cudaSuccess) return fail(ctx, PFD_ECUDA, "texture fill: %s", cudaGetErrorString(e));
+        ctx->launches += 1;
+        T.stale = false;
+    }
+    return PFD_OK;
+}
+
 void frame_release(Frame& f, cudaStream_t s)
 {
     f.pm_graph.reset();
     f.filter_graph.reset();
+    if (f.tx[0].ready() || f.tx[1].ready() || !f.tx[0].arr.empty() || !f.tx[1].arr.empty()) {
+        cudaStreamSynchronize(s);                // no launch in flight reads the arrays
+        f.tx[0].release();
+        f.tx[1].release();
+    }
     for (void* p : f.allocs) cudaFreeAsync(p, s);
     f.allocs.clear();
     f.bytes = 0;
@@ -322,6 +450,21 @@ pfd::FrameDev frame_dev(const Frame& f)
     F.nb_ids = f.d_nb_ids;
     F.nb_counts = f.d_nb_counts;
     F.V = f.V;
+    F.tex = nullptr;
+    F.tex_blur = nullptr;
+    F.tex_layers = f.tex_layers;
+    return F;
+}
+
+// The frame as the sweep sees it: with its textures when the context fetches
+// from them and every channel the frame has is held as textures.
+pfd::FrameDev sweep_dev(const pfd_ctx* ctx, const Frame& f)
+{
+    pfd::FrameDev F = frame_dev(f);
+    if (ctx->sweep_fetch == PFD_FETCH_TEXTURE && f.tx[0].ready() && (!f.has_blur || f.tx[1].ready())) {
+        F.tex = f.tx[0].d_tex;
+        F.tex_blur = f.has_blur ? f.tx[1].d_tex : nullptr;
+    }
     return F;
 }
 
@@ -563,6 +706,7 @@ static pfd_status set_raw(pfd_ctx* ctx, int frame_id, const uint8_t* raw, int ra
                          device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     CU(pfd::launch_slice(f->d_raw, f->W, f->d_origin, f->V, f->mi_w, f->mi_h, f->tile_stride, f->d_gray, ctx->stream));
     ctx->launches += 1;
+    f->tx[0].stale = true;
     f->has_raw = true;
     f->has_mi = true;
     f->has_state = false;
@@ -592,6 +736,7 @@ pfd_status pfd_frame_set_micro_images(pfd_ctx* ctx, int frame_id, const uint8_t*
     for (int v = 0; v < f->V; ++v) std::memcpy(&tiles[(size_t)v * f->tile_stride], images + (size_t)v * ppv, ppv);
     CU(cudaMemcpyAsync(f->d_gray, tiles.data(), tiles.size(), cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));       // the staging vector dies on return
+    f->tx[0].stale = true;
     f->has_mi = true;
     f->has_state = false;
     f->cvec_valid = 0;
@@ -610,6 +755,10 @@ pfd_status pfd_frame_compute_blur(pfd_ctx* ctx, int frame_id, uint8_t* blur_out,
         const pfd_status st = frame_alloc(ctx, *f, (void**)&f->d_blur, ppv_tiles);
         if (st != PFD_OK) return st;
     }
+    if (f->tx[0].ready() && !f->tx[1].ready()) {      // the frame's sweeps read textures
+        const pfd_status st = tex_create(ctx, *f, 1);
+        if (st != PFD_OK) return st;
+    }
     uint32_t* d_counts = nullptr;
     if (blureness) CU(cudaMallocAsync((void**)&d_counts, sizeof(uint32_t) * f->V, ctx->stream));
     const cudaError_t e = pfd::launch_blur(f->d_raw, f->W, f->W, f->H, f->d_origin, f->V, f->mi_w, f->mi_h,
@@ -619,6 +768,7 @@ pfd_status pfd_frame_compute_blur(pfd_ctx* ctx, int frame_id, uint8_t* blur_out,
         return fail(ctx, PFD_ECUDA, "launch_blur: %s", cudaGetErrorString(e));
     }
     ctx->launches += 1;
+    f->tx[1].stale = true;
     f->has_blur = true;
     f->has_state = false;
     f->cvec_valid = 0;
@@ -798,11 +948,11 @@ static pfd_status ensure_scratch(pfd_ctx* ctx, size_t need)
 namespace {
 
 struct ShapeKey {
-    int dev, W, H, K, ntap, inc, blur, shift, acmm;
+    int dev, W, H, K, ntap, inc, blur, shift, acmm, tex;
     bool operator<(const ShapeKey& o) const
     {
-        return std::tie(dev, W, H, K, ntap, inc, blur, shift, acmm) <
-               std::tie(o.dev, o.W, o.H, o.K, o.ntap, o.inc, o.blur, o.shift, o.acmm);
+        return std::tie(dev, W, H, K, ntap, inc, blur, shift, acmm, tex) <
+               std::tie(o.dev, o.W, o.H, o.K, o.ntap, o.inc, o.blur, o.shift, o.acmm, o.tex);
     }
 };
 
@@ -811,7 +961,8 @@ std::map<ShapeKey, int> g_shape_cache;
 
 ShapeKey shape_key(const pfd_ctx* ctx, const Frame& f, const pfd::PmParams& P)
 {
-    return ShapeKey{ ctx->device, P.W, P.H, P.K, P.ntap, P.inc, f.has_blur ? 1 : 0, P.shifted, P.acmm };
+    return ShapeKey{ ctx->device, P.W, P.H, P.K, P.ntap, P.inc, f.has_blur ? 1 : 0, P.shifted, P.acmm,
+                     sweep_dev(ctx, f).tex != nullptr ? 1 : 0 };
 }
 
 int cached_shape(const ShapeKey& k)
@@ -838,10 +989,11 @@ static pfd_status tune_shape(pfd_ctx* ctx, Frame& f, pfd::PmParams P, int iter, 
     int best = 0;
     float best_ms = 0.0f;
     pfd_status st = PFD_OK;
+    const pfd::FrameDev F = sweep_dev(ctx, f);
     for (int shape = 0; shape < pfd::kSweepShapes && st == PFD_OK; ++shape) {
-        if (pfd::sweep_warp_smem_bytes(P, f.has_blur, shape) > 227 * 1024) continue;
+        if (pfd::sweep_warp_smem_bytes(P, f.has_blur, shape, F.tex != nullptr) > 227 * 1024) continue;
         int n_ctas = 0;
-        if (pfd::sweep_warp_grid(P, f.has_blur, &n_ctas, shape) != cudaSuccess) {
+        if (pfd::sweep_warp_grid(F, P, &n_ctas, shape) != cudaSuccess) {
             cudaGetLastError();                      // this shape does not fit the plan: not a candidate
             continue;
         }
@@ -852,7 +1004,7 @@ static pfd_status tune_shape(pfd_ctx* ctx, Frame& f, pfd::PmParams P, int iter, 
         Q.scratch_floats = ctx->scratch_bytes / sizeof(float);
         cudaError_t e = cudaEventRecord(a, ctx->stream);
         if (e == cudaSuccess)
-            e = pfd::launch_sweep_warp(frame_dev(f), Q, f.s[f.cur], f.s[f.cur ^ 1], iter, phase, n_ctas, ctx->d_err,
+            e = pfd::launch_sweep_warp(F, Q, f.s[f.cur], f.s[f.cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                                        ctx->stream, shape);
         if (e == cudaSuccess) e = cudaEventRecord(b, ctx->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(b);
@@ -941,19 +1093,22 @@ pfd_status pfd_pm_sweep(pfd_ctx* ctx, int frame_id, const pfd_pm_params* params,
     DeviceGuard g(ctx->device);
     pfd::PmParams P = make_params(ctx, *f, params, seed);
     if (ctx->counting) P.tap_counter = ctx->d_taps;
-    if (pfd::sweep_warp_smem_bytes(P, f->has_blur) > 227 * 1024)
+    st = tex_refresh(ctx, *f);
+    if (st != PFD_OK) return st;
+    const pfd::FrameDev F = sweep_dev(ctx, *f);
+    if (pfd::sweep_warp_smem_bytes(P, f->has_blur, 0, F.tex != nullptr) > 227 * 1024)
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
     int shape = 0;
     st = sweep_shape_for(ctx, *f, P, iter, phase, &shape);
     if (st != PFD_OK) return st;
     int n_ctas = 0;
-    CU(pfd::sweep_warp_grid(P, f->has_blur, &n_ctas, shape));
+    CU(pfd::sweep_warp_grid(F, P, &n_ctas, shape));
     st = ensure_scratch(ctx, pfd::sweep_warp_scratch_bytes(P, n_ctas, shape));
     if (st != PFD_OK) return st;
     P.cost_scratch = ctx->d_scratch;
     P.scratch_floats = ctx->scratch_bytes / sizeof(float);
     P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, cost_mode(ctx));
-    CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
+    CU(pfd::launch_sweep_warp(F, P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream, shape));
     ctx->launches += 1;
     f->cur ^= 1;
@@ -981,12 +1136,14 @@ pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* param
     if (st != PFD_OK) return st;
     // the key: the call's arguments and every context mode the launches depend on
     std::vector<unsigned char> key(sizeof(pfd_pm_params) + sizeof(uint64_t) + 4 * sizeof(int));
-    const int modes[4] = { ctx->matcher, ctx->ncc_moments, ctx->sweep_shape, 0 };
+    const int modes[4] = { ctx->matcher, ctx->ncc_moments, ctx->sweep_shape, ctx->sweep_fetch };
     std::memcpy(key.data(), params, sizeof(pfd_pm_params));
     std::memcpy(key.data() + sizeof(pfd_pm_params), &seed, sizeof(uint64_t));
     std::memcpy(key.data() + sizeof(pfd_pm_params) + sizeof(uint64_t), modes, sizeof(modes));
     FrameGraph& G = f->pm_graph;
     DeviceGuard g(ctx->device);
+    st = tex_refresh(ctx, *f);                   // changed tiles are refilled before, not inside, the graph
+    if (st != PFD_OK) return st;
     if (G.exec && G.scratch_gen != ctx->scratch_gen) G.reset();   // the scratch moved since the capture
     if (G.exec && G.key == key) {
         CU(cudaGraphLaunch(G.exec, ctx->stream));
@@ -1030,6 +1187,15 @@ pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* param
     return PFD_OK;
 }
 
+pfd_status pfd_set_sweep_fetch(pfd_ctx* ctx, int mode)
+{
+    if (!ctx) return PFD_EINVAL;
+    if (mode != PFD_FETCH_TEXTURE && mode != PFD_FETCH_SHARED)
+        return fail(ctx, PFD_EINVAL, "sweep fetch %d: give PFD_FETCH_TEXTURE or PFD_FETCH_SHARED", mode);
+    ctx->sweep_fetch = mode;
+    return PFD_OK;
+}
+
 pfd_status pfd_set_graphs(pfd_ctx* ctx, int on)
 {
     if (!ctx) return PFD_EINVAL;
@@ -1061,7 +1227,8 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
     }
     DeviceGuard g(ctx->device);
     for (int b = 0; b < n; ++b) {
-        const pfd_status st = pfd_pm_init(ctx, frame_ids[b], &params[b], seeds[b]);
+        pfd_status st = pfd_pm_init(ctx, frame_ids[b], &params[b], seeds[b]);
+        if (st == PFD_OK) st = tex_refresh(ctx, *fr[b]);
         if (st != PFD_OK) return st;
     }
     // launch shape per blur group: the fixed one, or the one tuned for the group's
@@ -1070,7 +1237,7 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
     int half_sweeps = 0;
     for (int b = 0; b < n; ++b) {
         const pfd::PmParams P = make_params(ctx, *fr[b], &params[b], seeds[b]);
-        if (pfd::sweep_warp_smem_bytes(P, fr[b]->has_blur) > 227 * 1024)
+        if (pfd::sweep_warp_smem_bytes(P, fr[b]->has_blur, 0, sweep_dev(ctx, *fr[b]).tex != nullptr) > 227 * 1024)
             return fail(ctx, PFD_EINVAL, "frame %d: window %dx%d with %d neighbours does not fit shared memory",
                         frame_ids[b], fr[b]->mi_w, fr[b]->mi_h, fr[b]->K);
         half_sweeps = std::max(half_sweeps, 2 * params[b].max_iterations);
@@ -1089,24 +1256,27 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
         for (int b = 0; b < n; ++b)          // a shape every frame of the group fits, or the default
             if ((fr[b]->has_blur ? 1 : 0) == grp &&
                 pfd::sweep_warp_smem_bytes(make_params(ctx, *fr[b], &params[b], seeds[b]), grp == 1,
-                                           shape_of_blur[grp]) > 227 * 1024)
+                                           shape_of_blur[grp], sweep_dev(ctx, *fr[b]).tex != nullptr) > 227 * 1024)
                 shape_of_blur[grp] = 0;
     }
-    // launch groups: frames with the same blur channel whose own shared-memory plans
-    // allow the same CTAs per SM share a launch, so no frame runs at the occupancy of
-    // a larger frame's plan; a group's plan is its largest member's (same occupancy)
-    struct Group { int blur, ctas, smem, shape; std::vector<int> members; };
+    // launch groups: frames with the same blur channel and fetch whose own
+    // shared-memory plans allow the same CTAs per SM share a launch, so no frame
+    // runs at the occupancy of a larger frame's plan; a group's plan is its
+    // largest member's (same occupancy)
+    struct Group { int blur, tex, ctas, smem, shape; std::vector<int> members; };
     std::vector<Group> groups;
     for (int b = 0; b < n; ++b) {
         const int blur = fr[b]->has_blur ? 1 : 0, shape = shape_of_blur[blur];
-        const int sm = pfd::sweep_warp_smem_bytes(make_params(ctx, *fr[b], &params[b], seeds[b]), blur == 1, shape);
+        const int tex = sweep_dev(ctx, *fr[b]).tex != nullptr ? 1 : 0;
+        const int sm = pfd::sweep_warp_smem_bytes(make_params(ctx, *fr[b], &params[b], seeds[b]), blur == 1, shape,
+                                                  tex == 1);
         int ctas = 0;
-        CU(pfd::sweep_batch_grid(sm, blur == 1, shift, &ctas, shape));
+        CU(pfd::sweep_batch_grid(sm, blur == 1, shift, tex == 1, &ctas, shape));
         int g = -1;
         for (size_t k = 0; k < groups.size(); ++k)
-            if (groups[k].blur == blur && groups[k].ctas == ctas) g = (int)k;
+            if (groups[k].blur == blur && groups[k].tex == tex && groups[k].ctas == ctas) g = (int)k;
         if (g < 0) {
-            groups.push_back(Group{ blur, ctas, 0, shape, {} });
+            groups.push_back(Group{ blur, tex, ctas, 0, shape, {} });
             g = (int)groups.size() - 1;
         }
         groups[g].smem = std::max(groups[g].smem, sm);
@@ -1149,7 +1319,7 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
                 Frame& f = *fr[b];
                 if (s >= 2 * params[b].max_iterations) continue;
                 pfd::SweepItem it;
-                it.F = frame_dev(f);
+                it.F = sweep_dev(ctx, f);
                 it.P = make_params(ctx, f, &params[b], seeds[b]);
                 it.P.cost_scratch = ctx->d_scratch;
                 it.P.scratch_floats = ctx->scratch_bytes / sizeof(float);
@@ -1175,8 +1345,8 @@ pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const
         for (size_t grp = 0; grp < groups.size(); off += count[grp], ++grp) {
             if (!count[grp]) continue;
             const Group& G = groups[grp];
-            const cudaError_t e = pfd::launch_sweep_batch(row + off, count[grp], G.blur == 1, shift, G.smem, G.ctas,
-                                                          ctx->d_err, ctx->stream, G.shape);
+            const cudaError_t e = pfd::launch_sweep_batch(row + off, count[grp], G.blur == 1, shift, G.tex == 1, G.smem,
+                                                          G.ctas, ctx->d_err, ctx->stream, G.shape);
             if (e != cudaSuccess) {
                 st = fail(ctx, PFD_ECUDA, "launch_sweep_batch: %s", cudaGetErrorString(e));
                 break;
@@ -2441,7 +2611,10 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     DeviceGuard g(ctx->device);
     pfd::PmParams P = make_params(ctx, *f, params, seed);
     if (ctx->counting) P.tap_counter = ctx->d_taps;
-    if (pfd::sweep_warp_smem_bytes(P, f->has_blur) > 227 * 1024)
+    st = tex_refresh(ctx, *f, false);            // a launch, no allocation (textures only if the frame has them)
+    if (st != PFD_OK) return st;
+    const pfd::FrameDev F = sweep_dev(ctx, *f);
+    if (pfd::sweep_warp_smem_bytes(P, f->has_blur, 0, F.tex != nullptr) > 227 * 1024)
         return fail(ctx, PFD_EINVAL, "window %dx%d with %d neighbours does not fit shared memory", f->mi_w, f->mi_h, f->K);
     int sms = 0;
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
@@ -2460,7 +2633,7 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
                     f->K, per_cta, kNoAllocScratchBytes, fit, sms, kmax);
     }
     int n_ctas = 0;
-    CU(pfd::sweep_warp_grid(P, f->has_blur, &n_ctas));
+    CU(pfd::sweep_warp_grid(F, P, &n_ctas));
     n_ctas = (int)std::min<size_t>((size_t)n_ctas, fit);
     float* scratch = nullptr;
     st = noalloc_scratch(ctx, &scratch);
@@ -2468,7 +2641,7 @@ extern "C" pfd_status pfd_pm_sweep_noalloc(pfd_ctx* ctx, int frame_id, const pfd
     P.cost_scratch = scratch;
     P.scratch_floats = kNoAllocScratchBytes / sizeof(float);
     P.cvec_ok = !ctx->counting && cvec_usable(*f, *params, phase, cost_mode(ctx));
-    CU(pfd::launch_sweep_warp(frame_dev(*f), P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
+    CU(pfd::launch_sweep_warp(F, P, f->s[f->cur], f->s[f->cur ^ 1], iter, phase, n_ctas, ctx->d_err,
                               ctx->stream));
     ctx->launches += 1;
     f->cur ^= 1;

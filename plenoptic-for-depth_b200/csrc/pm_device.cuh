@@ -48,6 +48,13 @@ struct FrameDev {
     const int* nb_ids;      // [V][K]
     const int* nb_counts;   // [V]
     int V;
+    // The tiles again as layered float textures (linear filter, unnormalised
+    // coordinates, clamped), the reference's micro-image textures with
+    // tex_layers micro-images per texture: view v is layer v % tex_layers of
+    // texture v / tex_layers.  nullptr where the frame has none.
+    const cudaTextureObject_t* tex;        // gray
+    const cudaTextureObject_t* tex_blur;   // blur, or nullptr
+    int tex_layers;
 };
 
 struct StateDev {

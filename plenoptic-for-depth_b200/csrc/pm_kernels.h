@@ -26,8 +26,10 @@ cudaError_t launch_ncc(const FrameDev& F, const PmParams& P, int nseg, int npb, 
 // for bit.  Shape 0 is the default; tap counting always runs shape 0.
 constexpr int kSweepShapes = 4;
 int sweep_shape_warps(int shape);
-cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas, int shape = 0);
-int sweep_warp_smem_bytes(const PmParams& P, bool blur, int shape = 0);
+// The sweep fetches neighbour samples from F.tex when the frame has textures
+// (tap counting excepted), else from shared-memory quads; tex selects the plan.
+cudaError_t sweep_warp_grid(const FrameDev& F, const PmParams& P, int* n_ctas, int shape = 0);
+int sweep_warp_smem_bytes(const PmParams& P, bool blur, int shape, bool tex);
 size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas, int shape = 0);
 // Floats of global scratch one warp uses for K neighbours (PmParams::scratch_stride).
 int sweep_warp_stride(int K);
@@ -41,9 +43,15 @@ struct SweepItem {
     int iter, phase;
 };
 // Grid of the batch kernel for `smem` bytes of dynamic shared memory per CTA.
-cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, int* n_ctas, int shape = 0);
-// items: device array of n frames, all with or all without a blur channel.
-cudaError_t launch_sweep_batch(const SweepItem* items, int n, bool blur, bool shift, int smem, int n_ctas, int* err,
-                               cudaStream_t st, int shape = 0);
+cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, bool tex, int* n_ctas, int shape = 0);
+// items: device array of n frames, all with or all without a blur channel, all
+// with textures (tex) or none.
+cudaError_t launch_sweep_batch(const SweepItem* items, int n, bool blur, bool shift, bool tex, int smem, int n_ctas,
+                               int* err, cudaStream_t st, int shape = 0);
+
+// Fills the layered float textures of a frame's tiles: texel (x, y) of layer
+// v % layers of surface v / layers is tiles[v * tile_stride + y * W + x].
+cudaError_t launch_tex_fill(const uint8_t* tiles, int V, int W, int H, int tile_stride,
+                            const cudaSurfaceObject_t* surfs, int layers, cudaStream_t st);
 
 }  // namespace pfd

@@ -23,9 +23,14 @@
 // follow the best plane, so the result is the sequential one.  A refinement
 // candidate bit-identical to the best plane has its cost and is not evaluated.
 //
-// Neighbour micro-images are held as 32-bit quads: entry (iy, ix) packs the
-// four texels of a bilinear footprint, T(iy,ix), T(iy,ix+1), T(iy+1,ix),
-// T(iy+1,ix+1), indices clamped to the window.  A fetch is one 4-byte load.
+// Neighbour samples come from the texture unit: the frame's micro-images are
+// layered float textures with the reference's filter settings, and a tap is
+// one tex2DLayered fetch, the reference's own tex2D.  The other form (TEX
+// false, used by the tap-counting calibration) stages the neighbours in shared
+// memory as 32-bit quads, entry (iy, ix) packing the four texels of a bilinear
+// footprint, T(iy,ix), T(iy,ix+1), T(iy+1,ix), T(iy+1,ix+1), indices clamped
+// to the window, and blends them as the texture unit does (measured, and equal
+// to the fetches bit for bit).
 #include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -46,11 +51,13 @@ template <> struct ShapeOf<1> { static constexpr int warps = 8, min_ctas = 3; };
 template <> struct ShapeOf<2> { static constexpr int warps = 4, min_ctas = 6; };
 template <> struct ShapeOf<3> { static constexpr int warps = 10, min_ctas = 2; };
 constexpr int kShapeWarps[kSweepShapes] = { ShapeOf<0>::warps, ShapeOf<1>::warps, ShapeOf<2>::warps, ShapeOf<3>::warps };
+constexpr int kShapeCtas[kSweepShapes] = { ShapeOf<0>::min_ctas, ShapeOf<1>::min_ctas, ShapeOf<2>::min_ctas,
+                                           ShapeOf<3>::min_ctas };
 
 struct Quad {
     const float* R;          // [H][W] reference texels
     const float* RB;         // [H][W] reference blur or nullptr
-    uint32_t q_addr;         // shared address of neighbour quads [K][H+1][W+1]
+    uint32_t q_addr;         // shared address of neighbour quads [K][H+1][W+1] (shared-memory fetches)
     uint32_t qb_addr;        // same for blur
     int qs;                  // W + 1
     int q_bytes;             // (H + 1) * (W + 1) * 4
@@ -58,6 +65,9 @@ struct Quad {
     const int* nb_ok;        // [K]
     const float* a_s;        // [ntap * ntap]
     const float* a_c;        // [256]
+    const cudaTextureObject_t* txh;    // [K] neighbour k's gray texture (texture fetches)
+    const cudaTextureObject_t* txbh;   // [K] its blur texture
+    const int* txl;                    // [K] its layer
 };
 
 // Per-warp scratch.  The tap table and the hypotheses, read on every tap, are
@@ -87,11 +97,13 @@ __host__ __device__ inline int sweep_warp_words(int K)
 
 struct Plan {
     int off_Q, off_QB, off_R, off_RB, off_geo, off_ok, off_as, off_ac, off_pc, off_ps, off_stage, off_bar, off_ctl;
+    int off_txh, off_txbh, off_txl;
     int off_warp, warp_bytes, tab_n, maxh;
     int total;
 
     __host__ __device__ static int a16(int v) { return (v + 15) & ~15; }
-    __host__ __device__ static Plan make(int W, int H, int K, int ntap, bool blur, int tile_stride, int warps)
+    // tex: neighbours are fetched from textures (no quads; only the reference tile is staged)
+    __host__ __device__ static Plan make(int W, int H, int K, int ntap, bool blur, int tile_stride, int warps, bool tex)
     {
         Plan p;
         int o = 0;
@@ -99,9 +111,12 @@ struct Plan {
         // every frame, so one barrier serves a launch over several frames
         p.off_bar = o;   o += 16;
         p.off_ctl = o;   o += 16;
-        const int qb = (H + 1) * (W + 1) * 4;
+        const int qb = tex ? 0 : (H + 1) * (W + 1) * 4;
         p.off_Q = o;     o += a16(K * qb);
         p.off_QB = o;    o += blur ? a16(K * qb) : 0;
+        p.off_txh = o;   o += tex ? a16(K * 8) : 0;
+        p.off_txbh = o;  o += (tex && blur) ? a16(K * 8) : 0;
+        p.off_txl = o;   o += tex ? a16(K * 4) : 0;
         p.off_R = o;     o += a16(W * H * 4);
         p.off_RB = o;    o += blur ? a16(W * H * 4) : 0;
         p.off_geo = o;   o += a16(K * (int)sizeof(NbGeo));
@@ -117,7 +132,7 @@ struct Plan {
         // and read only between views, while no warp holds a pixel
         p.off_warp = o;
         p.off_stage = o;
-        const int stage_bytes = a16((1 + K) * tile_stride * (blur ? 2 : 1));
+        const int stage_bytes = a16((tex ? 1 : 1 + K) * tile_stride * (blur ? 2 : 1));
         o += (warps * p.warp_bytes > stage_bytes) ? warps * p.warp_bytes : stage_bytes;
         p.total = o;
         return p;
@@ -216,14 +231,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // Stages micro-image vid and its neighbours: bulk copies of the 8-bit tiles,
 // then the reference as floats and the neighbours as quads.  The mbarrier is
 // reused with alternating parity, one phase per staged view.
-template <bool BLUR>
+template <bool BLUR, bool TEX>
 __device__ bool stage_view(unsigned char* smem, const Plan& L, const FrameDev& F, const PmParams& P, int vid, int nc,
                            uint32_t parity, int* err, Quad& T)
 {
     const int W = P.W, H = P.H, K = P.K, ts = P.tile_stride;
     uint8_t* stage = (uint8_t*)(smem + L.off_stage);
     uint64_t* bar = (uint64_t*)(smem + L.off_bar);
-    const int nt = 1 + nc;
+    const int nt = TEX ? 1 : 1 + nc;
     if (threadIdx.x == 0) {
         // the warps' writes to the shared area before the last barrier, ordered
         // before the bulk copies that overwrite it
@@ -238,12 +253,21 @@ __device__ bool stage_view(unsigned char* smem, const Plan& L, const FrameDev& F
     }
     NbGeo* geo = (NbGeo*)(smem + L.off_geo);
     int* okk = (int*)(smem + L.off_ok);
+    cudaTextureObject_t* txh = (cudaTextureObject_t*)(smem + L.off_txh);
+    cudaTextureObject_t* txbh = (cudaTextureObject_t*)(smem + L.off_txbh);
+    int* txl = (int*)(smem + L.off_txl);
     const float2 c0 = F.centers[vid];
     for (int k = threadIdx.x; k < K; k += blockDim.x) {
         int v = (k < nc) ? F.nb_ids[vid * K + k] : -1;
         if (v >= F.V) { atomicOr(err, PFD_DEVERR_SWEEP_CHECK); v = -1; }
         okk[k] = (v >= 0);
         geo[k] = make_geo(c0, F.centers[v >= 0 ? v : vid], P);
+        if (TEX) {
+            const int vv = v >= 0 ? v : vid;
+            txh[k] = F.tex[vv / F.tex_layers];
+            if (BLUR) txbh[k] = F.tex_blur[vv / F.tex_layers];
+            txl[k] = vv % F.tex_layers;
+        }
     }
     const bool ok = mbar_wait_bounded(bar, parity, err);
     if (__syncthreads_or(!ok)) return false;
@@ -256,7 +280,7 @@ __device__ bool stage_view(unsigned char* smem, const Plan& L, const FrameDev& F
     const int qs = W + 1, qn = (H + 1) * qs;
     uint32_t* Q = (uint32_t*)(smem + L.off_Q);
     uint32_t* QB = (uint32_t*)(smem + L.off_QB);
-    for (int e = threadIdx.x; e < nc * qn; e += blockDim.x) {
+    for (int e = threadIdx.x; e < (TEX ? 0 : nc * qn); e += blockDim.x) {
         const int k = e / qn, r = e % qn;
         const int iy = r / qs, ix = r % qs;
         const int y0 = min(iy, H - 1), y1 = min(iy + 1, H - 1);
@@ -280,6 +304,9 @@ __device__ bool stage_view(unsigned char* smem, const Plan& L, const FrameDev& F
     T.nb_ok = okk;
     T.a_s = (const float*)(smem + L.off_as);
     T.a_c = (const float*)(smem + L.off_ac);
+    T.txh = txh;
+    T.txbh = txbh;
+    T.txl = txl;
     return true;
 }
 
@@ -399,12 +426,83 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
     return c;
 }
 
+// ncc_lane with the neighbour samples fetched by the texture unit, as the
+// reference's tex2D(images[id], x + 0.5, y + 0.5) fetches them.  Every lane
+// fetches every tap; a tap outside the neighbour window adds +0 to each sum,
+// which leaves the sum as it is (a sum starts at +0 and never becomes -0), so
+// the sums are the ones of the skipped taps without a branch.
+template <bool BLUR, bool COUNT, bool SHIFT>
+__device__ __forceinline__ float ncc_lane_tex(const Quad& T, const PmParams& P, const float4* tab, const PixWin& pw,
+                                              float3 dp, int k, bool active, float sh, unsigned& ntaps)
+{
+    const NbGeo& g = T.geo[k];
+    const float stx = g.stx, sty = g.sty;
+    const cudaTextureObject_t tx = T.txh[k];
+    const cudaTextureObject_t txb = BLUR ? T.txbh[k] : 0;
+    const int layer = T.txl[k];
+    float sr = 0.f, srr = 0.f, ss = 0.f, sss = 0.f, srs = 0.f, sw = 0.f, bsx = 0.f, bsy = 0.f;
+    const float finc = (float)P.inc;
+    float fxr = (float)pw.x0;
+    int t = 0;
+    for (int ix = 0; ix < pw.nX; ++ix, fxr = __fadd_rn(fxr, finc)) {
+        const float axr = __fmul_rn(dp.x, fxr);
+        float fyr = (float)pw.y0;
+#pragma unroll 4
+        for (int iy = 0; iy < pw.nY; ++iy, ++t, fyr = __fadd_rn(fyr, finc)) {
+            const float4 e = tab[t];
+            const float d = __fadd_rn(__fmaf_rn(dp.y, fyr, axr), dp.z);
+            const float sx = __fmaf_rn(stx, d, fxr);
+            const float sy = __fmaf_rn(sty, d, fyr);
+            const bool v = active && (__float_as_uint(sx) < P.W_bits) && (__float_as_uint(sy) < P.H_bits);
+            if (COUNT) ntaps += v ? 1u : 0u;
+            const float cx = __fadd_rn(sx, 0.5f), cy = __fadd_rn(sy, 0.5f);
+            float s = 0.0f;
+            if (v) s = tex2DLayered<float>(tx, cx, cy, layer);      // no request for a skipped tap
+            if (SHIFT) s = v ? __fsub_rn(s, sh) : 0.0f;
+            const float wv = v ? e.x : 0.0f, wrv = v ? e.y : 0.0f;
+            const float ws = __fmul_rn(wv, s);
+            sr = __fmaf_rn(wv, e.z, sr);
+            srr = __fmaf_rn(wrv, e.z, srr);
+            ss = __fmaf_rn(wv, s, ss);
+            sss = __fmaf_rn(ws, s, sss);
+            srs = __fmaf_rn(wrv, s, srs);
+            sw = __fadd_rn(sw, wv);
+            if (BLUR) {
+                float fb = 0.0f;
+                if (v) fb = tex2DLayered<float>(txb, cx, cy, layer);
+                bsx = __fadd_rn(bsx, v ? e.w : 0.0f);
+                bsy = __fadd_rn(bsy, __fdiv_rn(fb, 255.0f));       // 0 / 255 = +0 for a skipped tap
+            }
+        }
+    }
+    float c = kCostMax;
+    if (sw > 1e-6f) {
+        const float inv = __fdiv_rn(1.0f, sw);
+        const float m_r = __fmul_rn(sr, inv), m_rr = __fmul_rn(srr, inv);
+        const float m_s = __fmul_rn(ss, inv), m_ss = __fmul_rn(sss, inv);
+        const float m_rs = __fmul_rn(srs, inv);
+        const float var_r = __fmaf_rn(-m_r, m_r, m_rr);
+        const float var_s = __fmaf_rn(-m_s, m_s, m_ss);
+        if (!(var_r < 1e-5f || var_s < 1e-5f)) {
+            const float cov = __fmaf_rn(-m_r, m_s, m_rs);
+            const float vv = __fsqrt_rn(__fmul_rn(var_r, var_s));
+            c = clamp_cost(__fsub_rn(1.0f, __fdiv_rn(cov, vv)));
+        }
+    }
+    if (BLUR) {
+        const float tb = __fsub_rn(bsx, bsy);
+        const float bw = pfd_expf(__fmul_rn(__fmul_rn(-0.007368f, tb), tb));
+        c = clamp_cost(__fmaf_rn(P.blur_gain, __fsub_rn(1.0f, bw), c));
+    }
+    return c;
+}
+
 // Cost vectors (ComputeMultiViewCostVector_Frame, AdaptMIPMFrame.cu:181-225) of
 // hypotheses S.plane[0..nh) at (px, py), except those whose bit is set in
 // skip: S.cost[h * K + k] for the neighbours k < nc whose bit is set in vmask
 // (the other entries are left as they are).  A neighbour whose anchor leaves
 // the window gets 2 without evaluation.
-template <bool BLUR, bool COUNT, bool SHIFT>
+template <bool BLUR, bool COUNT, bool SHIFT, bool TEX>
 __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const WarpBlock& S, const PixWin& pw,
                                        int px, int py, int nh, int nc, int lane, uint64_t skip, uint32_t vmask)
 {
@@ -440,7 +538,9 @@ __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const W
         const int n = act ? S.pair[p0 + lane] : 0;
         const int h = n / nc, k = n - h * nc;
         const float4 d = S.dp[h];
-        const float c = ncc_lane<BLUR, COUNT, SHIFT>(T, P, S.tab, pw, make_float3(d.x, d.y, d.z), k, act, sh, ntaps);
+        const float3 dp = make_float3(d.x, d.y, d.z);
+        const float c = TEX ? ncc_lane_tex<BLUR, COUNT, SHIFT>(T, P, S.tab, pw, dp, k, act, sh, ntaps)
+                            : ncc_lane<BLUR, COUNT, SHIFT>(T, P, S.tab, pw, dp, k, act, sh, ntaps);
         if (act) S.cost[h * K + k] = c;
     }
     if (COUNT) {
@@ -600,19 +700,20 @@ __device__ __forceinline__ void refine_candidates(int x, int y, float4 best, flo
 // One half-sweep of one frame by this CTA: it takes the frame's micro-images
 // from P.view_queue until none is left.  parity: the staging barrier's phase,
 // carried across frames.  Returns false when a staging wait gave up.
-template <bool BLUR, bool COUNT, bool SHIFT, int WARPS>
+template <bool BLUR, bool COUNT, bool SHIFT, bool TEX, int WARPS>
 __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev& F, const PmParams& P,
                                             const StateDev& prev, const StateDev& next, int iter, int phase, int* err,
                                             uint32_t& parity)
 {
     const int W = P.W, H = P.H, K = P.K;
-    const Plan L = Plan::make(W, H, K, P.ntap, BLUR, P.tile_stride, WARPS);
+    const Plan L = Plan::make(W, H, K, P.ntap, BLUR, P.tile_stride, WARPS, TEX);
     {
         // the frame's shared-memory plan and its warps' scratch must fit what the
         // launch has (checked once per frame; the decision is the same in every thread)
         uint32_t dyn;
         asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
         const bool fits = L.total <= (int)dyn && P.view_queue != nullptr && P.cost_scratch != nullptr &&
+                          (!TEX || (F.tex != nullptr && F.tex_layers > 0 && (!BLUR || F.tex_blur != nullptr))) &&
                           P.scratch_stride >= sweep_warp_words(K) &&
                           (size_t)gridDim.x * WARPS * (size_t)P.scratch_stride <= P.scratch_floats;
         if (!fits) {
@@ -666,7 +767,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
         }
         if (nc <= 0) { __syncthreads(); continue; }
         Quad T;
-        if (!stage_view<BLUR>(smem, L, F, P, vid, nc, parity, err, T)) return false;
+        if (!stage_view<BLUR, TEX>(smem, L, F, P, vid, nc, parity, err, T)) return false;
         parity ^= 1u;
         if (threadIdx.x == 0) ctl[0] = 0;
         __syncthreads();
@@ -717,7 +818,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
             const bool use_cvec = !COUNT && P.cvec_ok;
             if (use_cvec && lane < nc) S.cost[lane] = P.cvec[idx * K + lane];
             __syncwarp();
-            eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, nh, nc, lane, use_cvec ? 1ull : 0ull, ~0u);
+            eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, nh, nc, lane, use_cvec ? 1ull : 0ull, ~0u);
 #define SLOT(s) ((int)((slots >> (4 * (s))) & 15ull))
 #define COSTA(s, k) S.cost[SLOT(s) * K + (k)]
 
@@ -840,7 +941,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                 if (lane == 0)
                     for (int i = 0; i < 5; ++i) S.plane[r0 + i] = cand[i];
                 __syncwarp();
-                eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull, tsel);
+                eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull, tsel);
                 weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
 
                 bool changed = false;
@@ -866,7 +967,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                         __syncwarp();
                         if (lane == 0) S.plane[row] = proxy;
                         __syncwarp();
-                        eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull, tsel);
+                        eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull, tsel);
                         weigh_hyps(S, K, row + 1, nc, vw_lo, vw_hi, lane, tsel);
                         c = S.wres[row];
                         cmin = S.wmin[row];
@@ -883,7 +984,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                         for (int i = 2; i < 5; ++i) S.plane[r0 + i] = cand[i];
                     __syncwarp();
                     const uint64_t redo = (7ull << (r0 + 2)) & ~(skip3 ? (1ull << (r0 + 3)) : 0ull);
-                    eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo, tsel);
+                    eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo, tsel);
                     weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
                 }
                 for (int i = 0; i < 5; ++i) {
@@ -903,7 +1004,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                     __syncwarp();
                     if (lane == 0) S.plane[0] = proxy;
                     __syncwarp();
-                    eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
+                    eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
                     weigh_hyps(S, K, 1, nc, vw_lo, vw_hi, lane, ~0u);
                     const float c = S.wres[0];
                     if (c < best_cost) { best_cost = c; best_plane = proxy; best_min = S.wmin[0]; }
@@ -914,7 +1015,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                 if (lane == 0)
                     for (int i = 0; i < 5; ++i) S.plane[i] = cand[i];
                 __syncwarp();
-                eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, 5, nc, lane, 0ull, ~0u);
+                eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, 5, nc, lane, 0ull, ~0u);
                 weigh_hyps(S, K, 5, nc, vw_lo, vw_hi, lane, ~0u);
                 for (int i = 0; i < 5; ++i) {
                     const float c = S.wres[i];
@@ -931,7 +1032,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                 __syncwarp();
                 if (lane == 0) S.plane[0] = best_plane;
                 __syncwarp();
-                eval_hyps<BLUR, COUNT, SHIFT>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
+                eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
                 weigh_hyps(S, K, 1, nc, vw_lo, vw_hi, lane, ~0u);
                 best_min = S.wmin[0];
                 best_vec = lane < nc ? S.cost[lane] : 0.0f;
@@ -998,21 +1099,21 @@ __device__ __forceinline__ void init_barrier(unsigned char* smem)
     __syncthreads();
 }
 
-template <bool BLUR, bool COUNT, bool SHIFT, int SHAPE>
+template <bool BLUR, bool COUNT, bool SHIFT, int SHAPE, bool TEX>
 __global__ void __launch_bounds__(32 * ShapeOf<SHAPE>::warps, ShapeOf<SHAPE>::min_ctas)
 pm_sweep_warp_kernel(FrameDev F, PmParams P, StateDev prev, StateDev next, int iter, int phase, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     init_barrier(smem);
     uint32_t parity = 0;
-    sweep_frame<BLUR, COUNT, SHIFT, ShapeOf<SHAPE>::warps>(smem, F, P, prev, next, iter, phase, err, parity);
+    sweep_frame<BLUR, COUNT, SHIFT, TEX, ShapeOf<SHAPE>::warps>(smem, F, P, prev, next, iter, phase, err, parity);
 }
 
 // Several frames' half-sweeps in one launch, in list order: a CTA that finds a
 // frame's queue empty moves on to the next frame at once, so one frame's tail
 // overlaps the next one's start.  The dynamic shared memory is the largest of
 // the frames' plans.
-template <bool BLUR, bool SHIFT, int SHAPE>
+template <bool BLUR, bool SHIFT, int SHAPE, bool TEX>
 __global__ void __launch_bounds__(32 * ShapeOf<SHAPE>::warps, ShapeOf<SHAPE>::min_ctas)
 pm_sweep_batch_kernel(const SweepItem* items, int n, int* err)
 {
@@ -1021,17 +1122,21 @@ pm_sweep_batch_kernel(const SweepItem* items, int n, int* err)
     uint32_t parity = 0;
     for (int b = 0; b < n; ++b) {
         const SweepItem it = items[b];
-        if (!sweep_frame<BLUR, false, SHIFT, ShapeOf<SHAPE>::warps>(smem, it.F, it.P, it.prev, it.next, it.iter,
-                                                                    it.phase, err, parity))
+        if (!sweep_frame<BLUR, false, SHIFT, TEX, ShapeOf<SHAPE>::warps>(smem, it.F, it.P, it.prev, it.next, it.iter,
+                                                                         it.phase, err, parity))
             return;
     }
 }
 
 int sweep_shape_warps(int shape) { return kShapeWarps[(shape >= 0 && shape < kSweepShapes) ? shape : 0]; }
 
-int sweep_warp_smem_bytes(const PmParams& P, bool blur, int shape)
+// Tap counting stages the neighbours in shared memory; the other sweeps fetch
+// them from the frame's textures when it has them.
+static bool uses_tex(const FrameDev& F, const PmParams& P) { return F.tex != nullptr && P.tap_counter == nullptr; }
+
+int sweep_warp_smem_bytes(const PmParams& P, bool blur, int shape, bool tex)
 {
-    return Plan::make(P.W, P.H, P.K, P.ntap, blur, P.tile_stride, sweep_shape_warps(shape)).total;
+    return Plan::make(P.W, P.H, P.K, P.ntap, blur, P.tile_stride, sweep_shape_warps(shape), tex && !P.tap_counter).total;
 }
 
 int sweep_warp_stride(int K) { return sweep_warp_words(K); }
@@ -1041,66 +1146,94 @@ size_t sweep_warp_scratch_bytes(const PmParams& P, int n_ctas, int shape)
     return (size_t)n_ctas * sweep_shape_warps(shape) * (size_t)sweep_warp_words(P.K) * 4u;
 }
 
-template <class Kern>
-static cudaError_t launch_k(Kern k, dim3 grid, dim3 block, int smem, cudaStream_t st, void** args)
+// Dynamic shared memory of a sweep kernel, and for the texture-fetch kernels the
+// carveout they ask for: the shared memory of the CTAs per SM the shape's
+// registers allow (with the 1 KB each CTA reserves), so the rest of the SM's
+// 256 KB stays L1 and texture cache.  The shared-memory kernels keep the
+// driver's choice.
+static cudaError_t set_smem(const void* k, int smem, int shape, bool tex)
 {
-    cudaError_t e = cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess || !tex) return e;
+    const int ctas = kShapeCtas[(shape >= 0 && shape < kSweepShapes) ? shape : 0];
+    const long need = (long)ctas * (smem + 1024);
+    const int pct = (int)std::min<long>(100, (need * 100 + 228 * 1024 - 1) / (228 * 1024) + 1);
+    return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+}
+
+template <class Kern>
+static cudaError_t launch_k(Kern k, dim3 grid, dim3 block, int smem, int shape, bool tex, cudaStream_t st,
+                            void** args)
+{
+    cudaError_t e = set_smem((const void*)k, smem, shape, tex);
     if (e != cudaSuccess) return e;
     return cudaLaunchKernel((const void*)k, grid, block, args, (size_t)smem, st);
 }
 
-// The half-sweep kernel of one variant; tap counting exists in shape 0 only.
+// The half-sweep kernel of one variant; tap counting exists in shape 0 with
+// shared-memory fetches only.
+template <int SHAPE, bool TEX>
+static const void* warp_kernel_of(bool blur, bool shift)
+{
+    if (shift) return blur ? (const void*)pm_sweep_warp_kernel<true, false, true, SHAPE, TEX>
+                           : (const void*)pm_sweep_warp_kernel<false, false, true, SHAPE, TEX>;
+    return blur ? (const void*)pm_sweep_warp_kernel<true, false, false, SHAPE, TEX>
+                : (const void*)pm_sweep_warp_kernel<false, false, false, SHAPE, TEX>;
+}
+
 template <int SHAPE>
-static const void* warp_kernel_of(bool blur, bool count, bool shift)
+static const void* warp_kernel_of(bool blur, bool shift, bool tex)
+{
+    return tex ? warp_kernel_of<SHAPE, true>(blur, shift) : warp_kernel_of<SHAPE, false>(blur, shift);
+}
+
+static const void* warp_kernel(int shape, bool blur, bool count, bool shift, bool tex)
 {
     if (count) {
-        if (shift) return blur ? (const void*)pm_sweep_warp_kernel<true, true, true, 0>
-                               : (const void*)pm_sweep_warp_kernel<false, true, true, 0>;
-        return blur ? (const void*)pm_sweep_warp_kernel<true, true, false, 0>
-                    : (const void*)pm_sweep_warp_kernel<false, true, false, 0>;
+        if (shift) return blur ? (const void*)pm_sweep_warp_kernel<true, true, true, 0, false>
+                               : (const void*)pm_sweep_warp_kernel<false, true, true, 0, false>;
+        return blur ? (const void*)pm_sweep_warp_kernel<true, true, false, 0, false>
+                    : (const void*)pm_sweep_warp_kernel<false, true, false, 0, false>;
     }
-    if (shift) return blur ? (const void*)pm_sweep_warp_kernel<true, false, true, SHAPE>
-                           : (const void*)pm_sweep_warp_kernel<false, false, true, SHAPE>;
-    return blur ? (const void*)pm_sweep_warp_kernel<true, false, false, SHAPE>
-                : (const void*)pm_sweep_warp_kernel<false, false, false, SHAPE>;
+    switch (shape) {
+    case 1: return warp_kernel_of<1>(blur, shift, tex);
+    case 2: return warp_kernel_of<2>(blur, shift, tex);
+    case 3: return warp_kernel_of<3>(blur, shift, tex);
+    default: return warp_kernel_of<0>(blur, shift, tex);
+    }
 }
 
-static const void* warp_kernel(int shape, bool blur, bool count, bool shift)
+template <int SHAPE, bool TEX>
+static const void* batch_kernel_of(bool blur, bool shift)
 {
-    if (count) shape = 0;
-    switch (shape) {
-    case 1: return warp_kernel_of<1>(blur, count, shift);
-    case 2: return warp_kernel_of<2>(blur, count, shift);
-    case 3: return warp_kernel_of<3>(blur, count, shift);
-    default: return warp_kernel_of<0>(blur, count, shift);
-    }
+    if (blur) return shift ? (const void*)pm_sweep_batch_kernel<true, true, SHAPE, TEX>
+                           : (const void*)pm_sweep_batch_kernel<true, false, SHAPE, TEX>;
+    return shift ? (const void*)pm_sweep_batch_kernel<false, true, SHAPE, TEX>
+                 : (const void*)pm_sweep_batch_kernel<false, false, SHAPE, TEX>;
 }
 
 template <int SHAPE>
-static const void* batch_kernel_of(bool blur, bool shift)
+static const void* batch_kernel_of(bool blur, bool shift, bool tex)
 {
-    if (blur) return shift ? (const void*)pm_sweep_batch_kernel<true, true, SHAPE>
-                           : (const void*)pm_sweep_batch_kernel<true, false, SHAPE>;
-    return shift ? (const void*)pm_sweep_batch_kernel<false, true, SHAPE>
-                 : (const void*)pm_sweep_batch_kernel<false, false, SHAPE>;
+    return tex ? batch_kernel_of<SHAPE, true>(blur, shift) : batch_kernel_of<SHAPE, false>(blur, shift);
 }
 
-static const void* batch_kernel(int shape, bool blur, bool shift)
+static const void* batch_kernel(int shape, bool blur, bool shift, bool tex)
 {
     switch (shape) {
-    case 1: return batch_kernel_of<1>(blur, shift);
-    case 2: return batch_kernel_of<2>(blur, shift);
-    case 3: return batch_kernel_of<3>(blur, shift);
-    default: return batch_kernel_of<0>(blur, shift);
+    case 1: return batch_kernel_of<1>(blur, shift, tex);
+    case 2: return batch_kernel_of<2>(blur, shift, tex);
+    case 3: return batch_kernel_of<3>(blur, shift, tex);
+    default: return batch_kernel_of<0>(blur, shift, tex);
     }
 }
 
-static cudaError_t grid_for(const void* k, int threads, int smem, int* n_ctas)
+static cudaError_t grid_for(const void* k, int threads, int smem, int shape, bool tex, int* n_ctas)
 {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = set_smem(k, smem, shape, tex);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
     if (e != cudaSuccess) return e;
@@ -1109,43 +1242,72 @@ static cudaError_t grid_for(const void* k, int threads, int smem, int* n_ctas)
     return cudaSuccess;
 }
 
-cudaError_t sweep_warp_grid(const PmParams& P, bool blur, int* n_ctas, int shape)
+cudaError_t sweep_warp_grid(const FrameDev& F, const PmParams& P, int* n_ctas, int shape)
 {
+    const bool blur = F.blur != nullptr, tex = uses_tex(F, P);
     if (P.tap_counter) shape = 0;
-    return grid_for(warp_kernel(shape, blur, P.tap_counter != nullptr, P.shifted != 0), 32 * sweep_shape_warps(shape),
-                    sweep_warp_smem_bytes(P, blur, shape), n_ctas);
+    return grid_for(warp_kernel(shape, blur, P.tap_counter != nullptr, P.shifted != 0, tex),
+                    32 * sweep_shape_warps(shape), sweep_warp_smem_bytes(P, blur, shape, tex), shape, tex, n_ctas);
 }
 
 cudaError_t launch_sweep_warp(const FrameDev& F, const PmParams& P, const StateDev& prev, const StateDev& next,
                               int iter, int phase, int n_ctas, int* err, cudaStream_t st, int shape)
 {
-    const bool blur = F.blur != nullptr;
+    const bool blur = F.blur != nullptr, tex = uses_tex(F, P);
     if (P.tap_counter) shape = 0;
-    const int smem = sweep_warp_smem_bytes(P, blur, shape);
+    const int smem = sweep_warp_smem_bytes(P, blur, shape, tex);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     const int grid = std::max(1, std::min(n_ctas, F.V));
     cudaError_t qe = cudaMemsetAsync(P.view_queue, 0, sizeof(int), st);
     if (qe != cudaSuccess) return qe;
     FrameDev f = F; PmParams p = P; StateDev a = prev, b = next; int it = iter, ph = phase; int* e = err;
     void* args[] = { &f, &p, &a, &b, &it, &ph, &e };
-    return launch_k(warp_kernel(shape, blur, P.tap_counter != nullptr, P.shifted != 0), grid,
-                    32 * sweep_shape_warps(shape), smem, st, args);
+    return launch_k(warp_kernel(shape, blur, P.tap_counter != nullptr, P.shifted != 0, tex), grid,
+                    32 * sweep_shape_warps(shape), smem, shape, tex, st, args);
 }
 
-cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, int* n_ctas, int shape)
+// One thread per texel; a write outside a surface is dropped (boundary mode
+// zero), though none is made: v % layers < the layers of surface v / layers.
+__global__ void __launch_bounds__(256) tex_fill_kernel(const uint8_t* tiles, int V, int W, int H, int ts,
+                                                       const cudaSurfaceObject_t* surfs, int layers)
 {
-    return grid_for(batch_kernel(shape, blur, shift), 32 * sweep_shape_warps(shape), smem, n_ctas);
+    const int per = W * H;
+    const size_t n = (size_t)V * per;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int v = (int)(e / per), r = (int)(e - (size_t)v * per);
+        const int y = r / W, x = r - y * W;
+        surf2DLayeredwrite<float>((float)tiles[(size_t)v * ts + r], surfs[v / layers], x * (int)sizeof(float), y,
+                                  v % layers, cudaBoundaryModeZero);
+    }
 }
 
-cudaError_t launch_sweep_batch(const SweepItem* items, int n, bool blur, bool shift, int smem, int n_ctas, int* err,
-                               cudaStream_t st, int shape)
+cudaError_t launch_tex_fill(const uint8_t* tiles, int V, int W, int H, int tile_stride,
+                            const cudaSurfaceObject_t* surfs, int layers, cudaStream_t st)
+{
+    if (V <= 0 || W <= 0 || H <= 0 || layers <= 0) return cudaErrorInvalidValue;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t n = (size_t)V * W * H;
+    const int grid = (int)std::min<size_t>((n + 255) / 256, (size_t)std::max(sms, 1) * 8);
+    tex_fill_kernel<<<grid, 256, 0, st>>>(tiles, V, W, H, tile_stride, surfs, layers);
+    return cudaGetLastError();
+}
+
+cudaError_t sweep_batch_grid(int smem, bool blur, bool shift, bool tex, int* n_ctas, int shape)
+{
+    return grid_for(batch_kernel(shape, blur, shift, tex), 32 * sweep_shape_warps(shape), smem, shape, tex, n_ctas);
+}
+
+cudaError_t launch_sweep_batch(const SweepItem* items, int n, bool blur, bool shift, bool tex, int smem, int n_ctas,
+                               int* err, cudaStream_t st, int shape)
 {
     if (n <= 0) return cudaSuccess;
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     const SweepItem* it = items; int nn = n; int* e = err;
     void* args[] = { &it, &nn, &e };
-    return launch_k(batch_kernel(shape, blur, shift), dim3(std::max(1, n_ctas)), 32 * sweep_shape_warps(shape), smem,
-                    st, args);
+    return launch_k(batch_kernel(shape, blur, shift, tex), dim3(std::max(1, n_ctas)), 32 * sweep_shape_warps(shape),
+                    smem, shape, tex, st, args);
 }
 
 }  // namespace pfd
