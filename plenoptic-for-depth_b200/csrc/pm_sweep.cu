@@ -158,6 +158,13 @@ struct Plan {
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+__device__ __forceinline__ float4 lds_f4(uint32_t addr)
+{
+    float4 v;
+    asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
+    return v;
+}
+
 __device__ __forceinline__ uint32_t lds_u32(uint32_t addr)
 {
     uint32_t v;
@@ -357,30 +364,35 @@ __device__ __forceinline__ void build_table(const Quad& T, const PmParams& P, co
 
 // One lane's NCC (ComputeBilateralNCC_Frame, AdaptMIPMFrame.cu:73-179) of the
 // pixel under plane dp against neighbour k.  Every lane of the warp walks the
-// same taps; a lane skips the taps it does not keep.
+// same taps; a lane skips the taps it does not keep.  The loop's invariants
+// (window bounds wb / hb as float bits, quad row stride, tap step) arrive as
+// values, not as fields of the caller's structures (see eval_hyps).
 template <bool BLUR, bool COUNT, bool SHIFT>
-__device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, const float4* tab, const PixWin& pw,
-                                          float3 dp, int k, bool active, float sh, unsigned& ntaps)
+__device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, const float4* tab, const PixWin pw,
+                                          float3 dp, int k, bool active, float sh, unsigned& ntaps, uint32_t wb,
+                                          uint32_t hb, uint32_t q_stride, float finc)
 {
     const NbGeo& g = T.geo[k];
     const float stx = g.stx, sty = g.sty;
-    const uint32_t fold = 0x4B0000u * (uint32_t)(T.qs + 1) * 4u;
+    const uint32_t fold = 0x4B0000u * (q_stride + 1u) * 4u;
     const uint32_t base = T.q_addr + (uint32_t)(k * T.q_bytes) - fold;
     const uint32_t bbase = BLUR ? T.qb_addr + (uint32_t)(k * T.q_bytes) - fold : 0u;
-    const uint32_t qs = (uint32_t)T.qs;
+    const uint32_t qs = q_stride;
+    const uint32_t tab_s = smem_u32(tab);
     float sr = 0.f, srr = 0.f, ss = 0.f, sss = 0.f, srs = 0.f, sw = 0.f, bsx = 0.f, bsy = 0.f;
-    const float finc = (float)P.inc;
     float fxr = (float)pw.x0;
     int t = 0;
     for (int ix = 0; ix < pw.nX; ++ix, fxr = __fadd_rn(fxr, finc)) {
         const float axr = __fmul_rn(dp.x, fxr);
         float fyr = (float)pw.y0;
+        // two taps per iteration, the table read through its shared-window address
+#pragma unroll 2
         for (int iy = 0; iy < pw.nY; ++iy, ++t, fyr = __fadd_rn(fyr, finc)) {
-            const float4 e = tab[t];
+            const float4 e = lds_f4(tab_s + (uint32_t)t * 16u);
             const float d = __fadd_rn(__fmaf_rn(dp.y, fyr, axr), dp.z);
             const float sx = __fmaf_rn(stx, d, fxr);
             const float sy = __fmaf_rn(sty, d, fyr);
-            const bool v = active && (__float_as_uint(sx) < P.W_bits) && (__float_as_uint(sy) < P.H_bits);
+            const bool v = active && (__float_as_uint(sx) < wb) && (__float_as_uint(sy) < hb);
             if (COUNT) ntaps += v ? 1u : 0u;
             if (v) {                         // a skipped tap leaves the sums as they are
                 const int tbx = tex_coord_bits(sx), tby = tex_coord_bits(sy);
@@ -432,8 +444,9 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
 // which leaves the sum as it is (a sum starts at +0 and never becomes -0), so
 // the sums are the ones of the skipped taps without a branch.
 template <bool BLUR, bool COUNT, bool SHIFT>
-__device__ __forceinline__ float ncc_lane_tex(const Quad& T, const PmParams& P, const float4* tab, const PixWin& pw,
-                                              float3 dp, int k, bool active, float sh, unsigned& ntaps)
+__device__ __forceinline__ float ncc_lane_tex(const Quad& T, const PmParams& P, const float4* tab, const PixWin pw,
+                                              float3 dp, int k, bool active, float sh, unsigned& ntaps, uint32_t wb,
+                                              uint32_t hb, float finc)
 {
     const NbGeo& g = T.geo[k];
     const float stx = g.stx, sty = g.sty;
@@ -441,7 +454,6 @@ __device__ __forceinline__ float ncc_lane_tex(const Quad& T, const PmParams& P, 
     const cudaTextureObject_t txb = BLUR ? T.txbh[k] : 0;
     const int layer = T.txl[k];
     float sr = 0.f, srr = 0.f, ss = 0.f, sss = 0.f, srs = 0.f, sw = 0.f, bsx = 0.f, bsy = 0.f;
-    const float finc = (float)P.inc;
     float fxr = (float)pw.x0;
     int t = 0;
     for (int ix = 0; ix < pw.nX; ++ix, fxr = __fadd_rn(fxr, finc)) {
@@ -453,7 +465,7 @@ __device__ __forceinline__ float ncc_lane_tex(const Quad& T, const PmParams& P, 
             const float d = __fadd_rn(__fmaf_rn(dp.y, fyr, axr), dp.z);
             const float sx = __fmaf_rn(stx, d, fxr);
             const float sy = __fmaf_rn(sty, d, fyr);
-            const bool v = active && (__float_as_uint(sx) < P.W_bits) && (__float_as_uint(sy) < P.H_bits);
+            const bool v = active && (__float_as_uint(sx) < wb) && (__float_as_uint(sy) < hb);
             if (COUNT) ntaps += v ? 1u : 0u;
             const float cx = __fadd_rn(sx, 0.5f), cy = __fadd_rn(sy, 0.5f);
             float s = 0.0f;
@@ -502,8 +514,16 @@ __device__ __forceinline__ float ncc_lane_tex(const Quad& T, const PmParams& P, 
 // skip: S.cost[h * K + k] for the neighbours k < nc whose bit is set in vmask
 // (the other entries are left as they are).  A neighbour whose anchor leaves
 // the window gets 2 without evaluation.
+//
+// Not inlined (its seven call sites would overflow the instruction cache), so
+// what its tap loop reads on every tap arrives by value: the window, its bounds
+// (wb, hb: (float)W and (float)H as bits), the quad row stride, the tap step and
+// the tap table.  Read through references into the caller's frame they were
+// reloaded from local memory on every tap (2.0e9 local loads in one half-sweep
+// of a 2048x1536 frame, 3.2e8 with the values passed; 8% of the sweep's time).
 template <bool BLUR, bool COUNT, bool SHIFT, bool TEX>
-__device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const WarpBlock& S, const PixWin& pw,
+__device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const WarpBlock& S, const PixWin pw,
+                                       uint32_t wb, uint32_t hb, uint32_t q_stride, float finc, const float4* tab,
                                        int px, int py, int nh, int nc, int lane, uint64_t skip, uint32_t vmask)
 {
     const int K = P.K;
@@ -539,8 +559,8 @@ __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const W
         const int h = n / nc, k = n - h * nc;
         const float4 d = S.dp[h];
         const float3 dp = make_float3(d.x, d.y, d.z);
-        const float c = TEX ? ncc_lane_tex<BLUR, COUNT, SHIFT>(T, P, S.tab, pw, dp, k, act, sh, ntaps)
-                            : ncc_lane<BLUR, COUNT, SHIFT>(T, P, S.tab, pw, dp, k, act, sh, ntaps);
+        const float c = TEX ? ncc_lane_tex<BLUR, COUNT, SHIFT>(T, P, tab, pw, dp, k, act, sh, ntaps, wb, hb, finc)
+                            : ncc_lane<BLUR, COUNT, SHIFT>(T, P, tab, pw, dp, k, act, sh, ntaps, wb, hb, q_stride, finc);
         if (act) S.cost[h * K + k] = c;
     }
     if (COUNT) {
@@ -554,8 +574,8 @@ __device__ __noinline__ void eval_hyps(const Quad& T, const PmParams& P, const W
 // one lane per hypothesis; view weights packed 4 bits per view.  Only the
 // views in vmask are read: the weighted cost is exact whenever vmask holds
 // every view of non-zero weight, the lowest-cost index covers vmask's views.
-__device__ __forceinline__ void weigh_hyps(const WarpBlock& S, int K, int nh, int nc, uint64_t vw_lo, uint64_t vw_hi,
-                                           int lane, uint32_t vmask)
+__device__ __noinline__ void weigh_hyps(const WarpBlock& S, int K, int nh, int nc, uint64_t vw_lo, uint64_t vw_hi,
+                                        int lane, uint32_t vmask)
 {
     for (int h = lane; h < nh; h += 32) {
         WeightedCost wc;
@@ -678,8 +698,8 @@ __device__ __forceinline__ float4 proposal_plane(const NbGeo& gk, const float4* 
 // 400-471) for the best plane `best`, from the draws already taken (c0: the
 // random plane, rn: the random normal, u1-u3: the perturbation, u4: the depth
 // perturbation).
-__device__ __forceinline__ void refine_candidates(int x, int y, float4 best, float4 c0, float4 rn, float u1, float u2,
-                                                  float u3, float u4, float pert, float4 (&cand)[5])
+__device__ __noinline__ void refine_candidates(int x, int y, float4 best, float4 c0, float4 rn, float u1, float u2,
+                                               float u3, float u4, float pert, float4 (&cand)[5])
 {
     const float depth_now = best.w;
     const float4 pn = perturbed_normal_u(x, y, best, u1, u2, u3, pert);
@@ -783,6 +803,12 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
             const size_t idx = vbase + center;
             const PixWin pw = pixel_window(P, x, y);
             build_table<BLUR>(T, P, pw, x, y, S.tab, lane);
+            // NCC passes of this pixel: hypotheses [0, nh) on the views in vmask, except
+            // the hypotheses in skip (the tap loop's invariants by value, see eval_hyps)
+            auto eval = [&](int nh_, uint64_t skip, uint32_t vmask) {
+                eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, P.W_bits, P.H_bits, (uint32_t)T.qs, (float)P.inc, S.tab,
+                                                   x, y, nh_, nc, lane, skip, vmask);
+            };
 
             // ---- propagation candidates and the current plane --------------
             // Row 0 holds the current plane, then one row per distinct candidate plane:
@@ -818,7 +844,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
             const bool use_cvec = !COUNT && P.cvec_ok;
             if (use_cvec && lane < nc) S.cost[lane] = P.cvec[idx * K + lane];
             __syncwarp();
-            eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, nh, nc, lane, use_cvec ? 1ull : 0ull, ~0u);
+            eval(nh, use_cvec ? 1ull : 0ull, ~0u);
 #define SLOT(s) ((int)((slots >> (4 * (s))) & 15ull))
 #define COSTA(s, k) S.cost[SLOT(s) * K + (k)]
 
@@ -941,7 +967,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                 if (lane == 0)
                     for (int i = 0; i < 5; ++i) S.plane[r0 + i] = cand[i];
                 __syncwarp();
-                eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, r0 + 5, nc, lane, skip3 ? (1ull << (r0 + 3)) : 0ull, tsel);
+                eval(r0 + 5, skip3 ? (1ull << (r0 + 3)) : 0ull, tsel);
                 weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
 
                 bool changed = false;
@@ -967,7 +993,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                         __syncwarp();
                         if (lane == 0) S.plane[row] = proxy;
                         __syncwarp();
-                        eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, row + 1, nc, lane, (1ull << row) - 1ull, tsel);
+                        eval(row + 1, (1ull << row) - 1ull, tsel);
                         weigh_hyps(S, K, row + 1, nc, vw_lo, vw_hi, lane, tsel);
                         c = S.wres[row];
                         cmin = S.wmin[row];
@@ -984,7 +1010,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                         for (int i = 2; i < 5; ++i) S.plane[r0 + i] = cand[i];
                     __syncwarp();
                     const uint64_t redo = (7ull << (r0 + 2)) & ~(skip3 ? (1ull << (r0 + 3)) : 0ull);
-                    eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, r0 + 5, nc, lane, ~redo, tsel);
+                    eval(r0 + 5, ~redo, tsel);
                     weigh_hyps(S, K, r0 + 5, nc, vw_lo, vw_hi, lane, tsel);
                 }
                 for (int i = 0; i < 5; ++i) {
@@ -1004,7 +1030,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                     __syncwarp();
                     if (lane == 0) S.plane[0] = proxy;
                     __syncwarp();
-                    eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
+                    eval(1, 0ull, ~0u);
                     weigh_hyps(S, K, 1, nc, vw_lo, vw_hi, lane, ~0u);
                     const float c = S.wres[0];
                     if (c < best_cost) { best_cost = c; best_plane = proxy; best_min = S.wmin[0]; }
@@ -1015,7 +1041,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                 if (lane == 0)
                     for (int i = 0; i < 5; ++i) S.plane[i] = cand[i];
                 __syncwarp();
-                eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, 5, nc, lane, 0ull, ~0u);
+                eval(5, 0ull, ~0u);
                 weigh_hyps(S, K, 5, nc, vw_lo, vw_hi, lane, ~0u);
                 for (int i = 0; i < 5; ++i) {
                     const float c = S.wres[i];
@@ -1032,7 +1058,7 @@ __device__ __forceinline__ bool sweep_frame(unsigned char* smem, const FrameDev&
                 __syncwarp();
                 if (lane == 0) S.plane[0] = best_plane;
                 __syncwarp();
-                eval_hyps<BLUR, COUNT, SHIFT, TEX>(T, P, S, pw, x, y, 1, nc, lane, 0ull, ~0u);
+                eval(1, 0ull, ~0u);
                 weigh_hyps(S, K, 1, nc, vw_lo, vw_hi, lane, ~0u);
                 best_min = S.wmin[0];
                 best_vec = lane < nc ? S.cost[lane] : 0.0f;
