@@ -174,7 +174,10 @@ pfd_status pfd_patchmatch(pfd_ctx* ctx, int frame_id, const pfd_pm_params* param
  * ones do not leave the GPU idle between launches.  params[b] and seeds[b] are
  * frame b's own (sizes, neighbour counts, patch sizes and iteration counts may
  * all differ); every frame's result is bit for bit what pfd_patchmatch gives it
- * alone.  Tap counting (pfd_set_tap_counting) runs the frames one by one. */
+ * alone.  A frame whose micro-images fill the sweep's grid four times over or
+ * more runs as pfd_patchmatch (measured slower inside a shared launch); the
+ * others share launches.  Tap counting (pfd_set_tap_counting) runs the frames
+ * one by one. */
 pfd_status pfd_patchmatch_batch(pfd_ctx* ctx, const int* frame_ids, int n, const pfd_pm_params* params,
                                 const uint64_t* seeds);
 /* CUDA graphs for the context's later pfd_patchmatch calls and enqueue-only

@@ -12,11 +12,7 @@
 // the tile are gathered from a bucket grid of lens centres, sorted by view
 // index (so the sum order is the oracle's), and their micro-images are staged
 // through shared memory in chunks.  A warp owns output rows, so the row test of
-// a lens is warp-uniform; each lane owns two columns.  The micro-image
-// coordinates of a staged lens depend only on the column (u) or only on the row
-// (w): they are computed once per (lens, column) and (lens, row) into shared
-// memory, the same IEEE expressions, by all threads together, instead of by
-// every thread for its own pixels (four divisions per lens and thread).
+// a lens is warp-uniform; each lane owns two columns.
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "refocus_kernels.h"
@@ -38,8 +34,6 @@ __global__ void __launch_bounds__(kThreads) pm_refocus_kernel(RefocusFrame F, co
     int* sorted = cand + kMaxRefocusCand;                    // [kMaxRefocusCand] ascending
     float2* cc = (float2*)(sorted + kMaxRefocusCand);        // [kChunk] centres of the staged chunk
     uint8_t* tiles = (uint8_t*)(cc + kChunk);                // [kChunk][tile_stride]
-    float* U = (float*)(tiles + (size_t)kChunk * F.tile_stride);   // [kChunk][kTileW] u of lens t, column
-    float* Wr = U + kChunk * kTileW;                         // [kChunk][kTileH] w of lens t, row
     __shared__ int n_cand;
 
     const int s = blockIdx.z;
@@ -93,6 +87,9 @@ __global__ void __launch_bounds__(kThreads) pm_refocus_kernel(RefocusFrame F, co
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float sum[2][2] = { { 0.f, 0.f }, { 0.f, 0.f } };
     int cnt[2][2] = { { 0, 0 }, { 0, 0 } };
+    float Xa[2], Yb[2];
+    for (int a = 0; a < 2; ++a) Xa[a] = ((float)(ox0 + lane + 32 * a) + 0.5f) * sx - 0.5f;
+    for (int b = 0; b < 2; ++b) Yb[b] = ((float)(oy0 + warp + 8 * b) + 0.5f) * sy - 0.5f;
     const int words = F.tile_stride / 16;
     for (int base = 0; base < n; base += kChunk) {
         const int nc = min(kChunk, n - base);
@@ -104,23 +101,14 @@ __global__ void __launch_bounds__(kThreads) pm_refocus_kernel(RefocusFrame F, co
         }
         for (int t = threadIdx.x; t < nc; t += blockDim.x) cc[t] = F.centers[sorted[base + t]];
         __syncthreads();
-        for (int e = threadIdx.x; e < nc * kTileW; e += blockDim.x) {
-            const int t = e / kTileW, col = e - t * kTileW;
-            const float X = ((float)(ox0 + col) + 0.5f) * sx - 0.5f;
-            U[e] = __fadd_rn(__fdiv_rn(__fsub_rn(X, cc[t].x), v), cmx);
-        }
-        for (int e = threadIdx.x; e < nc * kTileH; e += blockDim.x) {
-            const int t = e / kTileH, row = e - t * kTileH;
-            const float Y = ((float)(oy0 + row) + 0.5f) * sy - 0.5f;
-            Wr[e] = __fadd_rn(__fdiv_rn(__fsub_rn(Y, cc[t].y), v), cmy);
-        }
-        __syncthreads();
         for (int t = 0; t < nc; ++t) {
+            const float2 c = cc[t];
             const uint8_t* T = tiles + (size_t)t * F.tile_stride;
+            // the column coordinates do not depend on the row: one division per column
             float ua[2];
-            for (int a = 0; a < 2; ++a) ua[a] = U[t * kTileW + lane + 32 * a];
+            for (int a = 0; a < 2; ++a) ua[a] = __fadd_rn(__fdiv_rn(__fsub_rn(Xa[a], c.x), v), cmx);
             for (int b = 0; b < 2; ++b) {
-                const float w = Wr[t * kTileH + warp + 8 * b];                          // warp-uniform
+                const float w = __fadd_rn(__fdiv_rn(__fsub_rn(Yb[b], c.y), v), cmy);   // warp-uniform
                 if (!(w >= 0.0f && w <= wmax)) continue;
                 const int y0 = (int)floorf(w);
                 const int y1 = min(y0 + 1, mh - 1);
@@ -155,7 +143,7 @@ __global__ void __launch_bounds__(kThreads) pm_refocus_kernel(RefocusFrame F, co
 
 int refocus_smem_bytes(const RefocusFrame& F)
 {
-    return 2 * kMaxRefocusCand * 4 + kChunk * 8 + kChunk * F.tile_stride + kChunk * (kTileW + kTileH) * 4;
+    return 2 * kMaxRefocusCand * 4 + kChunk * 8 + kChunk * F.tile_stride;
 }
 
 cudaError_t launch_refocus(const RefocusFrame& F, const float* slice_vd, int n_slices, int raw_w, int raw_h, int out_w,

@@ -68,3 +68,26 @@ def test_batch_rejects_bad_lists(pfd):
             ctx.patchmatch_batch([ids[0], ids[0]], [fr[0][1], fr[0][1]], [1, 2])
         with pytest.raises(pfd.PfdError):
             ctx.patchmatch_batch([ids[0], 999], [fr[0][1], fr[1][1]], [1, 2])
+
+
+def test_batch_with_grid_filling_frames(pfd):
+    """A batch holding frames that fill the sweep's grid four times over (run as
+    their own launches) and small frames (sharing launches): every frame equals
+    pfd_patchmatch alone."""
+    with pfd.Context(0) as ctx:
+        big = pfd.make_workload(2048, 1536, 23.2, 4, seed=71, max_nb=8)
+        assert big.centers.shape[0] >= 4 * 4 * 148       # four times a grid of 4 CTAs per SM on 148 SMs
+        fr = _frames(pfd, ctx)[:2]
+        fb = ctx.frame_upload(big.frame.raw, big.centers, big.tilekeys, big.mi, big.mi, big.nb_ids, big.nb_counts)
+        fr.insert(1, (fb, pfd.PmParams(base=23.2, patch_size=11, max_iterations=1), 77))
+        alone = []
+        for fid, P, seed in fr:
+            ctx.patchmatch(fid, P, seed)
+            alone.append(ctx.download(fid))
+        ctx.patchmatch_batch([f for f, _, _ in fr], [P for _, P, _ in fr], [s for _, _, s in fr])
+        for b, (fid, _, _) in enumerate(fr):
+            got = ctx.download(fid)
+            for name, x, y in zip(("plane", "cost", "disp", "sel"), got, alone[b]):
+                assert _same(x, y), f"frame {b}: {name} differs at {np.count_nonzero(x != y)} entries"
+        for fid, _, _ in fr:
+            ctx.frame_free(fid)
