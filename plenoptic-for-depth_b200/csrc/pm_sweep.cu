@@ -439,10 +439,11 @@ __device__ __forceinline__ float ncc_lane(const Quad& T, const PmParams& P, cons
 }
 
 // ncc_lane with the neighbour samples fetched by the texture unit, as the
-// reference's tex2D(images[id], x + 0.5, y + 0.5) fetches them.  Every lane
-// fetches every tap; a tap outside the neighbour window adds +0 to each sum,
-// which leaves the sum as it is (a sum starts at +0 and never becomes -0), so
-// the sums are the ones of the skipped taps without a branch.
+// reference's tex2D(images[id], x + 0.5, y + 0.5) fetches them.  A lane fetches
+// only the taps inside the neighbour window (the fetch is predicated); a tap
+// outside it adds +0 to each sum, which leaves the sum as it is (a sum starts
+// at +0 and never becomes -0), so the sums are the ones of the skipped taps
+// without a branch around the accumulation.
 template <bool BLUR, bool COUNT, bool SHIFT>
 __device__ __forceinline__ float ncc_lane_tex(const Quad& T, const PmParams& P, const float4* tab, const PixWin pw,
                                               float3 dp, int k, bool active, float sh, unsigned& ntaps, uint32_t wb,
